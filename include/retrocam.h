@@ -1,0 +1,323 @@
+/*
+ * retrocam.h -- C ABI of the B200 render hot path of RetroCam.
+ *
+ * The library replaces the bodies of three Java classes of the reference:
+ *   core/Renderer.java        (path-trace accumulation, pathtrace.comp)
+ *   scene/SPPMManager.java    (photon trace + gather, photon_trace.comp /
+ *                              photon_gather.comp, PhotonMap.java)
+ *   post/AtrousDenoiser.java  (post/atrous_denoise.frag, p00_normalize.frag)
+ * and offers the host-side scene logic those classes rely on
+ * (scene/BVHBuilder.java, scene/SceneUploader.java, scene/Box.java,
+ * scene/Sphere.java, scene/TransformedPrimitive.java,
+ * camera/ThinLensCamera.java) so a caller can stay in Java and bind these
+ * symbols with Panama FFM or JNI.
+ *
+ * Conventions:
+ *   - Every function returns an int: RC_OK (0) or a negative RC_ERR_* code.
+ *     rc_last_error() gives the text of the last failure on a context.
+ *   - No exceptions cross the ABI; no torch or CUDA types in signatures.
+ *   - Host arrays are owned by the caller and copied at call time; device
+ *     buffers are owned by the context.
+ *   - One rc_ctx owns one CUDA stream on one device.  Calls on one context
+ *     must be serialised by the caller; different contexts may be driven
+ *     from different threads.
+ *   - Struct layouts are the std430 layouts of the reference SSBOs, so the
+ *     Java side can pass its existing FloatBuffers unchanged.
+ */
+#ifndef RETROCAM_H
+#define RETROCAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RC_ABI_VERSION 1
+
+/* ---- status codes ---- */
+#define RC_OK 0
+#define RC_ERR_INVALID_ARG (-1)   /* null pointer, bad size, bad enum       */
+#define RC_ERR_CUDA (-2)          /* a CUDA runtime call failed             */
+#define RC_ERR_OUT_OF_MEMORY (-3) /* device allocation failed               */
+#define RC_ERR_NO_SCENE (-4)      /* render/trace before rc_scene_upload    */
+#define RC_ERR_DEVICE_GUARD (-5)  /* a kernel hit an iteration cap or a bad
+                                     index and stopped; see rc_counters     */
+#define RC_ERR_CAPACITY (-6)      /* output array too small                 */
+#define RC_ERR_BAD_SCENE (-7)     /* scene failed validation (e.g. a BVH
+                                     child index out of range)              */
+
+/* ---- std430 scene records (layouts of the reference SSBOs) ---- */
+
+/* scene/GpuTriangle.java:68-78, 128 bytes. */
+typedef struct rc_triangle {
+    float v0[3]; float pad0;
+    float v1[3]; float pad1;
+    float v2[3]; float pad2;
+    float n0[3]; float pad3;
+    float n1[3]; float pad4;
+    float n2[3]; float pad5;
+    float uv0[2]; float uv1[2];
+    float uv2[2]; int32_t mat_index; float pad6;
+} rc_triangle;
+
+/* scene/BVHNode.java:32-41, 48 bytes.  prim_count > 0 marks a leaf. */
+typedef struct rc_bvh_node {
+    float aabb_min[3]; float pad0;
+    float aabb_max[3]; float pad1;
+    int32_t left_child, right_child, prim_start, prim_count;
+} rc_bvh_node;
+
+/* scene/Material.java:61-69, 64 bytes. */
+typedef struct rc_material {
+    float albedo[3]; float metallic;
+    float emission[3]; float emission_strength;
+    float roughness; float ior; float transmission; int32_t albedo_tex;
+    float pad[4];
+} rc_material;
+
+/* scene/SceneUploader.java:18-23, 80 bytes. */
+typedef struct rc_light {
+    float v0[3]; float area;
+    float v1[3]; float pad1;
+    float v2[3]; float pad2;
+    float emission[3]; float power;
+    float normal[3]; float cdf_weight;
+} rc_light;
+
+/* scene/PhotonMap.java:16-21, 48 bytes. */
+typedef struct rc_photon {
+    float position[3]; float pad0;
+    float power[3]; float pad1;
+    float dir[3]; float pad2;
+} rc_photon;
+
+/* Uniforms of pathtrace.comp:11-24 as set by camera/ThinLensCamera.java:27-58.
+ * focal_dist is the caller's (for parity runs: RenderSettings.focusDistM). */
+typedef struct rc_camera {
+    float cam_pos[3];
+    float cam_right[3];
+    float cam_up[3];
+    float cam_forward[3];
+    float focal_dist;
+    float lens_radius;
+    float fov_tan_half;
+    int32_t aperture_blades;
+    float sa_strength;
+    float lca_delta[3];
+} rc_camera;
+
+/* NEE uniforms of pathtrace.comp:32-35 (core/Renderer.java:93-96). */
+typedef struct rc_settings {
+    int32_t nee_enabled;
+    float nee_firefly_clamp;
+} rc_settings;
+
+/* SPPM knobs (core/RenderSettings.java:35-38, scene/PhotonMap.java:33-36). */
+typedef struct rc_sppm_params {
+    int32_t photon_count;   /* photons emitted per iteration (<= capacity) */
+    int32_t hash_size;      /* power of two */
+    float alpha;            /* radius shrink parameter */
+} rc_sppm_params;
+
+/* À-trous knobs (core/RenderSettings.java:89-94, AtrousDenoiser.java:60-125). */
+typedef struct rc_atrous_params {
+    int32_t enabled;
+    int32_t iterations;     /* clamped to [1,5] */
+    float sigma_color;
+    float sigma_normal;
+    float sigma_depth;
+    int32_t max_spp;        /* 0 = always active */
+    float exposure;
+} rc_atrous_params;
+
+/* Device counters (replace the reference's console summaries and the BVH
+ * heat-map shader with numbers). */
+typedef struct rc_counters {
+    uint64_t camera_paths;   /* traced paths (3 per sample with LCA) */
+    uint64_t closest_rays;   /* closest-hit traversals (path tracer + g-buffer) */
+    uint64_t shadow_rays;    /* any-hit traversals (NEE) */
+    uint64_t photon_rays;    /* photon traversals */
+    uint64_t gather_rays;    /* gather pinhole/specular traversals */
+    uint64_t photons_stored; /* photons that reached the hash last trace */
+    uint32_t error_word;     /* RC_GUARD_* bits raised by kernels */
+    uint32_t reserved;
+} rc_counters;
+
+/* error_word bits. */
+#define RC_GUARD_TRAVERSAL_CAP 0x1u  /* a traversal exceeded its node-visit cap */
+#define RC_GUARD_BAD_INDEX 0x2u      /* a node/primitive/material index was out of range */
+#define RC_GUARD_CHAIN_CAP 0x4u      /* reserved: gather chain cap (512) is a
+                                        reference semantic, not an error */
+
+/* Math modes of the kernels. */
+#define RC_MATH_FAST 0   /* FMA contraction, CUDA intrinsics; checked by tolerance */
+#define RC_MATH_EXACT 1  /* no contraction, rc_exact_math.h transcendentals;
+                            bit-identical to the CPU oracle */
+
+typedef struct rc_ctx rc_ctx;
+
+/* ---------------------------------------------------------------------------
+ * Context
+ * ------------------------------------------------------------------------- */
+
+/* Creates a context rendering width x height on a CUDA device; allocates the
+ * accumulation (RGBA32F), G-buffer (RGBA16F), albedo (RGBA16F) and variance
+ * (R32F) images of core/Renderer.java:152-193. */
+int rc_ctx_create(int width, int height, int device, rc_ctx** out);
+int rc_ctx_destroy(rc_ctx* ctx);
+/* Copies the last error text of ctx (or of the last failed rc_ctx_create
+ * when ctx is NULL) into buf, NUL-terminated. */
+int rc_last_error(const rc_ctx* ctx, char* buf, size_t n);
+int rc_set_math_mode(rc_ctx* ctx, int mode);
+int rc_synchronize(rc_ctx* ctx);
+int rc_abi_version(void);
+
+/* ---------------------------------------------------------------------------
+ * Host scene logic (bit-exact restatements of the reference's Java)
+ * ------------------------------------------------------------------------- */
+
+/* scene/Box.java:25-76 plus scene/TransformedPrimitive.java:32-95 (applied
+ * when any rotation is non-zero, as scene/SceneObject.java:80-88 does).
+ * Writes 12 triangles. */
+int rc_tessellate_box(float cx, float cy, float cz, float hx, float hy, float hz,
+                      int mat_index, float rot_x_deg, float rot_y_deg, float rot_z_deg,
+                      rc_triangle* out12);
+
+/* scene/Sphere.java:34-101 (+ rotation as above).  Writes
+ * 2*stacks*slices - 2*slices triangles (poles skipped). */
+int rc_tessellate_sphere(float cx, float cy, float cz, float radius, int mat_index,
+                         int stacks, int slices, float rot_x_deg, float rot_y_deg,
+                         float rot_z_deg, rc_triangle* out, int capacity, int* count);
+
+/* A flat-normal triangle list from vertex positions (9 floats each), as the
+ * reference's Primitive.toTriangles extension point would produce with
+ * GpuTriangle.withFlatNormal (scene/GpuTriangle.java:38-50). */
+int rc_triangles_from_positions(const float* positions, int count, int mat_index,
+                                rc_triangle* out);
+
+/* scene/BVHBuilder.java:35-202: binned SAH (8 buckets, leaf <= 4,
+ * C_trav 1, C_isect 1.5), depth-first node order, in-place partition.
+ * Writes the reordered triangles and the nodes; node_capacity >= 2*count. */
+int rc_build_bvh(const rc_triangle* in, int count, rc_triangle* out_tris,
+                 rc_bvh_node* out_nodes, int node_capacity, int* node_count);
+
+/* scene/SceneUploader.java:144-216: light list (BVH triangle order) with
+ * power = luma601 * area * pi and a CDF whose last entry is 1.  With no
+ * emissive triangle it writes one zeroed stub and *light_count = 0. */
+int rc_build_lights(const rc_triangle* tris, int count, const rc_material* mats,
+                    int material_count, rc_light* out, int capacity,
+                    int* light_count, float* total_power);
+
+/* camera/ThinLensCamera.java:27-68: lens radius f/(2N) and tan(fov/2) for a
+ * 24 mm sensor height. */
+int rc_thin_lens(float focal_length_mm, float f_stop, float* lens_radius,
+                 float* fov_tan_half);
+
+/* camera/OrbitCamera.java:155-171,274-291: eye, forward, right, up from
+ * orbit angles about a target. out12 = eye[3], forward[3], right[3], up[3]. */
+int rc_orbit_basis(float theta, float phi, float radius, float target_x,
+                   float target_y, float target_z, float* out12);
+
+/* scene/SPPMManager.java:170-173: r *= (float)sqrt((n+alpha)/(n+1.0)). */
+float rc_sppm_next_radius(float radius, int iteration, float alpha);
+
+/* keyframe/KeyframeTrack.java:102-178. interp[i]: 0 STEP, 1 LINEAR,
+ * 2 BEZIER (Catmull-Rom Hermite).  times ascending. */
+float rc_keyframe_evaluate(const float* times, const float* values,
+                           const int32_t* interp, int count, float time,
+                           float default_value);
+
+/* ---------------------------------------------------------------------------
+ * Device scene
+ * ------------------------------------------------------------------------- */
+
+/* scene/SceneUploader.java:54-99 after the BVH build: copies the four SSBO
+ * arrays to the device (converting them to the kernels' internal layout)
+ * and validates node and material indices (RC_ERR_BAD_SCENE on failure).
+ * lights may be NULL when light_count == 0. */
+int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count,
+                    const rc_bvh_node* nodes, int node_count,
+                    const rc_material* mats, int material_count,
+                    const rc_light* lights, int light_count, float total_light_power);
+
+/* ---------------------------------------------------------------------------
+ * Path tracer (core/Renderer.java:72-130, pathtrace.comp)
+ * ------------------------------------------------------------------------- */
+
+/* Adds n_spp samples per pixel with frame indices first_frame ..
+ * first_frame+n_spp-1 (u_frameIndex); frame 0 clears the accumulation and
+ * writes the G-buffer and albedo images. */
+int rc_render(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings,
+              int first_frame, int n_spp);
+
+/* Renderer.reset(): zeroes the images and the sample counter. */
+int rc_reset(rc_ctx* ctx);
+/* Samples accumulated since the last reset (Renderer.getTotalSamples). */
+int rc_total_samples(const rc_ctx* ctx);
+
+/* ---------------------------------------------------------------------------
+ * SPPM (scene/SPPMManager.java, scene/PhotonMap.java)
+ * ------------------------------------------------------------------------- */
+
+/* SPPMManager.reset: radius = r0, iteration = 0. */
+int rc_sppm_reset(rc_ctx* ctx, float initial_radius);
+/* SPPMManager.tracePhotons: clears the hash (PhotonMap.clear) and traces
+ * photon_count photons with seed iteration*7919+6271 at the current radius. */
+int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* params);
+/* SPPMManager.gatherRadiance: adds weight * caustic radiance into the
+ * accumulation image (weight 1 is the reference; the export loop uses
+ * spp/iterations when iterations < spp). */
+int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* params,
+                   float weight);
+/* SPPMManager.updateRadius. */
+int rc_sppm_update_radius(rc_ctx* ctx, float alpha);
+int rc_sppm_state(const rc_ctx* ctx, float* radius, int* iteration);
+
+/* ---------------------------------------------------------------------------
+ * Denoiser (post/AtrousDenoiser.java:60-125, PostProcessStack.java:112-147)
+ * ------------------------------------------------------------------------- */
+
+/* p00 normalisation then 1..5 à-trous passes (or the normalised image alone
+ * when disabled or over max_spp).  Result stays on the device; when
+ * out_rgba is non-NULL it is also copied to that host array (W*H*4 floats). */
+int rc_denoise_atrous(rc_ctx* ctx, const rc_atrous_params* params, float* out_rgba);
+
+/* ---------------------------------------------------------------------------
+ * Whole export frame (export/RenderPipeline.java:209-239)
+ * ------------------------------------------------------------------------- */
+
+/* renderer.reset; sppm.reset; for each block of spp/sppm_iterations samples:
+ * trace photons -> render the block -> gather (weighted) -> shrink radius;
+ * then p00 + à-trous.  sppm_iterations == spp reproduces the reference
+ * order exactly; sppm_iterations == 0 disables SPPM.  out_rgba (nullable)
+ * receives the denoised frame. */
+int rc_render_frame(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings,
+                    int spp, const rc_sppm_params* sppm, float sppm_initial_radius,
+                    int sppm_iterations, const rc_atrous_params* atrous,
+                    float* out_rgba);
+
+/* ---------------------------------------------------------------------------
+ * Read-back and counters
+ * ------------------------------------------------------------------------- */
+
+/* Copies the images to host arrays (any may be NULL): accum W*H*4 floats,
+ * gbuf/galb W*H*4 halves, variance W*H floats. */
+int rc_read_buffers(rc_ctx* ctx, float* accum_rgba, uint16_t* gbuffer_rgba16f,
+                    uint16_t* albedo_rgba16f, float* variance);
+/* Copies the last denoised/normalised frame (W*H*4 floats). */
+int rc_read_output(rc_ctx* ctx, float* out_rgba);
+/* Copies the photon map of the last trace (any may be NULL): photons
+ * (capacity entries), heads (hash_size), next (capacity), counter. */
+int rc_read_photon_map(rc_ctx* ctx, rc_photon* photons, int photon_capacity,
+                       int32_t* heads, int hash_size, int32_t* next,
+                       uint32_t* counter);
+int rc_get_counters(rc_ctx* ctx, rc_counters* out);
+int rc_reset_counters(rc_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RETROCAM_H */
