@@ -141,9 +141,26 @@ typedef struct rc_counters {
     uint64_t photon_rays;    /* photon traversals */
     uint64_t gather_rays;    /* gather pinhole/specular traversals */
     uint64_t photons_stored; /* photons that reached the hash last trace */
+    uint64_t node_tests;     /* ray-box tests of the path tracer */
+    uint64_t tri_tests;      /* ray-triangle tests of the path tracer */
+    uint64_t surface_hits;   /* path-tracer closest hits shaded (normal + material) */
+    uint64_t light_samples;  /* NEE light records fetched */
+    uint64_t photon_node_tests; /* ray-box tests of photon trace + gather */
+    uint64_t photon_tri_tests;  /* ray-triangle tests of photon trace + gather */
+    uint64_t kernel_launches;/* kernels this context launched */
+    uint64_t h2d_bytes;      /* host -> device bytes copied by this context */
+    uint64_t d2h_bytes;      /* device -> host bytes copied by this context */
     uint32_t error_word;     /* RC_GUARD_* bits raised by kernels */
     uint32_t reserved;
 } rc_counters;
+
+/* Kernel kinds for rc_get_kernel_times. */
+#define RC_KERNEL_RENDER 0
+#define RC_KERNEL_PHOTON_TRACE 1
+#define RC_KERNEL_PHOTON_GATHER 2
+#define RC_KERNEL_ATROUS 3
+#define RC_KERNEL_NORMALIZE 4
+#define RC_KERNEL_KINDS 5
 
 /* error_word bits. */
 #define RC_GUARD_TRAVERSAL_CAP 0x1u  /* a traversal exceeded its node-visit cap */
@@ -172,6 +189,14 @@ int rc_ctx_destroy(rc_ctx* ctx);
 int rc_last_error(const rc_ctx* ctx, char* buf, size_t n);
 int rc_set_math_mode(rc_ctx* ctx, int mode);
 int rc_synchronize(rc_ctx* ctx);
+/* Runs the context's work on a caller-owned cudaStream_t (passed as void*),
+ * or on the context's own stream again when cuda_stream is NULL. */
+int rc_ctx_set_stream(rc_ctx* ctx, void* cuda_stream);
+/* When enabled, every kernel launch is bracketed by CUDA events on the
+ * launching stream; rc_get_kernel_times synchronises and returns, per kernel
+ * kind, the summed milliseconds and the launch count since the last call. */
+int rc_set_kernel_timing(rc_ctx* ctx, int enable);
+int rc_get_kernel_times(rc_ctx* ctx, double* ms_out, uint64_t* launches_out);
 int rc_abi_version(void);
 
 /* ---------------------------------------------------------------------------

@@ -206,18 +206,20 @@ class Reference:
 
     def __init__(self, path: str = REF_LIB):
         self.lib = lib = C.CDLL(path)
-        lib.ref_pathtrace.argtypes = [_VP, _VP, _VP, _VP, _I, _F, _VP, _VP, _I, _I, _I, _VP, _VP, _VP, _VP, _I]
+        lib.ref_pathtrace.argtypes = [_VP, _VP, _VP, _VP, _I, _F, _VP, _VP, _I, _I, _I, _VP, _VP, _VP, _VP,
+                                      _I, _I, _I]
         lib.ref_photon_trace.argtypes = [_VP, _VP, _VP, _VP, _I, _F, _I, _F, _I, _I, _VP, _VP, _VP, _VP, _I]
-        lib.ref_photon_gather.argtypes = [_VP, _VP, _VP, _VP, _I, _I, _F, _I, _I, _I, _VP, _VP, _VP, _VP, _I]
+        lib.ref_photon_gather.argtypes = [_VP, _VP, _VP, _VP, _I, _I, _F, _I, _I, _I, _VP, _VP, _VP, _VP,
+                                          _I, _I, _I]
         lib.ref_p00.argtypes = [_VP, _I, _I, _I, _F, _VP, _I]
-        lib.ref_atrous_pass.argtypes = [_VP, _VP, _VP, _VP, _I, _I, _I, _F, _F, _F, _I, _F, _VP, _I]
+        lib.ref_atrous_pass.argtypes = [_VP, _VP, _VP, _VP, _I, _I, _I, _F, _F, _F, _I, _F, _VP, _I, _I, _I]
 
-    def pathtrace(self, scene, cam, settings, W, H, frame, buffers, threads=0):
+    def pathtrace(self, scene, cam, settings, W, H, frame, buffers, threads=0, rows=(0, 0)):
         acc, gb, ga, var = buffers
         self.lib.ref_pathtrace(_p(scene["tris"]), _p(scene["nodes"]), _p(scene["mats"]), _p(scene["lights"]),
                                scene["light_count"], scene["total_power"], C.byref(camera_struct(cam)),
                                C.byref(Settings(*settings)), W, H, frame, _p(acc), _p(gb), _p(ga), _p(var),
-                               threads)
+                               rows[0], rows[1], threads)
 
     def render(self, scene, cam, settings, W, H, first, nspp, buffers=None, threads=0):
         bufs = buffers if buffers is not None else alloc_images(W, H)
@@ -235,10 +237,15 @@ class Reference:
                                   _p(ph), _p(heads), _p(nxt), _p(cnt), threads)
         return ph, heads, nxt, int(cnt[0])
 
-    def photon_gather(self, scene, cam, W, H, radius, N, hash_size, frame, ph, heads, nxt, accum, threads=0):
+    def photon_gather(self, scene, cam, W, H, radius, N, hash_size, frame, ph, heads, nxt, accum, threads=0,
+                      rows=(0, 0)):
         self.lib.ref_photon_gather(_p(scene["tris"]), _p(scene["nodes"]), _p(scene["mats"]),
                                    C.byref(camera_struct(cam)), W, H, radius, N, hash_size, frame, _p(ph),
-                                   _p(heads), _p(nxt), _p(accum), threads)
+                                   _p(heads), _p(nxt), _p(accum), rows[0], rows[1], threads)
+
+    def atrous_pass(self, col, gb, ga, var, W, H, step, sc, sn, sd, N, exposure, out, rows=(0, 0), threads=0):
+        self.lib.ref_atrous_pass(_p(col), _p(gb), _p(ga), _p(var), W, H, step, sc, sn, sd, N, exposure, _p(out),
+                                 rows[0], rows[1], threads)
 
     def denoise(self, acc, gb, ga, var, W, H, total, params: AtrousParams, threads=0):
         a = np.zeros((H, W, 4), np.float32)
@@ -249,7 +256,7 @@ class Reference:
                 b = np.zeros_like(a)
                 self.lib.ref_atrous_pass(_p(a), _p(gb), _p(ga), _p(var), W, H, 1 << i, params.sigma_color,
                                          params.sigma_normal, params.sigma_depth, max(total, 1),
-                                         params.exposure, _p(b), threads)
+                                         params.exposure, _p(b), 0, 0, threads)
                 a = b
         return a
 

@@ -1,0 +1,724 @@
+// api.cu -- the device half of the C ABI declared in include/retrocam.h.
+//
+// One rc_ctx = one device, one CUDA stream, the four renderer images, the
+// uploaded scene in the kernels' layout (device_scene.h), the SPPM photon map
+// and a block of device counters.  Calls are asynchronous on the context's
+// stream unless they return data to the host.
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "device_scene.h"
+#include "retrocam.h"
+
+namespace rc {
+namespace exact {
+cudaError_t launch_render(const RenderArgs&, cudaStream_t);
+cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
+cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
+cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
+cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
+}  // namespace exact
+namespace fast {
+cudaError_t launch_render(const RenderArgs&, cudaStream_t);
+cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
+cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
+cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
+cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
+}  // namespace fast
+}  // namespace rc
+
+using namespace rc;
+
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct rc_ctx {
+    int device = 0;
+    int width = 0, height = 0;
+    int math_mode = RC_MATH_FAST;
+    cudaStream_t stream = nullptr;      // stream the work runs on
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    Images img;
+    float4* out = nullptr;    // last denoised / normalised frame
+    float4* ping = nullptr;   // à-trous ping-pong
+    float4* pong = nullptr;
+    float4* result = nullptr; // which buffer holds the last output
+    int total_samples = 0;
+    // scene
+    DeviceScene scene;
+    bool has_scene = false;
+    DevBuf nodes, tri_isect, tri_shade, mats, lights, cdf;
+    // SPPM
+    DevBuf photons, heads, next, counter;
+    int photon_cap = 0, hash_cap = 0, last_hash = 0, last_photons = 0;
+    float sppm_radius = 0.05f;
+    int sppm_iteration = 0;
+    // counters
+    DevCounters* counters = nullptr;
+    unsigned long long launches = 0, h2d = 0, d2h = 0;
+    // kernel timing with CUDA events on the launching stream
+    bool timing = false;
+    struct Timed {
+        int kind;
+        cudaEvent_t a, b;
+    };
+    std::vector<Timed> pending;
+    double ms[RC_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+    unsigned long long nlaunch[RC_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+    std::string err;
+};
+
+// Launch one kernel through `fn` (a launcher returning cudaError_t), with
+// optional event bracketing for rc_get_kernel_times.
+template <class F>
+static cudaError_t timed_launch(rc_ctx* ctx, int kind, F fn) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (ctx->timing) {
+        cudaError_t e = cudaEventCreate(&a);
+        if (e == cudaSuccess) e = cudaEventCreate(&b);
+        if (e == cudaSuccess) e = cudaEventRecord(a, ctx->stream);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = fn();
+    if (e != cudaSuccess) return e;
+    ctx->launches++;
+    if (ctx->timing) {
+        e = cudaEventRecord(b, ctx->stream);
+        if (e != cudaSuccess) return e;
+        ctx->pending.push_back({kind, a, b});
+    }
+    return cudaSuccess;
+}
+
+static cudaError_t copy_h2d(rc_ctx* ctx, void* dst, const void* src, size_t n) {
+    ctx->h2d += n;
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, ctx->stream);
+}
+
+static cudaError_t copy_d2h(rc_ctx* ctx, void* dst, const void* src, size_t n) {
+    ctx->d2h += n;
+    return cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, ctx->stream);
+}
+
+static std::mutex g_err_mutex;
+static std::string g_create_err;
+
+static int fail(rc_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (c) {
+        c->err = buf;
+    } else {
+        std::lock_guard<std::mutex> lk(g_err_mutex);
+        g_create_err = buf;
+    }
+    return code;
+}
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(ctx, e_ == cudaErrorMemoryAllocation ? RC_ERR_OUT_OF_MEMORY : RC_ERR_CUDA,  \
+                        "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);       \
+    } while (0)
+
+static cudaError_t ensure(DevBuf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.ptr) return cudaSuccess;
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+    if (bytes == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    if (e == cudaSuccess) b.bytes = bytes;
+    return e;
+}
+
+static void release(DevBuf& b) {
+    if (b.ptr) cudaFree(b.ptr);
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+static CamParams cam_params(const rc_camera* c) {
+    CamParams k;
+    for (int a = 0; a < 3; ++a) {
+        k.pos[a] = c->cam_pos[a];
+        k.right[a] = c->cam_right[a];
+        k.up[a] = c->cam_up[a];
+        k.fwd[a] = c->cam_forward[a];
+        k.lca[a] = c->lca_delta[a];
+    }
+    k.focal = c->focal_dist;
+    k.lens_radius = c->lens_radius;
+    k.tan_half = c->fov_tan_half;
+    k.sa = c->sa_strength;
+    k.blades = c->aperture_blades;
+    return k;
+}
+
+extern "C" {
+
+int rc_ctx_create(int width, int height, int device, rc_ctx** out) {
+    rc_ctx* ctx = nullptr;
+    if (!out || width < 1 || height < 1 || width > 16384 || height > 16384)
+        return fail(nullptr, RC_ERR_INVALID_ARG, "rc_ctx_create: bad size %dx%d", width, height);
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || device < 0 || device >= ndev)
+        return fail(nullptr, RC_ERR_CUDA, "rc_ctx_create: device %d unavailable (%s)", device,
+                    e == cudaSuccess ? "no such device" : cudaGetErrorString(e));
+    ctx = new rc_ctx();
+    ctx->device = device;
+    ctx->width = width;
+    ctx->height = height;
+    const size_t px = (size_t)width * height;
+    auto bail = [&](cudaError_t err, const char* what) {
+        fail(nullptr, err == cudaErrorMemoryAllocation ? RC_ERR_OUT_OF_MEMORY : RC_ERR_CUDA, "rc_ctx_create: %s: %s",
+             what, cudaGetErrorString(err));
+        rc_ctx_destroy(ctx);
+        return err == cudaErrorMemoryAllocation ? RC_ERR_OUT_OF_MEMORY : RC_ERR_CUDA;
+    };
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return bail(e, "cudaStreamCreate");
+    ctx->stream = ctx->own_stream;
+    if ((e = cudaMalloc(&ctx->img.accum, px * sizeof(float4))) != cudaSuccess) return bail(e, "accum");
+    if ((e = cudaMalloc(&ctx->img.gbuf, px * sizeof(ushort4))) != cudaSuccess) return bail(e, "gbuffer");
+    if ((e = cudaMalloc(&ctx->img.galb, px * sizeof(ushort4))) != cudaSuccess) return bail(e, "albedo");
+    if ((e = cudaMalloc(&ctx->img.var, px * sizeof(float))) != cudaSuccess) return bail(e, "variance");
+    if ((e = cudaMalloc(&ctx->out, px * sizeof(float4))) != cudaSuccess) return bail(e, "out");
+    if ((e = cudaMalloc(&ctx->ping, px * sizeof(float4))) != cudaSuccess) return bail(e, "ping");
+    if ((e = cudaMalloc(&ctx->pong, px * sizeof(float4))) != cudaSuccess) return bail(e, "pong");
+    if ((e = cudaMalloc(&ctx->counters, sizeof(DevCounters))) != cudaSuccess) return bail(e, "counters");
+    ctx->img.width = width;
+    ctx->img.height = height;
+    ctx->result = ctx->out;
+    if ((e = cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), ctx->stream)) != cudaSuccess)
+        return bail(e, "memset counters");
+    int rcode = rc_reset(ctx);
+    if (rcode != RC_OK) {
+        fail(nullptr, rcode, "rc_ctx_create: reset failed: %s", ctx->err.c_str());
+        rc_ctx_destroy(ctx);
+        return rcode;
+    }
+    *out = ctx;
+    return RC_OK;
+}
+
+int rc_ctx_destroy(rc_ctx* ctx) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& t : ctx->pending) {
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    for (void* p : {(void*)ctx->img.accum, (void*)ctx->img.gbuf, (void*)ctx->img.galb, (void*)ctx->img.var,
+                    (void*)ctx->out, (void*)ctx->ping, (void*)ctx->pong, (void*)ctx->counters})
+        if (p) cudaFree(p);
+    for (DevBuf* b : {&ctx->nodes, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
+                      &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter})
+        release(*b);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return RC_OK;
+}
+
+int rc_last_error(const rc_ctx* ctx, char* buf, size_t n) {
+    if (!buf || n == 0) return RC_ERR_INVALID_ARG;
+    std::string s;
+    if (ctx) {
+        s = ctx->err;
+    } else {
+        std::lock_guard<std::mutex> lk(g_err_mutex);
+        s = g_create_err;
+    }
+    const size_t k = s.size() < n - 1 ? s.size() : n - 1;
+    memcpy(buf, s.data(), k);
+    buf[k] = '\0';
+    return RC_OK;
+}
+
+int rc_set_math_mode(rc_ctx* ctx, int mode) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (mode != RC_MATH_FAST && mode != RC_MATH_EXACT) return fail(ctx, RC_ERR_INVALID_ARG, "bad math mode %d", mode);
+    ctx->math_mode = mode;
+    return RC_OK;
+}
+
+int rc_synchronize(rc_ctx* ctx) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned int word = 0;
+    CK(cudaMemcpy(&word, &ctx->counters->error_word, sizeof(word), cudaMemcpyDeviceToHost));
+    if (word) return fail(ctx, RC_ERR_DEVICE_GUARD, "kernel guard raised (error word 0x%x)", word);
+    return RC_OK;
+}
+
+int rc_ctx_set_stream(rc_ctx* ctx, void* cuda_stream) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+    return RC_OK;
+}
+
+int rc_set_kernel_timing(rc_ctx* ctx, int enable) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    ctx->timing = enable != 0;
+    return RC_OK;
+}
+
+int rc_get_kernel_times(rc_ctx* ctx, double* ms_out, uint64_t* launches_out) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (auto& t : ctx->pending) {
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, t.a, t.b));
+        ctx->ms[t.kind] += ms;
+        ctx->nlaunch[t.kind]++;
+        cudaEventDestroy(t.a);
+        cudaEventDestroy(t.b);
+    }
+    ctx->pending.clear();
+    for (int k = 0; k < RC_KERNEL_KINDS; ++k) {
+        if (ms_out) ms_out[k] = ctx->ms[k];
+        if (launches_out) launches_out[k] = ctx->nlaunch[k];
+        ctx->ms[k] = 0.0;
+        ctx->nlaunch[k] = 0;
+    }
+    return RC_OK;
+}
+
+int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const rc_bvh_node* nodes,
+                    int node_count, const rc_material* mats, int material_count, const rc_light* lights,
+                    int light_count, float total_light_power) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (tri_count < 0 || node_count < 1 || material_count < 1 || light_count < 0 || !nodes || !mats ||
+        (tri_count > 0 && !tris) || (light_count > 0 && !lights))
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_scene_upload: bad arguments");
+    // ---- validate: a tree rooted at node 0 over [0, tri_count) ----
+    std::vector<int> seen(node_count, 0), depth(node_count, 0);
+    std::vector<int> todo;
+    todo.push_back(0);
+    seen[0] = 1;
+    int max_depth = 0;
+    while (!todo.empty()) {
+        const int i = todo.back();
+        todo.pop_back();
+        const rc_bvh_node& n = nodes[i];
+        if (n.prim_count > 0) {
+            if (n.prim_start < 0 || (long)n.prim_start + n.prim_count > tri_count)
+                return fail(ctx, RC_ERR_BAD_SCENE, "node %d: primitives [%d,+%d) outside %d triangles", i,
+                            n.prim_start, n.prim_count, tri_count);
+            if (depth[i] > max_depth) max_depth = depth[i];
+            continue;
+        }
+        if (tri_count == 0 && i == 0) break;
+        for (int ch : {n.left_child, n.right_child}) {
+            if (ch < 0 || ch >= node_count)
+                return fail(ctx, RC_ERR_BAD_SCENE, "node %d: child index %d out of range [0,%d)", i, ch, node_count);
+            if (seen[ch]) return fail(ctx, RC_ERR_BAD_SCENE, "node %d: child %d referenced twice", i, ch);
+            seen[ch] = 1;
+            depth[ch] = depth[i] + 1;
+            todo.push_back(ch);
+        }
+    }
+    for (int i = 0; i < tri_count; ++i)
+        if (tris[i].mat_index < 0 || tris[i].mat_index >= material_count)
+            return fail(ctx, RC_ERR_BAD_SCENE, "triangle %d: material %d out of range", i, tris[i].mat_index);
+    // ---- convert to the kernels' layout ----
+    std::vector<NodeRec> recs(node_count);
+    memset(recs.data(), 0, recs.size() * sizeof(NodeRec));
+    for (int i = 0; i < node_count; ++i) {
+        const rc_bvh_node& n = nodes[i];
+        if (n.prim_count > 0 || !seen[i] || (tri_count == 0)) continue;
+        const rc_bvh_node& L = nodes[n.left_child];
+        const rc_bvh_node& R = nodes[n.right_child];
+        NodeRec& r = recs[i];
+        r.a = make_float4(L.aabb_min[0], L.aabb_min[1], L.aabb_min[2], L.aabb_max[0]);
+        r.b = make_float4(L.aabb_max[1], L.aabb_max[2], R.aabb_min[0], R.aabb_min[1]);
+        r.c = make_float4(R.aabb_min[2], R.aabb_max[0], R.aabb_max[1], R.aabb_max[2]);
+        r.d = make_int4(L.prim_count > 0 ? L.prim_start : n.left_child, L.prim_count,
+                        R.prim_count > 0 ? R.prim_start : n.right_child, R.prim_count);
+    }
+    std::vector<float4> isect(3 * (size_t)tri_count), shade(3 * (size_t)tri_count);
+    for (int i = 0; i < tri_count; ++i) {
+        const rc_triangle& t = tris[i];
+        // e1, e2 with the same float subtraction the reference does per test
+        isect[3 * i + 0] = make_float4(t.v0[0], t.v0[1], t.v0[2], 0.0f);
+        isect[3 * i + 1] = make_float4(t.v1[0] - t.v0[0], t.v1[1] - t.v0[1], t.v1[2] - t.v0[2], 0.0f);
+        isect[3 * i + 2] = make_float4(t.v2[0] - t.v0[0], t.v2[1] - t.v0[1], t.v2[2] - t.v0[2], 0.0f);
+        float mbits;
+        memcpy(&mbits, &t.mat_index, 4);
+        shade[3 * i + 0] = make_float4(t.n0[0], t.n0[1], t.n0[2], mbits);
+        shade[3 * i + 1] = make_float4(t.n1[0], t.n1[1], t.n1[2], 0.0f);
+        shade[3 * i + 2] = make_float4(t.n2[0], t.n2[1], t.n2[2], 0.0f);
+    }
+    std::vector<float> cdf(light_count > 0 ? light_count : 1, 1.0f);
+    for (int i = 0; i < light_count; ++i) cdf[i] = lights[i].cdf_weight;
+    rc_light stub;
+    memset(&stub, 0, sizeof(stub));
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->stream));  // buffers may be in use by queued work
+    CK(ensure(ctx->nodes, recs.size() * sizeof(NodeRec)));
+    CK(ensure(ctx->tri_isect, std::max<size_t>(16, isect.size() * sizeof(float4))));
+    CK(ensure(ctx->tri_shade, std::max<size_t>(16, shade.size() * sizeof(float4))));
+    CK(ensure(ctx->mats, (size_t)material_count * sizeof(rc_material)));
+    CK(ensure(ctx->lights, (size_t)(light_count > 0 ? light_count : 1) * sizeof(rc_light)));
+    CK(ensure(ctx->cdf, cdf.size() * sizeof(float)));
+    CK(copy_h2d(ctx, ctx->nodes.ptr, recs.data(), recs.size() * sizeof(NodeRec)));
+    if (tri_count > 0) {
+        CK(copy_h2d(ctx, ctx->tri_isect.ptr, isect.data(), isect.size() * sizeof(float4)));
+        CK(copy_h2d(ctx, ctx->tri_shade.ptr, shade.data(), shade.size() * sizeof(float4)));
+    }
+    CK(copy_h2d(ctx, ctx->mats.ptr, mats, (size_t)material_count * sizeof(rc_material)));
+    CK(copy_h2d(ctx, ctx->lights.ptr, light_count > 0 ? (const void*)lights : (const void*)&stub,
+                (size_t)(light_count > 0 ? light_count : 1) * sizeof(rc_light)));
+    CK(copy_h2d(ctx, ctx->cdf.ptr, cdf.data(), cdf.size() * sizeof(float)));
+    CK(cudaStreamSynchronize(ctx->stream));  // host staging vectors go out of scope
+    DeviceScene& S = ctx->scene;
+    S.nodes = (const NodeRec*)ctx->nodes.ptr;
+    S.tri_isect = (const float4*)ctx->tri_isect.ptr;
+    S.tri_shade = (const float4*)ctx->tri_shade.ptr;
+    S.materials = (const float4*)ctx->mats.ptr;
+    S.lights = (const float4*)ctx->lights.ptr;
+    S.light_cdf = (const float*)ctx->cdf.ptr;
+    S.node_count = node_count;
+    S.tri_count = tri_count;
+    S.material_count = material_count;
+    S.light_count = light_count;
+    S.total_light_power = total_light_power;
+    for (int a = 0; a < 3; ++a) {
+        S.root_min[a] = nodes[0].aabb_min[a];
+        S.root_max[a] = nodes[0].aabb_max[a];
+    }
+    if (tri_count == 0) {
+        // no geometry: an inverted root box that no ray can enter
+        for (int a = 0; a < 3; ++a) {
+            S.root_min[a] = 1e30f;
+            S.root_max[a] = -1e30f;
+        }
+    }
+    S.root_ref = nodes[0].prim_count > 0 ? nodes[0].prim_start : 0;
+    S.root_count = nodes[0].prim_count;
+    S.depth = max_depth;
+    ctx->has_scene = true;
+    return RC_OK;
+}
+
+static int launch_err(rc_ctx* ctx, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return RC_OK;
+    return fail(ctx, RC_ERR_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
+}
+
+int rc_render(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, int first_frame, int n_spp) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!cam || !settings || first_frame < 0 || n_spp < 0)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_render: bad arguments");
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_render: no scene uploaded");
+    if (n_spp == 0) return RC_OK;
+    CK(cudaSetDevice(ctx->device));
+    RenderArgs A;
+    A.scene = ctx->scene;
+    A.img = ctx->img;
+    A.cam = cam_params(cam);
+    A.nee_enabled = settings->nee_enabled;
+    A.firefly_clamp = settings->nee_firefly_clamp;
+    A.first_frame = first_frame;
+    A.n_spp = n_spp;
+    A.counters = ctx->counters;
+    const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    const cudaError_t e = timed_launch(ctx, RC_KERNEL_RENDER, [&] {
+        return ex ? exact::launch_render(A, ctx->stream) : fast::launch_render(A, ctx->stream);
+    });
+    if (e != cudaSuccess) return launch_err(ctx, e, "render");
+    // Renderer.getTotalSamples(): frames 0 .. first_frame + n_spp - 1 done
+    ctx->total_samples = first_frame + n_spp;
+    return RC_OK;
+}
+
+int rc_reset(rc_ctx* ctx) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    const size_t px = (size_t)ctx->width * ctx->height;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(ctx->img.accum, 0, px * sizeof(float4), ctx->stream));
+    CK(cudaMemsetAsync(ctx->img.gbuf, 0, px * sizeof(ushort4), ctx->stream));
+    CK(cudaMemsetAsync(ctx->img.galb, 0, px * sizeof(ushort4), ctx->stream));
+    CK(cudaMemsetAsync(ctx->img.var, 0, px * sizeof(float), ctx->stream));
+    ctx->total_samples = 0;
+    return RC_OK;
+}
+
+int rc_total_samples(const rc_ctx* ctx) { return ctx ? ctx->total_samples : RC_ERR_INVALID_ARG; }
+
+int rc_sppm_reset(rc_ctx* ctx, float initial_radius) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!(initial_radius > 0.0f)) return fail(ctx, RC_ERR_INVALID_ARG, "rc_sppm_reset: radius must be > 0");
+    ctx->sppm_radius = initial_radius;
+    ctx->sppm_iteration = 0;
+    return RC_OK;
+}
+
+int rc_sppm_update_radius(rc_ctx* ctx, float alpha) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    ctx->sppm_radius = rc_sppm_next_radius(ctx->sppm_radius, ctx->sppm_iteration, alpha);
+    ctx->sppm_iteration++;
+    return RC_OK;
+}
+
+int rc_sppm_state(const rc_ctx* ctx, float* radius, int* iteration) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (radius) *radius = ctx->sppm_radius;
+    if (iteration) *iteration = ctx->sppm_iteration;
+    return RC_OK;
+}
+
+static int check_sppm(rc_ctx* ctx, const rc_sppm_params* p) {
+    if (!p || p->photon_count < 0 || p->hash_size < 1 || (p->hash_size & (p->hash_size - 1)) != 0)
+        return fail(ctx, RC_ERR_INVALID_ARG, "sppm: photon_count must be >= 0 and hash_size a power of two");
+    return RC_OK;
+}
+
+int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    int r = check_sppm(ctx, p);
+    if (r != RC_OK) return r;
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_sppm_trace: no scene uploaded");
+    CK(cudaSetDevice(ctx->device));
+    const int cap = p->photon_count > 0 ? p->photon_count : 1;
+    if (cap > ctx->photon_cap || p->hash_size > ctx->hash_cap) CK(cudaStreamSynchronize(ctx->stream));
+    if (cap > ctx->photon_cap) {
+        CK(ensure(ctx->photons, (size_t)cap * 3 * sizeof(float4)));
+        CK(ensure(ctx->next, (size_t)cap * sizeof(int)));
+        ctx->photon_cap = cap;
+    }
+    if (p->hash_size > ctx->hash_cap) {
+        CK(ensure(ctx->heads, (size_t)p->hash_size * sizeof(int)));
+        ctx->hash_cap = p->hash_size;
+    }
+    CK(ensure(ctx->counter, sizeof(unsigned int)));
+    // PhotonMap.clear(): heads = -1, counter = 0
+    CK(cudaMemsetAsync(ctx->heads.ptr, 0xff, (size_t)p->hash_size * sizeof(int), ctx->stream));
+    CK(cudaMemsetAsync(ctx->counter.ptr, 0, sizeof(unsigned int), ctx->stream));
+    ctx->last_hash = p->hash_size;
+    ctx->last_photons = p->photon_count;
+    if (p->photon_count == 0 || ctx->scene.light_count == 0) return RC_OK;
+    PhotonArgs A;
+    A.scene = ctx->scene;
+    A.photons = (float4*)ctx->photons.ptr;
+    A.heads = (int*)ctx->heads.ptr;
+    A.next = (int*)ctx->next.ptr;
+    A.counter = (unsigned int*)ctx->counter.ptr;
+    A.photon_count = p->photon_count;
+    A.hash_size = p->hash_size;
+    A.radius = ctx->sppm_radius;
+    A.seed = ctx->sppm_iteration * 7919 + 6271;
+    A.counters = ctx->counters;
+    const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    const cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_TRACE, [&] {
+        return ex ? exact::launch_photon_trace(A, ctx->stream) : fast::launch_photon_trace(A, ctx->stream);
+    });
+    return launch_err(ctx, e, "photon trace");
+}
+
+int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, float weight) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    int r = check_sppm(ctx, p);
+    if (r != RC_OK) return r;
+    if (!cam) return fail(ctx, RC_ERR_INVALID_ARG, "rc_sppm_gather: null camera");
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_sppm_gather: no scene uploaded");
+    if (!ctx->heads.ptr || p->hash_size != ctx->last_hash)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_sppm_gather: no photon map traced with hash_size %d", p->hash_size);
+    CK(cudaSetDevice(ctx->device));
+    GatherArgs A;
+    A.scene = ctx->scene;
+    A.img = ctx->img;
+    A.cam = cam_params(cam);
+    A.photons = (const float4*)ctx->photons.ptr;
+    A.heads = (const int*)ctx->heads.ptr;
+    A.next = (const int*)ctx->next.ptr;
+    A.hash_size = p->hash_size;
+    A.radius = ctx->sppm_radius;
+    A.weight = weight;
+    A.counters = ctx->counters;
+    const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    const cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_GATHER, [&] {
+        return ex ? exact::launch_photon_gather(A, ctx->stream) : fast::launch_photon_gather(A, ctx->stream);
+    });
+    return launch_err(ctx, e, "photon gather");
+}
+
+int rc_denoise_atrous(rc_ctx* ctx, const rc_atrous_params* p, float* out_rgba) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!p) return fail(ctx, RC_ERR_INVALID_ARG, "rc_denoise_atrous: null params");
+    CK(cudaSetDevice(ctx->device));
+    const int N = ctx->total_samples;
+    const int W = ctx->width, H = ctx->height;
+    const bool over = p->max_spp > 0 && N > p->max_spp;
+    const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    if (p->enabled && !over) {
+        const int passes = p->iterations < 1 ? 1 : (p->iterations > 5 ? 5 : p->iterations);
+        const float4* src = ctx->img.accum;
+        float4* bufs[2] = {ctx->ping, ctx->pong};
+        for (int i = 0; i < passes; ++i) {
+            float4* dst = (i == passes - 1) ? ctx->out : bufs[i & 1];
+            AtrousArgs A;
+            A.color = src;
+            A.gbuf = ctx->img.gbuf;
+            A.galb = ctx->img.galb;
+            A.var = ctx->img.var;
+            A.out = dst;
+            A.width = W;
+            A.height = H;
+            A.step = 1 << i;
+            A.sigma_color = p->sigma_color;
+            A.sigma_normal = p->sigma_normal;
+            A.sigma_depth = p->sigma_depth;
+            A.sample_count = N > 1 ? N : 1;
+            A.exposure = p->exposure;
+            A.normalize = (i == 0) ? 1 : 0;
+            A.inv_n_unused = 0.0f;
+            const cudaError_t e = timed_launch(ctx, RC_KERNEL_ATROUS, [&] {
+                return ex ? exact::launch_atrous(A, ctx->stream) : fast::launch_atrous(A, ctx->stream);
+            });
+            if (e != cudaSuccess) return launch_err(ctx, e, "atrous");
+            src = dst;
+        }
+    } else {
+        NormalizeArgs A;
+        A.accum = ctx->img.accum;
+        A.out = ctx->out;
+        A.count = W * H;
+        A.total_samples = N;
+        A.exposure = p->exposure;
+        const cudaError_t e = timed_launch(ctx, RC_KERNEL_NORMALIZE, [&] {
+            return ex ? exact::launch_normalize(A, ctx->stream) : fast::launch_normalize(A, ctx->stream);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "normalize");
+    }
+    ctx->result = ctx->out;
+    if (out_rgba) return rc_read_output(ctx, out_rgba);
+    return RC_OK;
+}
+
+int rc_render_frame(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, int spp,
+                    const rc_sppm_params* sppm, float sppm_initial_radius, int sppm_iterations,
+                    const rc_atrous_params* atrous, float* out_rgba) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!cam || !settings || !atrous || spp < 1 || sppm_iterations < 0 || sppm_iterations > spp ||
+        (sppm_iterations > 0 && !sppm))
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_render_frame: bad arguments");
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_render_frame: no scene uploaded");
+    int r = rc_reset(ctx);
+    if (r != RC_OK) return r;
+    const bool use_sppm = sppm_iterations > 0 && ctx->scene.light_count > 0;
+    if (use_sppm) {
+        if ((r = rc_sppm_reset(ctx, sppm_initial_radius)) != RC_OK) return r;
+        for (int k = 0; k < sppm_iterations; ++k) {
+            const int s0 = (int)((long)k * spp / sppm_iterations);
+            const int s1 = (int)((long)(k + 1) * spp / sppm_iterations);
+            if ((r = rc_sppm_trace(ctx, sppm)) != RC_OK) return r;
+            if ((r = rc_render(ctx, cam, settings, s0, s1 - s0)) != RC_OK) return r;
+            if ((r = rc_sppm_gather(ctx, cam, sppm, (float)(s1 - s0))) != RC_OK) return r;
+            if ((r = rc_sppm_update_radius(ctx, sppm->alpha)) != RC_OK) return r;
+        }
+    } else {
+        if ((r = rc_render(ctx, cam, settings, 0, spp)) != RC_OK) return r;
+    }
+    return rc_denoise_atrous(ctx, atrous, out_rgba);
+}
+
+int rc_read_buffers(rc_ctx* ctx, float* accum, uint16_t* gbuf, uint16_t* galb, float* var) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    const size_t px = (size_t)ctx->width * ctx->height;
+    CK(cudaSetDevice(ctx->device));
+    if (accum) CK(copy_d2h(ctx, accum, ctx->img.accum, px * sizeof(float4)));
+    if (gbuf) CK(copy_d2h(ctx, gbuf, ctx->img.gbuf, px * sizeof(ushort4)));
+    if (galb) CK(copy_d2h(ctx, galb, ctx->img.galb, px * sizeof(ushort4)));
+    if (var) CK(copy_d2h(ctx, var, ctx->img.var, px * sizeof(float)));
+    return rc_synchronize(ctx);
+}
+
+int rc_read_output(rc_ctx* ctx, float* out_rgba) {
+    if (!ctx || !out_rgba) return RC_ERR_INVALID_ARG;
+    const size_t px = (size_t)ctx->width * ctx->height;
+    CK(cudaSetDevice(ctx->device));
+    CK(copy_d2h(ctx, out_rgba, ctx->result, px * sizeof(float4)));
+    return rc_synchronize(ctx);
+}
+
+int rc_read_photon_map(rc_ctx* ctx, rc_photon* photons, int photon_capacity, int32_t* heads, int hash_size,
+                       int32_t* next, uint32_t* counter) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!ctx->heads.ptr) return fail(ctx, RC_ERR_INVALID_ARG, "rc_read_photon_map: no photon map");
+    if (heads && hash_size != ctx->last_hash)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_read_photon_map: hash_size %d != traced %d", hash_size,
+                    ctx->last_hash);
+    const int n = photon_capacity < ctx->photon_cap ? photon_capacity : ctx->photon_cap;
+    CK(cudaSetDevice(ctx->device));
+    if (photons && n > 0)
+        CK(cudaMemcpyAsync(photons, ctx->photons.ptr, (size_t)n * sizeof(rc_photon), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    if (heads)
+        CK(cudaMemcpyAsync(heads, ctx->heads.ptr, (size_t)hash_size * sizeof(int), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    if (next && n > 0)
+        CK(cudaMemcpyAsync(next, ctx->next.ptr, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if (counter) CK(cudaMemcpyAsync(counter, ctx->counter.ptr, sizeof(unsigned int), cudaMemcpyDeviceToHost, ctx->stream));
+    return rc_synchronize(ctx);
+}
+
+int rc_get_counters(rc_ctx* ctx, rc_counters* out) {
+    if (!ctx || !out) return RC_ERR_INVALID_ARG;
+    DevCounters d;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(&d, ctx->counters, sizeof(d), cudaMemcpyDeviceToHost, ctx->stream));
+    unsigned int stored = 0;
+    if (ctx->counter.ptr)
+        CK(cudaMemcpyAsync(&stored, ctx->counter.ptr, sizeof(stored), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    out->camera_paths = d.camera_paths;
+    out->closest_rays = d.closest_rays;
+    out->shadow_rays = d.shadow_rays;
+    out->photon_rays = d.photon_rays;
+    out->gather_rays = d.gather_rays;
+    out->photons_stored = stored < (unsigned)ctx->last_photons ? stored : (unsigned)ctx->last_photons;
+    out->node_tests = d.node_tests;
+    out->tri_tests = d.tri_tests;
+    out->surface_hits = d.surface_hits;
+    out->light_samples = d.light_samples;
+    out->photon_node_tests = d.photon_node_tests;
+    out->photon_tri_tests = d.photon_tri_tests;
+    out->kernel_launches = ctx->launches;
+    out->h2d_bytes = ctx->h2d;
+    out->d2h_bytes = ctx->d2h;
+    out->error_word = d.error_word;
+    out->reserved = 0;
+    return RC_OK;
+}
+
+int rc_reset_counters(rc_ctx* ctx) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), ctx->stream));
+    ctx->launches = ctx->h2d = ctx->d2h = 0;
+    return RC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,154 @@
+// device_scene.h -- device-side layout of a scene and of the per-context
+// images, shared by the C-ABI layer (api.cu) and the kernels.
+//
+// HBM layout (all arrays 16-byte aligned, read with 128-bit loads):
+//   node records   64 B per BVH node: the AABBs of BOTH children plus their
+//                  (ref, count) pairs, so an interior visit is one 64-byte
+//                  line and the child tests need no further loads.
+//                    a = (L.min.x, L.min.y, L.min.z, L.max.x)
+//                    b = (L.max.y, L.max.z, R.min.x, R.min.y)
+//                    c = (R.min.z, R.max.x, R.max.y, R.max.z)
+//                    d = (L.ref, L.count, R.ref, R.count)
+//                  ref is a node index when count == 0, else prim_start.
+//                  Records of leaf nodes are never read.
+//   tri_isect      48 B per triangle: v0, e1 = v1 - v0, e2 = v2 - v0 (the
+//                  differences the reference computes per test, computed once
+//                  on the host with the same float subtraction).
+//   tri_shade      48 B per triangle: n0 (+ material index bits in .w), n1, n2;
+//                  read only for the accepted closest hit.
+//   materials      64 B per material (the std430 record).
+//   lights         80 B per light (the std430 record) + a separate float CDF
+//                  array so the linear CDF scan touches 4 B per light.
+// Triangles and nodes keep the reference's BVH order, so indices match the
+// reference buffers one to one.
+#ifndef RC_DEVICE_SCENE_H
+#define RC_DEVICE_SCENE_H
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rc {
+
+struct NodeRec {
+    float4 a, b, c;
+    int4 d;
+};
+
+struct DeviceScene {
+    const NodeRec* nodes = nullptr;
+    const float4* tri_isect = nullptr;   // 3 per triangle
+    const float4* tri_shade = nullptr;   // 3 per triangle
+    const float4* materials = nullptr;   // 4 per material
+    const float4* lights = nullptr;      // 5 per light
+    const float* light_cdf = nullptr;
+    int node_count = 0;
+    int tri_count = 0;
+    int material_count = 0;
+    int light_count = 0;
+    float total_light_power = 0.0f;
+    // root node as the reference stores it
+    float root_min[3] = {0, 0, 0};
+    float root_max[3] = {0, 0, 0};
+    int root_ref = 0;     // prim_start when the root is a leaf, else 0
+    int root_count = 0;   // > 0 when the root is a leaf
+    int depth = 0;        // max leaf depth (root = 0)
+};
+
+// Per-context images (core/Renderer.java:152-193).
+struct Images {
+    float4* accum = nullptr;      // RGBA32F running sum, alpha = samples
+    ushort4* gbuf = nullptr;      // RGBA16F (facing normal, hit t)
+    ushort4* galb = nullptr;      // RGBA16F first-hit albedo
+    float* var = nullptr;         // R32F sum of luma^2
+    int width = 0, height = 0;
+};
+
+// Camera uniforms of pathtrace.comp:11-24.
+struct CamParams {
+    float pos[3], right[3], up[3], fwd[3];
+    float focal, lens_radius, tan_half, sa;
+    int blades;
+    float lca[3];
+};
+
+// Device counters; one block of these per context.
+struct DevCounters {
+    unsigned long long camera_paths;
+    unsigned long long closest_rays;
+    unsigned long long shadow_rays;
+    unsigned long long photon_rays;
+    unsigned long long gather_rays;
+    unsigned long long photons_stored;
+    unsigned long long node_tests;
+    unsigned long long tri_tests;
+    unsigned long long surface_hits;
+    unsigned long long light_samples;
+    unsigned long long photon_node_tests;   // photon trace + gather traversals
+    unsigned long long photon_tri_tests;
+    unsigned int error_word;
+    unsigned int pad;
+};
+
+struct RenderArgs {
+    DeviceScene scene;
+    Images img;
+    CamParams cam;
+    int nee_enabled;
+    float firefly_clamp;
+    int first_frame;
+    int n_spp;
+    DevCounters* counters;
+};
+
+struct PhotonArgs {
+    DeviceScene scene;
+    float4* photons;        // 3 float4 per photon (std430 record)
+    int* heads;
+    int* next;
+    unsigned int* counter;
+    int photon_count;
+    int hash_size;
+    float radius;
+    int seed;
+    DevCounters* counters;
+};
+
+struct GatherArgs {
+    DeviceScene scene;
+    Images img;
+    CamParams cam;
+    const float4* photons;
+    const int* heads;
+    const int* next;
+    int hash_size;
+    float radius;
+    float weight;
+    DevCounters* counters;
+};
+
+struct AtrousArgs {
+    const float4* color;      // RGBA32F input (or accum when normalize != 0)
+    const ushort4* gbuf;
+    const ushort4* galb;
+    const float* var;
+    float4* out;
+    int width, height;
+    int step;
+    float sigma_color, sigma_normal, sigma_depth;
+    int sample_count;         // max(N, 1)
+    float exposure;
+    int normalize;            // 1: color is the raw accumulation (p00 fused)
+    float inv_n_unused;
+};
+
+struct NormalizeArgs {
+    const float4* accum;
+    float4* out;
+    int count;
+    int total_samples;
+    float exposure;
+};
+
+}  // namespace rc
+
+#endif

@@ -1,0 +1,307 @@
+"""Parity of the CUDA path tracer, photon passes and denoiser with the CPU
+oracle, through the C ABI.
+
+Exact math mode (RC_MATH_EXACT) must be bit-identical to the oracle for
+every deterministic output (accumulation, variance, G-buffer, albedo,
+photon records and cells, à-trous).  The gather sums photons in hash-chain
+order, which the GPU's atomic insertion leaves unordered, so it is compared
+within 2e-5 relative.  Fast mode is compared by tolerance (see each test).
+"""
+import numpy as np
+import pytest
+
+from conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(product, orc, workload):
+    import pyoracle as po
+    from retrocam_b200 import scenes
+    w = workload()
+    sc = scenes.build_scene(w.scene, orc, po.MAT)
+    cam = scenes.camera(w.orbit, w.lens, orc)
+    return w, sc, cam
+
+
+def _ctx(product, W, H, mode):
+    return product.Context(W, H, 0, mode)
+
+
+@pytest.fixture(scope="module")
+def c0(product, orc, cuda_ok):
+    from retrocam_b200 import scenes
+    return _scene(product, orc, scenes.cornell_small)
+
+
+@pytest.fixture(scope="module")
+def c1(product, orc, cuda_ok):
+    from retrocam_b200 import scenes
+    return _scene(product, orc, scenes.export_frame)
+
+
+def _same_images(gpu, cpu):
+    names = ("accum", "gbuffer", "albedo", "variance")
+    for n, g, c in zip(names, gpu, cpu):
+        if not np.array_equal(bits(g), bits(c)):
+            bad = np.argwhere(bits(g) != bits(c))
+            raise AssertionError(f"{n}: {len(bad)} words differ, first at {bad[:3].tolist()}")
+
+
+@pytest.mark.parametrize("size,spp,lca", [((64, 64), 1, False), ((256, 256), 1, False), ((256, 256), 4, True),
+                                          ((97, 61), 3, False)])
+def test_render_exact_bit_identical_cornell(product, orc, c0, size, spp, lca):
+    w, sc, cam = c0
+    cam = dict(cam)
+    if lca:
+        cam["lca_delta"] = (-0.009, 0.0, 0.009)
+    W, H = size
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, spp)
+        gpu = ctx.read_buffers()
+    cpu, _ = orc.render(sc, cam, (1, 1.0), W, H, 0, spp)
+    _same_images(gpu, cpu)
+
+
+def test_render_exact_bit_identical_export_scene(product, orc, c1):
+    w, sc, cam = c1
+    W, H = 160, 90
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, 3)
+        gpu = ctx.read_buffers()
+        cnt = ctx.counters()
+    cpu, st = orc.render(sc, cam, (1, 1.0), W, H, 0, 3)
+    _same_images(gpu, cpu)
+    # the device counters count the same traversals as the oracle
+    assert cnt["camera_paths"] == st[0]
+    assert cnt["closest_rays"] == st[1]
+    assert cnt["shadow_rays"] == st[2]
+    assert cnt["error_word"] == 0
+
+
+def test_render_split_launches_equal_one_launch(product, c1):
+    """n_spp frames in one launch == one launch per frame (same additions)."""
+    w, sc, cam = c1
+    W, H = 64, 48
+    out = []
+    for split in (False, True):
+        with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+            ctx.upload(sc)
+            if split:
+                for f in range(5):
+                    ctx.render(cam, (1, 1.0), f, 1)
+            else:
+                ctx.render(cam, (1, 1.0), 0, 5)
+            out.append(ctx.read_buffers())
+            assert ctx.total_samples == 5
+    _same_images(out[0], out[1])
+
+
+def test_render_nee_off_and_clamp(product, orc, c1):
+    w, sc, cam = c1
+    W, H = 48, 32
+    for settings in ((0, 1.0), (1, 20.0)):
+        with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+            ctx.upload(sc)
+            ctx.render(cam, settings, 0, 2)
+            gpu = ctx.read_buffers()
+        cpu, _ = orc.render(sc, cam, settings, W, H, 0, 2)
+        _same_images(gpu, cpu)
+
+
+def test_render_fast_close_to_oracle(product, orc, c1):
+    """Fast math reorders rounding, so a few paths take another branch; the
+    per-pixel check is statistical and the image mean must agree."""
+    w, sc, cam = c1
+    W, H, spp = 160, 90, 4
+    with _ctx(product, W, H, product.RC_MATH_FAST) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, spp)
+        acc, gb, ga, var = ctx.read_buffers()
+    (cacc, cgb, cga, cvar), _ = orc.render(sc, cam, (1, 1.0), W, H, 0, spp)
+    rel = np.abs(acc[..., :3] - cacc[..., :3]) / np.maximum(np.abs(cacc[..., :3]), 1e-3)
+    frac_close = np.mean(np.all(rel <= 1e-4, axis=-1))
+    assert frac_close >= 0.97, frac_close
+    m_gpu, m_cpu = acc[..., :3].mean(), cacc[..., :3].mean()
+    assert abs(m_gpu - m_cpu) / m_cpu < 0.01
+    np.testing.assert_array_equal(acc[..., 3], cacc[..., 3])
+    # G-buffer: same surfaces; values within half precision of the oracle's
+    g, c = gb.view(np.float16).astype(np.float32), cgb.view(np.float16).astype(np.float32)
+    assert np.mean(np.all(np.abs(g - c) <= 2e-3 * np.maximum(np.abs(c), 1.0), axis=-1)) >= 0.99
+
+
+def _photon_records(ph, n):
+    r = ph[:n].view(np.float32).reshape(n, 12)
+    u = r.view(np.uint32)
+    return r[np.lexsort(u.T[::-1])]
+
+
+def test_photon_map_exact(product, orc, c1):
+    w, sc, cam = c1
+    N, r0, hs = 300_000, 0.02, 1 << 20
+    with _ctx(product, 64, 64, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.sppm_reset(r0)
+        ctx.sppm_trace(N, hs)
+        ph, heads, nxt, cnt = ctx.read_photon_map(N, hs)
+        counters = ctx.counters()
+    cph, cheads, cnxt, ccnt, st = orc.photon_trace(sc, N, r0, 0 * 7919 + 6271, hs)
+    assert cnt == ccnt > 1000
+    assert counters["photon_rays"] == st[3]
+    # same set of photon records (insertion order differs: GPU atomics)
+    g = _photon_records(ph, cnt)
+    c = _photon_records(cph, ccnt)
+    np.testing.assert_array_equal(g.view(np.uint32), c.view(np.uint32))
+    # chains: every photon sits in exactly one chain, the one of its own cell
+    pos = ph[:cnt]["position"]
+    cells = np.floor(pos / np.float32(r0)).astype(np.int64)
+    h = ((cells[:, 0] * 73856093) ^ (cells[:, 1] * 19349663) ^ (cells[:, 2] * 83492791)) & (hs - 1)
+    seen = np.zeros(cnt, bool)
+    for cell in np.unique(h):
+        i = heads[cell]
+        while i >= 0:
+            assert not seen[i]
+            seen[i] = True
+            assert h[i] == cell
+            i = nxt[i]
+    assert seen.all()
+    # heads hold -1 exactly where the oracle's do
+    np.testing.assert_array_equal(heads < 0, cheads < 0)
+
+
+def _max_chain(ph, n, r, hs):
+    cells = np.floor(ph[:n]["position"] / np.float32(r)).astype(np.int64)
+    h = ((cells[:, 0] * 73856093) ^ (cells[:, 1] * 19349663) ^ (cells[:, 2] * 83492791)) & (hs - 1)
+    return np.bincount(h).max()
+
+
+def _gather_pair(product, orc, sc, cam, W, H, N, r0, hs):
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, 1)
+        before = ctx.read_buffers()[0]
+        ctx.sppm_reset(r0)
+        ctx.sppm_trace(N, hs)
+        ctx.sppm_gather(cam, N, hs, 1.0)
+        after = ctx.read_buffers()[0]
+    cph, cheads, cnxt, ccnt, _ = orc.photon_trace(sc, N, r0, 6271, hs)
+    cacc = before.copy()
+    orc.photon_gather(sc, cam, W, H, r0, hs, cph, cheads, cnxt, cacc)
+    return before, after, cacc, _max_chain(cph, ccnt, r0, hs)
+
+
+def test_gather_matches_oracle(product, orc, c1):
+    """Chains below the reference's 512-step walk cap: every photon in range
+    is summed, only the summation order differs (GPU insertion order)."""
+    w, sc, cam = c1
+    before, after, cacc, longest = _gather_pair(product, orc, sc, cam, 96, 64, 100_000, 0.02, 1 << 20)
+    assert longest < 512
+    assert np.abs(after - before).max() > 0  # caustics landed somewhere
+    np.testing.assert_allclose(after, cacc, rtol=2e-5, atol=1e-6)
+    np.testing.assert_array_equal(after[..., 3], before[..., 3])
+
+
+def test_gather_with_capped_chains(product, orc, c1):
+    """Chains longer than 512 are cut by the reference's `safety < 512` walk
+    cap (photon_gather.comp:193), so which photons count depends on insertion
+    order -- on the reference's own GPU too.  Pixels agree statistically."""
+    w, sc, cam = c1
+    before, after, cacc, longest = _gather_pair(product, orc, sc, cam, 96, 64, 300_000, 0.02, 1 << 20)
+    assert longest > 512
+    g, c = (after - before)[..., :3], (cacc - before)[..., :3]
+    close = np.all(np.abs(g - c) <= 2e-5 * np.abs(c) + 1e-6, axis=-1)
+    assert close.mean() > 0.98, close.mean()
+    assert abs(g.sum() - c.sum()) / c.sum() < 0.02
+
+
+def test_atrous_exact_bit_identical(product, orc, c1):
+    import pyoracle as po
+    w, sc, cam = c1
+    W, H, spp = 128, 72, 4
+    p = product.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, spp)
+        acc, gb, ga, var = ctx.read_buffers()
+        out = ctx.denoise(p)
+        # disabled denoiser = p00 only
+        p_off = product.rc_atrous_params(0, 5, 1.0, 128.0, 1.0, 0, 1.5)
+        out_off = ctx.denoise(p_off)
+    ref_out = orc.denoise(acc, gb, ga, var, W, H, spp, po.AtrousParams(1, 5, 1.0, 128.0, 1.0, 0, 1.0))
+    assert np.array_equal(bits(out), bits(ref_out))
+    ref_off = orc.p00(acc, W, H, spp, 1.5)
+    assert np.array_equal(bits(out_off), bits(ref_off))
+
+
+@pytest.mark.parametrize("iters,step_sigma", [(1, 64.0), (3, 16.0)])
+def test_atrous_fast_close(product, orc, c1, iters, step_sigma):
+    import pyoracle as po
+    w, sc, cam = c1
+    W, H, spp = 128, 72, 4
+    p = product.rc_atrous_params(1, iters, 1.0, step_sigma, 0.15, 0, 1.0)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, spp)
+        acc, gb, ga, var = ctx.read_buffers()
+        ctx.set_math_mode(product.RC_MATH_FAST)
+        out = ctx.denoise(p)
+    ref_out = orc.denoise(acc, gb, ga, var, W, H, spp, po.AtrousParams(1, iters, 1.0, step_sigma, 0.15, 0, 1.0))
+    np.testing.assert_allclose(out, ref_out, rtol=2e-3, atol=2e-4)
+
+
+def test_render_frame_matches_reference_sequence(product, orc, c1):
+    """rc_render_frame with SPPM iterations == spp is the reference export
+    loop: trace -> render 1 spp -> gather -> shrink radius, then p00+à-trous."""
+    import pyoracle as po
+    w, sc, cam = c1
+    W, H, spp, N, hs, r0, alpha = 96, 64, 3, 100_000, 1 << 18, 0.02, 0.7
+    p = product.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        out = ctx.render_frame(cam, (1, 1.0), spp, product.rc_sppm_params(N, hs, alpha), r0, spp, p)
+        acc = ctx.read_buffers()[0]
+        r_end, it_end = ctx.sppm_state()
+    bufs = po.alloc_images(W, H)
+    r = r0
+    for i in range(spp):
+        ph, hd, nx, cnt, _ = orc.photon_trace(sc, N, r, i * 7919 + 6271, hs)
+        orc.render(sc, cam, (1, 1.0), W, H, i, 1, buffers=bufs)
+        orc.photon_gather(sc, cam, W, H, r, hs, ph, hd, nx, bufs[0])
+        r = orc.lib.or_sppm_next_radius(r, i, alpha)
+    assert it_end == spp and np.float32(r_end) == np.float32(r)
+    np.testing.assert_allclose(acc, bufs[0], rtol=2e-5, atol=1e-6)
+    ref_out = orc.denoise(*bufs, W, H, spp, po.AtrousParams(1, 5, 1.0, 128.0, 1.0, 0, 1.0))
+    np.testing.assert_allclose(out, ref_out, rtol=1e-3, atol=1e-5)
+
+
+def test_errors_are_codes_not_crashes(product, c0):
+    w, sc, cam = c0
+    with _ctx(product, 32, 32, product.RC_MATH_FAST) as ctx:
+        with pytest.raises(product.RetroCamError) as e:
+            ctx.render(cam)
+        assert e.value.code == product.RC_ERR_NO_SCENE
+        bad = dict(sc)
+        nodes = sc["nodes"].copy()
+        interior = np.nonzero(nodes["prim_count"] == 0)[0]
+        nodes[interior[0]]["left_child"] = len(nodes) + 5
+        bad["nodes"] = nodes
+        with pytest.raises(product.RetroCamError) as e:
+            ctx.upload(bad)
+        assert e.value.code == product.RC_ERR_BAD_SCENE
+        cyc = sc["nodes"].copy()
+        cyc[interior[-1]]["left_child"] = 0       # a cycle back to the root
+        bad["nodes"] = cyc
+        with pytest.raises(product.RetroCamError) as e:
+            ctx.upload(bad)
+        assert e.value.code == product.RC_ERR_BAD_SCENE
+        ctx.upload(sc)
+        with pytest.raises(product.RetroCamError) as e:
+            ctx.sppm_trace(1000, 1000)               # not a power of two
+        assert e.value.code == product.RC_ERR_INVALID_ARG
+        with pytest.raises(product.RetroCamError) as e:
+            ctx.render(cam, (1, 1.0), -1, 1)
+        assert e.value.code == product.RC_ERR_INVALID_ARG
+        ctx.render(cam, (1, 1.0), 0, 1)             # still usable
+        ctx.synchronize()
