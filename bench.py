@@ -62,6 +62,8 @@ def parse_args(argv=None):
     ap.add_argument("--math", default="fast", choices=["fast", "exact"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--spp", type=int, default=0, help="override spp (profiling of a small case)")
+    ap.add_argument("--sppm-iterations", type=int, default=-1, help="override SPPM iterations")
     return ap.parse_args(argv)
 
 
@@ -155,9 +157,16 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # workload
 # ---------------------------------------------------------------------------
-def workload_setup(name):
+def workload_setup(name, args=None):
     from retrocam_b200 import api, scenes
     w = scenes.WORKLOADS[name]()
+    if args is not None and args.spp > 0:
+        w.spp = args.spp
+    if args is not None and args.sppm_iterations >= 0 and w.sppm is not None:
+        if args.sppm_iterations == 0:
+            w.sppm = None
+        else:
+            w.sppm.iterations = args.sppm_iterations
     sppm = None
     if w.sppm is not None:
         sppm = api.rc_sppm_params(w.sppm.photons, w.sppm.hash_size, w.sppm.alpha)
@@ -289,7 +298,7 @@ def run_reference(args):
     rank, _, world = dist_env()
     if rank != 0:
         return 0
-    w, _, _ = workload_setup(args.workload)
+    w, _, _ = workload_setup(args.workload, args)
     samples = w.width * w.height * w.spp
     budget = max(2.0, min(args.cpu_seconds, 240.0 / max(1, args.steps + args.warmup)))
     for _ in range(args.warmup):
@@ -339,7 +348,7 @@ def run_b200(args):
     torch.cuda.set_device(local_rank)
     device = torch.device("cuda", local_rank)
     dist = init_dist(world, "nccl")
-    w, sppm, atrous = workload_setup(args.workload)
+    w, sppm, atrous = workload_setup(args.workload, args)
     sc = api.build_scene(w.scene)
     cam = api.workload_camera(w)
     mode = api.RC_MATH_EXACT if args.math == "exact" else api.RC_MATH_FAST
