@@ -309,6 +309,25 @@ int rc_sppm_state(const rc_ctx* ctx, float* radius, int* iteration);
  * out_rgba is non-NULL it is also copied to that host array (W*H*4 floats). */
 int rc_denoise_atrous(rc_ctx* ctx, const rc_atrous_params* params, float* out_rgba);
 
+/* No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory -- hosts that own every device byte through their
+ * own pool and budget, or loops that must not hit the synchronisation an
+ * allocation can cause mid-frame.  Same p00 + à-trous chain as
+ * rc_denoise_atrous, but every image is a caller-owned DEVICE pointer (accum
+ * RGBA32F, gbuffer/albedo RGBA16F, variance R32F, out RGBA32F; out must not
+ * alias accum) and the one intermediate image lives in a static device array
+ * of RC_NOALLOC_MAX_PIXELS RGBA32F pixels (16 MiB) that every GPU loading this
+ * library holds until the process exits.  Larger images return
+ * RC_ERR_CAPACITY.  The first call on a device resolves that array's device
+ * address (make it before any stream capture); errors are read with
+ * rc_last_error(NULL, ...).  All calls on a device share the array, so calls
+ * that overlap on the GPU race.  cuda_stream may be NULL (legacy stream). */
+#define RC_NOALLOC_MAX_PIXELS 1048576
+int rc_denoise_atrous_noalloc(const float* accum_rgba, const uint16_t* gbuffer_rgba16f,
+                              const uint16_t* albedo_rgba16f, const float* variance,
+                              float* out_rgba, int width, int height, int total_samples,
+                              const rc_atrous_params* params, int math_mode, void* cuda_stream);
+
 /* ---------------------------------------------------------------------------
  * Whole export frame (export/RenderPipeline.java:209-239)
  * ------------------------------------------------------------------------- */

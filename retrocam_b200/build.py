@@ -66,9 +66,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
             o = os.path.join(BUILD, name + ".o")
             _run(common + flags + ["-c", os.path.join(CSRC, "kernels.cu"), "-o", o], log)
             objs.append(o)
-        o = os.path.join(BUILD, "api.o")
-        _run(common + ["-c", os.path.join(CSRC, "api.cu"), "-o", o], log)
-        objs.append(o)
+        for name in ("api", "noalloc"):
+            o = os.path.join(BUILD, name + ".o")
+            _run(common + ["-c", os.path.join(CSRC, name + ".cu"), "-o", o], log)
+            objs.append(o)
         o = os.path.join(BUILD, "host_scene.o")
         _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall"] + inc +
              ["-c", os.path.join(CSRC, "host_scene.cpp"), "-o", o], log)

@@ -112,6 +112,15 @@ static cudaError_t copy_d2h(rc_ctx* ctx, void* dst, const void* src, size_t n) {
 static std::mutex g_err_mutex;
 static std::string g_create_err;
 
+namespace rc {
+// Error text of calls that have no context (read with rc_last_error(NULL)).
+__attribute__((visibility("hidden"))) int set_global_error(int code, const char* msg) {
+    std::lock_guard<std::mutex> lk(g_err_mutex);
+    g_create_err = msg;
+    return code;
+}
+}  // namespace rc
+
 static int fail(rc_ctx* c, int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
