@@ -52,6 +52,31 @@ BYTES_LIGHT_SAMPLE = 80   # one light record
 BYTES_SAMPLE_RMW = 20     # accum RGBA32F (16) + variance R32F (4) per pixel sample
 
 
+KERNEL_SYMBOL = {"render": "render_kernel", "wf_trace": "wf_trace", "wf_shade": "wf_shade",
+                 "photon_trace": "photon_trace_kernel", "photon_gather": "photon_gather_kernel",
+                 "atrous": "atrous_kernel", "wf_generate": "wf_generate", "wf_accumulate": "wf_accumulate"}
+
+
+def algorithmic_bytes(kernel: str, ctr: dict, samples: int) -> float:
+    """Bytes the kernel must move at minimum for the work its counters record:
+    32 B per ray-box test (6 floats + 2 ints), 36 B per ray-triangle test
+    (v0, e1, e2), 104 B per shaded hit (3 normals + material index + the 64-B
+    material), 80 B per light record, 20 B per pixel sample (accum + variance
+    read-modify-write), and for the wavefront stages the path state they must
+    read and write (48 B per closest-hit ray, 96 B per shadow ray)."""
+    trav = BYTES_NODE_TEST * ctr["node_tests"] + BYTES_TRI_TEST * ctr["tri_tests"]
+    if kernel == "render":
+        return (trav + BYTES_SURFACE_HIT * ctr["surface_hits"] + BYTES_LIGHT_SAMPLE * ctr["light_samples"]
+                + BYTES_SAMPLE_RMW * samples)
+    if kernel == "wf_trace":
+        return trav + 48 * ctr["closest_rays"] + 96 * ctr["shadow_rays"]
+    if kernel == "wf_shade":
+        return (BYTES_SURFACE_HIT + 160) * ctr["surface_hits"] + BYTES_LIGHT_SAMPLE * ctr["light_samples"]
+    if kernel in ("photon_trace", "photon_gather"):
+        return BYTES_NODE_TEST * ctr["photon_node_tests"] + BYTES_TRI_TEST * ctr["photon_tri_tests"]
+    return 0.0
+
+
 def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -60,6 +85,8 @@ def parse_args(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="export_frame")
     ap.add_argument("--math", default="fast", choices=["fast", "exact"])
+    ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
+    ap.add_argument("--chunk-paths", type=int, default=0, help="wavefront paths in flight (0: default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--spp", type=int, default=0, help="override spp (profiling of a small case)")
@@ -325,7 +352,7 @@ def workload_config(w, args):
            "paths_per_sample": 3 if any(w.lens.lca_delta) else 1, "max_bounces": 6,
            "lens": f"{w.lens.focal_length_mm:g}mm f/{w.lens.f_stop:g} focus {w.lens.focus_dist_m:g} "
                    f"{w.lens.blades} blades",
-           "math": args.math, "parallelism": f"replicas x{args.gpus}",
+           "math": args.math, "engine": args.engine, "parallelism": f"replicas x{args.gpus}",
            "l2": "scene (BVH + triangles) is L2-resident by design; the 854x480 images (6.6 MB accum) are "
                  "rewritten every step"}
     if w.sppm is not None:
@@ -353,6 +380,8 @@ def run_b200(args):
     cam = api.workload_camera(w)
     mode = api.RC_MATH_EXACT if args.math == "exact" else api.RC_MATH_FAST
     ctx = api.Context(w.width, w.height, local_rank, mode)
+    ctx.set_engine(api.RC_ENGINE_WAVEFRONT if args.engine == "wavefront" else api.RC_ENGINE_MEGAKERNEL,
+                   args.chunk_paths)
     stream = torch.cuda.Stream(device=device)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload(sc)
@@ -427,15 +456,12 @@ def run_b200(args):
                        "with the frame read back into pinned host memory"}
 
     # ---- roofline of the dominant kernel ----
-    r_ms, r_launches = ktimes["render"]
-    render_bytes = (BYTES_NODE_TEST * ctr["node_tests"] + BYTES_TRI_TEST * ctr["tri_tests"]
-                    + BYTES_SURFACE_HIT * ctr["surface_hits"] + BYTES_LIGHT_SAMPLE * ctr["light_samples"]
-                    + BYTES_SAMPLE_RMW * samples_per_step * args.steps)
-    per_launch_bytes = render_bytes / max(1, r_launches)
-    avg_launch_s = (r_ms / max(1, r_launches)) / 1e3
+    kernel, (k_ms, k_launches) = max(ktimes.items(), key=lambda kv: kv[1][0])
+    per_launch_bytes = algorithmic_bytes(kernel, ctr, samples_per_step * args.steps) / max(1, k_launches)
+    avg_launch_s = (k_ms / max(1, k_launches)) / 1e3
     peak, peak_kind = hbm_peak()
     achieved = per_launch_bytes / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
-    traffic = read_traffic("render_kernel", w.name)
+    traffic = read_traffic(KERNEL_SYMBOL.get(kernel, kernel), w.name)
     rays = ctr["closest_rays"] + ctr["shadow_rays"] + ctr["photon_rays"] + ctr["gather_rays"]
     kernels_total_ms = sum(v[0] for v in ktimes.values())
     line = {
@@ -446,8 +472,8 @@ def run_b200(args):
         "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "render_kernel", "algorithmic_bytes_per_launch": per_launch_bytes,
-                     "avg_launch_ms": avg_launch_s * 1e3, "launches": r_launches},
+                     "kernel": KERNEL_SYMBOL.get(kernel, kernel), "algorithmic_bytes_per_launch": per_launch_bytes,
+                     "avg_launch_ms": avg_launch_s * 1e3, "launches": k_launches},
         "mrays_per_s": rays / (t_ms / 1e3) / 1e6,
         "kernel_ms": {k: v[0] / args.steps for k, v in ktimes.items()},
         "kernel_share": {k: (v[0] / kernels_total_ms if kernels_total_ms else 0.0) for k, v in ktimes.items()},

@@ -155,12 +155,20 @@ typedef struct rc_counters {
 } rc_counters;
 
 /* Kernel kinds for rc_get_kernel_times. */
-#define RC_KERNEL_RENDER 0
+#define RC_KERNEL_RENDER 0         /* megakernel path tracer */
 #define RC_KERNEL_PHOTON_TRACE 1
 #define RC_KERNEL_PHOTON_GATHER 2
 #define RC_KERNEL_ATROUS 3
 #define RC_KERNEL_NORMALIZE 4
-#define RC_KERNEL_KINDS 5
+#define RC_KERNEL_WF_GENERATE 5    /* wavefront: camera rays */
+#define RC_KERNEL_WF_TRACE 6       /* wavefront: closest-hit + shadow traversal */
+#define RC_KERNEL_WF_SHADE 7       /* wavefront: one bounce of shading + NEE sample */
+#define RC_KERNEL_WF_ACCUMULATE 8  /* wavefront: in-order accumulation, G-buffer */
+#define RC_KERNEL_KINDS 9
+
+/* Path-tracer engines (rc_set_engine). */
+#define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
+#define RC_ENGINE_WAVEFRONT 1   /* per-bounce kernels over compacted path queues */
 
 /* error_word bits. */
 #define RC_GUARD_TRAVERSAL_CAP 0x1u  /* a traversal exceeded its node-visit cap */
@@ -196,6 +204,10 @@ int rc_ctx_set_stream(rc_ctx* ctx, void* cuda_stream);
  * launching stream; rc_get_kernel_times synchronises and returns, per kernel
  * kind, the summed milliseconds and the launch count since the last call. */
 int rc_set_kernel_timing(rc_ctx* ctx, int enable);
+/* Selects the path-tracer engine; both give identical results in exact math.
+ * chunk_paths bounds the wavefront's in-flight paths (path state is about
+ * 200 bytes each); 0 picks the default. */
+int rc_set_engine(rc_ctx* ctx, int engine, int chunk_paths);
 int rc_get_kernel_times(rc_ctx* ctx, double* ms_out, uint64_t* launches_out);
 int rc_abi_version(void);
 

@@ -84,7 +84,10 @@ class rc_counters(C.Structure):
                 ("error_word", C.c_uint32), ("reserved", C.c_uint32)]
 
 
-KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize")
+KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",
+                "wf_shade", "wf_accumulate")
+RC_ENGINE_MEGAKERNEL = 0
+RC_ENGINE_WAVEFRONT = 1
 
 
 _VP, _I, _F = C.c_void_p, C.c_int, C.c_float
@@ -98,6 +101,7 @@ _SIGNATURES = {
     "rc_ctx_set_stream": (_I, [_VP, _VP]),
     "rc_set_kernel_timing": (_I, [_VP, _I]),
     "rc_get_kernel_times": (_I, [_VP, _VP, _VP]),
+    "rc_set_engine": (_I, [_VP, _I, _I]),
     "rc_tessellate_box": (_I, [_F] * 6 + [_I] + [_F] * 3 + [_VP]),
     "rc_tessellate_sphere": (_I, [_F] * 4 + [_I, _I, _I] + [_F] * 3 + [_VP, _I, C.POINTER(_I)]),
     "rc_triangles_from_positions": (_I, [_VP, _I, _I, _VP]),
@@ -353,6 +357,9 @@ class Context:
     def set_stream(self, cuda_stream_handle: int | None):
         """Run on a caller-owned cudaStream_t (e.g. torch.cuda.Stream().cuda_stream)."""
         self.check(lib().rc_ctx_set_stream(self.h, C.c_void_p(cuda_stream_handle or 0)))
+
+    def set_engine(self, engine: int, chunk_paths: int = 0):
+        self.check(lib().rc_set_engine(self.h, engine, chunk_paths))
 
     def set_kernel_timing(self, on: bool):
         self.check(lib().rc_set_kernel_timing(self.h, 1 if on else 0))

@@ -63,9 +63,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         for name, flags in (("kernels_exact", ["-DRC_EXACT=1", "-fmad=false", "-prec-div=true",
                                                "-prec-sqrt=true", "-ftz=false"]),
                             ("kernels_fast", ["-DRC_EXACT=0", "-fmad=true"])):
-            o = os.path.join(BUILD, name + ".o")
-            _run(common + flags + ["-c", os.path.join(CSRC, "kernels.cu"), "-o", o], log)
-            objs.append(o)
+            for src in ("kernels", "wavefront"):
+                o = os.path.join(BUILD, f"{src}_{name.split('_')[1]}.o")
+                _run(common + flags + ["-c", os.path.join(CSRC, src + ".cu"), "-o", o], log)
+                objs.append(o)
         for name in ("api", "noalloc"):
             o = os.path.join(BUILD, name + ".o")
             _run(common + ["-c", os.path.join(CSRC, name + ".cu"), "-o", o], log)

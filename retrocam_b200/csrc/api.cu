@@ -5,6 +5,7 @@
 // and a block of device counters.  Calls are asynchronous on the context's
 // stream unless they return data to the host.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -24,6 +25,10 @@ cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
+cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace exact
 namespace fast {
 cudaError_t launch_render(const RenderArgs&, cudaStream_t);
@@ -31,6 +36,10 @@ cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
+cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace fast
 }  // namespace rc
 
@@ -72,8 +81,14 @@ struct rc_ctx {
         cudaEvent_t a, b;
     };
     std::vector<Timed> pending;
-    double ms[RC_KERNEL_KINDS] = {0, 0, 0, 0, 0};
-    unsigned long long nlaunch[RC_KERNEL_KINDS] = {0, 0, 0, 0, 0};
+    double ms[RC_KERNEL_KINDS] = {};
+    unsigned long long nlaunch[RC_KERNEL_KINDS] = {};
+    // path-tracer engine and wavefront path state
+    int engine = RC_ENGINE_WAVEFRONT;
+    int chunk_paths = 0;   // 0: default
+    DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
+        wf_qlen;
+    int wf_capacity = 0;
     std::string err;
 };
 
@@ -239,7 +254,9 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                     (void*)ctx->out, (void*)ctx->ping, (void*)ctx->pong, (void*)ctx->counters})
         if (p) cudaFree(p);
     for (DevBuf* b : {&ctx->nodes, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
-                      &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter})
+                      &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter, &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
+                      &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
+                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen})
         release(*b);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
@@ -436,6 +453,104 @@ static int launch_err(rc_ctx* ctx, cudaError_t e, const char* what) {
     return fail(ctx, RC_ERR_CUDA, "%s launch failed: %s", what, cudaGetErrorString(e));
 }
 
+int rc_set_engine(rc_ctx* ctx, int engine, int chunk_paths) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if ((engine != RC_ENGINE_MEGAKERNEL && engine != RC_ENGINE_WAVEFRONT) || chunk_paths < 0)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_engine: bad engine %d or chunk %d", engine, chunk_paths);
+    ctx->engine = engine;
+    ctx->chunk_paths = chunk_paths;
+    return RC_OK;
+}
+
+// Default wavefront chunk: every sample of the call, up to 16M paths.
+static const int kDefaultChunkPaths = 16 << 20;
+
+static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
+    const int W = ctx->width, H = ctx->height;
+    const int tiles_x = (W + 7) / 8, tiles_y = (H + 3) / 4;
+    const int npix = tiles_x * tiles_y * 32;
+    // the device decides LCA with the same float expression
+    const bool lca = (fabsf(R.cam.lca[0]) + fabsf(R.cam.lca[2])) > 1e-4f;
+    const int C = lca ? 3 : 1;
+    const long per_sample = (long)npix * C;
+    const long cap_paths = ctx->chunk_paths > 0 ? ctx->chunk_paths : kDefaultChunkPaths;
+    int ns = (int)std::max<long>(1, std::min<long>(R.n_spp, cap_paths / per_sample));
+    const long cap = per_sample * ns;
+    if (cap > ctx->wf_capacity) {
+        CK(cudaStreamSynchronize(ctx->stream));
+        const size_t n = (size_t)cap;
+        CK(ensure(ctx->wf_o, n * 16));
+        CK(ensure(ctx->wf_d, n * 16));
+        CK(ensure(ctx->wf_thr, n * 16));
+        CK(ensure(ctx->wf_rad, n * 16));
+        CK(ensure(ctx->wf_hit, n * 16));
+        CK(ensure(ctx->wf_res, n * 16));
+        CK(ensure(ctx->wf_seed, n * 4));
+        CK(ensure(ctx->wf_rq0, n * 4));
+        CK(ensure(ctx->wf_rq1, n * 4));
+        CK(ensure(ctx->wf_sq0, n * 4));
+        CK(ensure(ctx->wf_sq1, n * 4));
+        CK(ensure(ctx->wf_srec0, n * 64));
+        CK(ensure(ctx->wf_srec1, n * 64));
+        CK(ensure(ctx->wf_qlen, 4 * sizeof(unsigned int)));
+        ctx->wf_capacity = (int)cap;
+    }
+    WaveArgs A;
+    A.scene = R.scene;
+    A.img = R.img;
+    A.cam = R.cam;
+    WaveBuffers& B = A.wb;
+    B.o = (float4*)ctx->wf_o.ptr;
+    B.d = (float4*)ctx->wf_d.ptr;
+    B.thr = (float4*)ctx->wf_thr.ptr;
+    B.rad = (float4*)ctx->wf_rad.ptr;
+    B.hit = (float4*)ctx->wf_hit.ptr;
+    B.res = (float4*)ctx->wf_res.ptr;
+    B.seed = (uint32_t*)ctx->wf_seed.ptr;
+    B.rq[0] = (int*)ctx->wf_rq0.ptr;
+    B.rq[1] = (int*)ctx->wf_rq1.ptr;
+    B.sq[0] = (int*)ctx->wf_sq0.ptr;
+    B.sq[1] = (int*)ctx->wf_sq1.ptr;
+    B.srec[0] = (float4*)ctx->wf_srec0.ptr;
+    B.srec[1] = (float4*)ctx->wf_srec1.ptr;
+    B.qlen = (unsigned int*)ctx->wf_qlen.ptr;
+    B.capacity = ctx->wf_capacity;
+    A.nee_enabled = R.nee_enabled;
+    A.firefly_clamp = R.firefly_clamp;
+    A.channels = C;
+    A.tiles_x = tiles_x;
+    A.npix = npix;
+    A.counters = R.counters;
+    const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    for (int s0 = 0; s0 < R.n_spp; s0 += ns) {
+        A.first_frame = R.first_frame + s0;
+        A.n_samples = std::min(ns, R.n_spp - s0);
+        A.paths = (int)(per_sample * A.n_samples);
+        A.bounce = 0;
+        cudaError_t e = timed_launch(ctx, RC_KERNEL_WF_GENERATE, [&] {
+            return ex ? exact::launch_wf_generate(A, ctx->stream) : fast::launch_wf_generate(A, ctx->stream);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront generate");
+        for (int b = 0; b <= 6; ++b) {
+            A.bounce = b;
+            e = timed_launch(ctx, RC_KERNEL_WF_TRACE, [&] {
+                return ex ? exact::launch_wf_trace(A, ctx->stream) : fast::launch_wf_trace(A, ctx->stream);
+            });
+            if (e != cudaSuccess) return launch_err(ctx, e, "wavefront trace");
+            if (b == 6) break;
+            e = timed_launch(ctx, RC_KERNEL_WF_SHADE, [&] {
+                return ex ? exact::launch_wf_shade(A, ctx->stream) : fast::launch_wf_shade(A, ctx->stream);
+            });
+            if (e != cudaSuccess) return launch_err(ctx, e, "wavefront shade");
+        }
+        e = timed_launch(ctx, RC_KERNEL_WF_ACCUMULATE, [&] {
+            return ex ? exact::launch_wf_accumulate(A, ctx->stream) : fast::launch_wf_accumulate(A, ctx->stream);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront accumulate");
+    }
+    return RC_OK;
+}
+
 int rc_render(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, int first_frame, int n_spp) {
     if (!ctx) return RC_ERR_INVALID_ARG;
     if (!cam || !settings || first_frame < 0 || n_spp < 0)
@@ -452,11 +567,16 @@ int rc_render(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, in
     A.first_frame = first_frame;
     A.n_spp = n_spp;
     A.counters = ctx->counters;
-    const bool ex = ctx->math_mode == RC_MATH_EXACT;
-    const cudaError_t e = timed_launch(ctx, RC_KERNEL_RENDER, [&] {
-        return ex ? exact::launch_render(A, ctx->stream) : fast::launch_render(A, ctx->stream);
-    });
-    if (e != cudaSuccess) return launch_err(ctx, e, "render");
+    if (ctx->engine == RC_ENGINE_WAVEFRONT) {
+        const int r = wavefront_render(ctx, A);
+        if (r != RC_OK) return r;
+    } else {
+        const bool ex = ctx->math_mode == RC_MATH_EXACT;
+        const cudaError_t e = timed_launch(ctx, RC_KERNEL_RENDER, [&] {
+            return ex ? exact::launch_render(A, ctx->stream) : fast::launch_render(A, ctx->stream);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "render");
+    }
     // Renderer.getTotalSamples(): frames 0 .. first_frame + n_spp - 1 done
     ctx->total_samples = first_frame + n_spp;
     return RC_OK;

@@ -149,6 +149,41 @@ struct NormalizeArgs {
     float exposure;
 };
 
+// Wavefront path state, structure of arrays over the paths of one chunk
+// (path p = tiled pixel j + NPIX * (channel + C * sample)).  Queues hold
+// path indices; counters: qlen[0..1] ray queues, qlen[2..3] shadow queues.
+struct WaveBuffers {
+    float4* o;        // ray origin
+    float4* d;        // ray direction
+    float4* thr;      // throughput
+    float4* rad;      // radiance so far
+    float4* hit;      // t, u, v, primitive (int bits; -1 = miss)
+    float4* res;      // final radiance of the path
+    uint32_t* seed;   // PCG state
+    int* rq[2];       // ray queues (ping-pong by bounce)
+    int* sq[2];       // shadow queues
+    float4* srec[2];  // shadow records, 4 float4 per queue slot
+    unsigned int* qlen;
+    int capacity;     // paths per chunk
+};
+
+struct WaveArgs {
+    DeviceScene scene;
+    Images img;
+    CamParams cam;
+    WaveBuffers wb;
+    int nee_enabled;
+    float firefly_clamp;
+    int first_frame;   // frame index of the chunk's first sample
+    int n_samples;     // samples in this chunk
+    int channels;      // 3 with per-channel lens offsets, else 1
+    int tiles_x;       // 8x4-pixel tiles across
+    int npix;          // tiles * 32
+    int paths;         // npix * channels * n_samples
+    int bounce;
+    DevCounters* counters;
+};
+
 }  // namespace rc
 
 #endif

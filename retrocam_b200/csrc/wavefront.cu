@@ -1,0 +1,465 @@
+// wavefront.cu -- the path tracer as a sequence of short kernels over path
+// queues (pathtrace.comp semantics, one kernel per stage instead of one
+// invocation per pixel).
+//
+// Per chunk of paths (all pixels x some samples x 1 or 3 lens channels):
+//   wf_generate    camera rays (pathtrace.comp:401-439) -> ray queue 0
+//   for bounce 0..5:
+//     wf_trace     closest hit for the ray queue AND the visibility test of
+//                  the shadow rays the previous shade produced (one launch,
+//                  two queues: a warp only ever holds one kind of ray)
+//     wf_shade     emission, Russian roulette, BSDF, NEE light sample
+//                  (pathtrace.comp:454-585); survivors -> next ray queue,
+//                  NEE rays -> shadow queue
+//   wf_trace       the last bounce's shadow rays
+//   wf_accumulate  per pixel, the samples in frame order, LCA channel
+//                  assembly, NaN scrub, variance, G-buffer on frame 0
+//                  (pathtrace.comp:601-655)
+// Queues are compacted with a warp ballot + popc and one atomicAdd per warp.
+// Path arithmetic is the megakernel's, operation for operation, and the
+// accumulation adds samples in frame order, so exact-math results stay
+// bit-identical to the oracle.  Kernels are grid-stride loops over device-side
+// queue lengths, launched with a grid that fills the GPU once.
+#include "device_common.cuh"
+
+namespace rc {
+namespace RC_NS {
+
+// Appends `value` to queue q when `want`, one atomic per warp.
+DI void push_queue(bool want, int value, int* q, unsigned int* len) {
+    const unsigned int active = __activemask();
+    const unsigned int m = __ballot_sync(active, want);
+    if (m == 0u) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned int base = 0;
+    if (lane == leader) base = atomicAdd(len, (unsigned int)__popc(m));
+    base = __shfl_sync(active, base, leader);
+    if (want) q[base + __popc(m & ((1u << lane) - 1u))] = value;
+}
+
+struct PathId {
+    int px, py, channel, sample;
+    bool valid;
+};
+
+DI PathId decode(const WaveArgs& A, int p) {
+    PathId id;
+    const int j = p % A.npix;
+    const int k = p / A.npix;
+    id.channel = k % A.channels;
+    id.sample = k / A.channels;
+    const int tile = j >> 5, lane = j & 31;
+    id.px = (tile % A.tiles_x) * 8 + (lane & 7);
+    id.py = (tile / A.tiles_x) * 4 + (lane >> 3);
+    id.valid = id.px < A.img.width && id.py < A.img.height;
+    return id;
+}
+
+DI bool lca_on(const CamParams& c) { return (fabs_(c.lca[0]) + fabs_(c.lca[2])) > 1e-4f; }
+
+__global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
+    const WaveBuffers& B = A.wb;
+    const bool lca = A.channels == 3;
+    uint32_t paths = 0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.paths; p += gridDim.x * blockDim.x) {
+        const PathId id = decode(A, p);
+        bool want = false;
+        if (id.valid) {
+            const int f = A.first_frame + id.sample;
+            uint32_t s = init_seed(id.px, id.py, lca ? f * 3 + id.channel : f);
+            const Ray r = generate_ray(A.cam, A.img.width, A.img.height, id.px, id.py, s,
+                                       lca ? A.cam.lca[id.channel] : 0.0f);
+            B.o[p] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
+            B.d[p] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
+            B.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            B.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            B.seed[p] = s;
+            want = true;
+            ++paths;
+        }
+        push_queue(want, p, B.rq[0], B.qlen + 0);
+    }
+    const unsigned int n = __reduce_add_sync(__activemask(), paths);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(&A.counters->camera_paths, (unsigned long long)n);
+}
+
+// Closest-hit traversal of ray queue rq[bounce&1] followed (same index
+// space) by the visibility tests of shadow queue sq[(bounce+1)&1].
+template <bool kShadowAtParent>
+__global__ void __launch_bounds__(128) wf_trace(WaveArgs A) {
+    const WaveBuffers& B = A.wb;
+    const int cur = A.bounce & 1;
+    const int prev = cur ^ 1;
+    const unsigned int nr = A.bounce < 6 ? B.qlen[cur] : 0u;
+    const unsigned int ns = B.qlen[2 + prev];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        B.qlen[prev] = 0u;      // the ray queue shade(bounce) fills
+        B.qlen[2 + cur] = 0u;   // the shadow queue shade(bounce) fills
+    }
+    Guard g = {0u, 0u, 0u};
+    uint32_t closest = 0, shadow = 0;
+    const unsigned int total = nr + ns;
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+        if (i < nr) {
+            const int p = B.rq[cur][i];
+            const Ray r = make_ray(xyz(B.o[p]), xyz(B.d[p]));
+            const Hit h = trace_closest(A.scene, r, g);
+            B.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
+            ++closest;
+        } else {
+            const int k = (int)(i - nr);
+            const float4* rec = B.srec[prev] + 4 * k;
+            const float4 so = rec[0], sd = rec[1], st = rec[2], sl = rec[3];
+            const int p = __float_as_int(sd.w);
+            const bool vis = trace_shadow<kShadowAtParent>(A.scene, make_ray(xyz(so), xyz(sd)), so.w, g);
+            ++shadow;
+            // radiance += throughput * sampleDirectLight(...), 0 when occluded
+            const float3 L = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
+            const float3 r = xyz(B.rad[p]) + xyz(st) * L;
+            B.rad[p] = make_float4(r.x, r.y, r.z, 0.0f);
+            if (__float_as_int(st.w) != 0) B.res[p] = make_float4(r.x, r.y, r.z, 0.0f);
+        }
+    }
+    const unsigned int active = __activemask();
+    const unsigned int c = __reduce_add_sync(active, closest);
+    const unsigned int s = __reduce_add_sync(active, shadow);
+    const unsigned int n = __reduce_add_sync(active, g.nodes);
+    const unsigned int t = __reduce_add_sync(active, g.tris);
+    const unsigned int gf = __reduce_or_sync(active, g.flags);
+    if ((threadIdx.x & 31) == 0) {
+        if (c) atomicAdd(&A.counters->closest_rays, (unsigned long long)c);
+        if (s) atomicAdd(&A.counters->shadow_rays, (unsigned long long)s);
+        if (n) atomicAdd(&A.counters->node_tests, (unsigned long long)n);
+        if (t) atomicAdd(&A.counters->tri_tests, (unsigned long long)t);
+        if (gf) atomicOr(&A.counters->error_word, gf);
+    }
+}
+
+// One bounce of pathtrace.comp's traceRadiance for every path in ray queue
+// rq[bounce&1] whose closest hit wf_trace has stored.
+__global__ void __launch_bounds__(128) wf_shade(WaveArgs A) {
+    const WaveBuffers& B = A.wb;
+    const DeviceScene& S = A.scene;
+    const int cur = A.bounce & 1;
+    const int nxt = cur ^ 1;
+    const int b = A.bounce;
+    const bool last = b == 5;
+    const unsigned int n = B.qlen[cur];
+    uint32_t hits = 0, lights = 0;
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int p = B.rq[cur][i];
+        const float4 hv = B.hit[p];
+        const int prim = __float_as_int(hv.w);
+        float3 rad = xyz(B.rad[p]);
+        bool cont = false, shadow_rec = false;
+        float4 rec0, rec1, rec2, rec3;
+        // frame-0 albedo image: first hit of the G channel (or the only one)
+        const bool alb_path = b == 0 && A.first_frame + (p / A.npix) / A.channels == 0 &&
+                              ((p / A.npix) % A.channels) == (A.channels == 3 ? 1 : 0);
+        if (prim < 0) {
+            if (alb_path) {
+                const PathId id = decode(A, p);
+                A.img.galb[(long)id.py * A.img.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
+            }
+            B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+        } else {
+            ++hits;
+            const Ray ray = make_ray(xyz(B.o[p]), xyz(B.d[p]));
+            Hit h;
+            h.t = hv.x;
+            h.u = hv.y;
+            h.v = hv.z;
+            h.prim = prim;
+            const Surf sf = surface(S, ray, h);
+            const Mat m = load_mat(S, sf.mat);
+            const float3 rd = ray.d;
+            const float3 nrm = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
+            uint32_t seed = B.seed[p];
+            float3 thr = xyz(B.thr[p]);
+            const bool last_diffuse = B.thr[p].w != 0.0f;
+            if (alb_path) {
+                const float3 a = (m.transmission > 0.5f) ? f3(1.0f, 1.0f, 1.0f) : m.albedo;
+                const PathId id = decode(A, p);
+                A.img.galb[(long)id.py * A.img.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
+            }
+            if (!last_diffuse) rad = rad + (thr * m.emission) * m.strength;
+            bool alive = true;
+            if (b >= 2) {
+                float survive = gmax(m.albedo.x, gmax(m.albedo.y, m.albedo.z));
+                if (m.metallic > 0.5f || m.transmission > 0.5f) survive = 0.95f;
+                survive = gclamp(survive, 0.01f, 0.95f);
+                if (rnd(seed) > survive) alive = false;
+                else thr = thr / survive;
+            }
+            float3 no = f3(0, 0, 0), nd = f3(0, 0, 0);
+            bool nd_diffuse = false;
+            if (alive) {
+                if (m.transmission > 0.5f) {
+                    const bool entering = dot(rd, sf.normal) < 0.0f;
+                    const float eta = entering ? (1.0f / m.ior) : m.ior;
+                    const float cosI = fabs_(dot(rd, nrm));
+                    float r0 = (1.0f - m.ior) / (1.0f + m.ior);
+                    r0 *= r0;
+                    const float F = r0 + (1.0f - r0) * pow5(gclamp(1.0f - cosI, 0.0f, 1.0f));
+                    if (rnd(seed) < F) {
+                        nd = reflect(rd, nrm);
+                    } else {
+                        float3 refr = refract(rd, nrm, eta);
+                        if (dot(refr, refr) < 0.001f) refr = reflect(rd, nrm);
+                        nd = normalize(refr);
+                    }
+                    no = sf.pos + nd * 2e-3f;
+                    thr = thr * m.albedo;
+                } else if (m.metallic > 0.5f) {
+                    const float3 wo = -rd;
+                    const float alpha = gmax(m.roughness, 1e-3f);
+                    const float3 up3 = fabs_(nrm.y) < 0.9999f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);
+                    const float3 T = normalize(cross(up3, nrm));
+                    const float3 Bv = cross(nrm, T);
+                    const float3 wol = f3(dot(wo, T), dot(wo, nrm), dot(wo, Bv));
+                    const float u1 = rnd(seed);
+                    const float u2 = rnd(seed);
+                    const float3 hl = sample_ggx_vndf(wol, alpha, u1, u2);
+                    const float3 hh = normalize(T * hl.x + nrm * hl.y + Bv * hl.z);
+                    nd = reflect(-wo, hh);
+                    if (dot(nd, nrm) <= 0.0f) nd = reflect(-wo, nrm);
+                    const float NdotL = gmax(dot(nrm, nd), 1e-4f);
+                    const float NdotV = gmax(dot(nrm, wo), 1e-4f);
+                    const float HdotV = gmax(dot(hh, wo), 1e-4f);
+                    const float p5 = pow5(1.0f - HdotV);
+                    const float3 F = m.albedo + f3(1.0f - m.albedo.x, 1.0f - m.albedo.y, 1.0f - m.albedo.z) * p5;
+                    const float G1 = smith_g1(NdotV, alpha);
+                    const float G2 = smith_g2(NdotL, NdotV, alpha);
+                    thr = thr * (F * (G2 / gmax(G1, 1e-7f)));
+                    no = sf.pos + nrm * 2e-3f;
+                } else {
+                    // NEE (pathtrace.comp:341-395) up to the visibility test;
+                    // the test and the add happen in the next wf_trace.
+                    if (A.nee_enabled != 0) {
+                        bool early = true;
+                        if (S.light_count > 0 && S.total_light_power > 0.0f) {
+                            const float u = rnd(seed);
+                            int sel = S.light_count - 1;
+                            for (int q = 0; q < S.light_count; ++q)
+                                if (u < __ldg(S.light_cdf + q)) {
+                                    sel = q;
+                                    break;
+                                }
+                            const float4* Lr = S.lights + 5 * sel;
+                            const float4 l0 = __ldg(Lr + 0), l1 = __ldg(Lr + 1), l2 = __ldg(Lr + 2);
+                            const float4 l3 = __ldg(Lr + 3), l4 = __ldg(Lr + 4);
+                            ++lights;
+                            const float pick = l3.w / S.total_light_power;
+                            if (pick > 0.0f) {
+                                float r1 = rnd(seed);
+                                float r2 = rnd(seed);
+                                if (r1 + r2 > 1.0f) {
+                                    r1 = 1.0f - r1;
+                                    r2 = 1.0f - r2;
+                                }
+                                const float3 lv0 = xyz(l0);
+                                const float3 lp = lv0 + r1 * (xyz(l1) - lv0) + r2 * (xyz(l2) - lv0);
+                                const float3 to = lp - sf.pos;
+                                const float dist2 = dot(to, to);
+                                const float dist = sqrtf(dist2);
+                                const float3 sd = to / dist;
+                                const float cos_hit = dot(nrm, sd);
+                                if (cos_hit > 0.0f) {
+                                    const float cos_light = fabs_(dot(xyz(l4), sd));
+                                    if (cos_light > 0.0f) {
+                                        const float area = l0.w;
+                                        const float dist2_safe = gmax(dist2, area);
+                                        const float pdf = pick * (dist2_safe / (area * cos_light));
+                                        float3 contrib = f3(0.0f, 0.0f, 0.0f);
+                                        if (pdf > 0.0f) {
+                                            const float3 em = xyz(l3);
+                                            contrib = (((m.albedo / 3.14159265359f) * em) * cos_hit) / pdf;
+                                            const float cap = dot(em, f3(0.299f, 0.587f, 0.114f)) * A.firefly_clamp;
+                                            contrib = vmin(contrib, f3(cap, cap, cap));
+                                        }
+                                        const float3 so = sf.pos + nrm * 2e-3f;
+                                        rec0 = make_float4(so.x, so.y, so.z, dist - 4e-3f);
+                                        rec1 = make_float4(sd.x, sd.y, sd.z, __int_as_float(p));
+                                        rec2 = make_float4(thr.x, thr.y, thr.z, __int_as_float(last ? 1 : 0));
+                                        rec3 = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                                        shadow_rec = true;
+                                        early = false;
+                                    }
+                                }
+                            }
+                        }
+                        if (early) rad = rad + thr * f3(0.0f, 0.0f, 0.0f);
+                    }
+                    const float u1 = rnd(seed);
+                    const float u2 = rnd(seed);
+                    nd = cosine_hemisphere(u1, u2, nrm);
+                    thr = thr * m.albedo;
+                    no = sf.pos + nrm * 1e-3f;
+                    nd_diffuse = true;
+                }
+                cont = !last;
+            }
+            B.rad[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+            if (cont) {
+                B.o[p] = make_float4(no.x, no.y, no.z, 0.0f);
+                B.d[p] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+                B.thr[p] = make_float4(thr.x, thr.y, thr.z, nd_diffuse ? 1.0f : 0.0f);
+                B.seed[p] = seed;
+            } else if (!shadow_rec) {
+                B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+            }
+        }
+        push_queue(cont, p, B.rq[nxt], B.qlen + nxt);
+        // shadow records go to the slot the ray index takes in sq[cur]
+        {
+            const unsigned int active = __activemask();
+            const unsigned int m = __ballot_sync(active, shadow_rec);
+            if (m != 0u) {
+                const int lane = threadIdx.x & 31;
+                const int leader = __ffs(m) - 1;
+                unsigned int base = 0;
+                if (lane == leader) base = atomicAdd(B.qlen + 2 + cur, (unsigned int)__popc(m));
+                base = __shfl_sync(active, base, leader);
+                if (shadow_rec) {
+                    float4* r = B.srec[cur] + 4 * (base + __popc(m & ((1u << lane) - 1u)));
+                    r[0] = rec0;
+                    r[1] = rec1;
+                    r[2] = rec2;
+                    r[3] = rec3;
+                }
+            }
+        }
+    }
+    const unsigned int active = __activemask();
+    const unsigned int hs = __reduce_add_sync(active, hits);
+    const unsigned int ls = __reduce_add_sync(active, lights);
+    if ((threadIdx.x & 31) == 0) {
+        if (hs) atomicAdd(&A.counters->surface_hits, (unsigned long long)hs);
+        if (ls) atomicAdd(&A.counters->light_samples, (unsigned long long)ls);
+    }
+}
+
+// pathtrace.comp:633-654 per pixel for the chunk's samples, in frame order;
+// on frame 0 also the G-buffer ray (seed 99991, no lens offset).
+__global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
+    const int W = A.img.width, H = A.img.height;
+    Guard g = {0u, 0u, 0u};
+    uint32_t closest = 0, ghits = 0;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < A.npix; j += gridDim.x * blockDim.x) {
+        const int tile = j >> 5, lane = j & 31;
+        const int px = (tile % A.tiles_x) * 8 + (lane & 7);
+        const int py = (tile / A.tiles_x) * 4 + (lane >> 3);
+        if (px >= W || py >= H) continue;
+        const long i = (long)py * W + px;
+        float4 acc = make_float4(0, 0, 0, 0);
+        float var = 0.0f;
+        if (A.first_frame > 0) {
+            acc = A.img.accum[i];
+            var = A.img.var[i];
+        }
+        for (int s = 0; s < A.n_samples; ++s) {
+            const int base = j + A.npix * (A.channels * s);
+            float3 rad;
+            if (A.channels == 3) {
+                rad = f3(A.wb.res[base].x, A.wb.res[base + A.npix].y, A.wb.res[base + 2 * A.npix].z);
+            } else {
+                rad = xyz(A.wb.res[base]);
+            }
+            if (bad(rad.x) || bad(rad.y) || bad(rad.z)) rad = f3(0, 0, 0);
+            const float l = luma709(rad);
+            const float l2 = l * l;
+            if (A.first_frame + s == 0) {
+                acc = make_float4(rad.x, rad.y, rad.z, 1.0f);
+                var = l2;
+                uint32_t gs = init_seed(px, py, 99991);
+                const Ray gr = generate_ray(A.cam, W, H, px, py, gs, 0.0f);
+                ++closest;
+                const Hit h = trace_closest(A.scene, gr, g);
+                float4 gv = make_float4(0.0f, 1.0f, 0.0f, 1e4f);
+                if (h.prim >= 0) {
+                    ++ghits;
+                    const Surf sf = surface(A.scene, gr, h);
+                    const float3 nn = dot(gr.d, sf.normal) < 0.0f ? sf.normal : -sf.normal;
+                    gv = make_float4(nn.x, nn.y, nn.z, h.t);
+                }
+                A.img.gbuf[i] = to_half4(gv.x, gv.y, gv.z, gv.w);
+            } else {
+                acc.x = acc.x + rad.x;
+                acc.y = acc.y + rad.y;
+                acc.z = acc.z + rad.z;
+                acc.w = acc.w + 1.0f;
+                var = var + l2;
+            }
+        }
+        A.img.accum[i] = acc;
+        A.img.var[i] = var;
+    }
+    const unsigned int active = __activemask();
+    const unsigned int c = __reduce_add_sync(active, closest);
+    const unsigned int n = __reduce_add_sync(active, g.nodes);
+    const unsigned int t = __reduce_add_sync(active, g.tris);
+    const unsigned int h = __reduce_add_sync(active, ghits);
+    const unsigned int gf = __reduce_or_sync(active, g.flags);
+    if ((threadIdx.x & 31) == 0) {
+        if (c) atomicAdd(&A.counters->closest_rays, (unsigned long long)c);
+        if (n) atomicAdd(&A.counters->node_tests, (unsigned long long)n);
+        if (t) atomicAdd(&A.counters->tri_tests, (unsigned long long)t);
+        if (h) atomicAdd(&A.counters->surface_hits, (unsigned long long)h);
+        if (gf) atomicOr(&A.counters->error_word, gf);
+    }
+}
+
+static int grid_for(const void* fn, int block) {
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0);
+    return sms * (per > 0 ? per : 1);
+}
+
+// Launchers; the chunk sequence (generate, 7 x trace, 6 x shade interleaved,
+// accumulate) is driven from api.cu so each launch can be timed.  Grids are
+// sized once to fill every SM (grid-stride kernels).
+struct WfGrids {
+    int gen = 0, trace0 = 0, trace1 = 0, shade = 0, acc = 0;
+};
+static WfGrids& grids() {
+    static WfGrids g;
+    if (!g.gen) {
+        g.gen = grid_for((const void*)wf_generate, 256);
+        g.trace0 = grid_for((const void*)wf_trace<false>, 128);
+        g.trace1 = grid_for((const void*)wf_trace<true>, 128);
+        g.shade = grid_for((const void*)wf_shade, 128);
+        g.acc = grid_for((const void*)wf_accumulate, 128);
+    }
+    return g;
+}
+
+cudaError_t launch_wf_generate(const WaveArgs& A, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(A.wb.qlen, 0, 4 * sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    wf_generate<<<grids().gen, 256, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s) {
+    if (A.scene.depth <= 28)
+        wf_trace<true><<<grids().trace1, 128, 0, s>>>(A);
+    else
+        wf_trace<false><<<grids().trace0, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_shade(const WaveArgs& A, cudaStream_t s) {
+    wf_shade<<<grids().shade, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_accumulate(const WaveArgs& A, cudaStream_t s) {
+    wf_accumulate<<<grids().acc, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+}  // namespace RC_NS
+}  // namespace rc

@@ -24,8 +24,18 @@ def _scene(product, orc, workload):
     return w, sc, cam
 
 
-def _ctx(product, W, H, mode):
-    return product.Context(W, H, 0, mode)
+ENGINES = ("megakernel", "wavefront", "wavefront_small_chunks")
+
+
+def _ctx(product, W, H, mode, engine="wavefront"):
+    ctx = product.Context(W, H, 0, mode)
+    if engine == "megakernel":
+        ctx.set_engine(product.RC_ENGINE_MEGAKERNEL)
+    elif engine == "wavefront_small_chunks":
+        ctx.set_engine(product.RC_ENGINE_WAVEFRONT, 5000)   # several chunks per call
+    else:
+        ctx.set_engine(product.RC_ENGINE_WAVEFRONT)
+    return ctx
 
 
 @pytest.fixture(scope="module")
@@ -48,15 +58,16 @@ def _same_images(gpu, cpu):
             raise AssertionError(f"{n}: {len(bad)} words differ, first at {bad[:3].tolist()}")
 
 
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("size,spp,lca", [((64, 64), 1, False), ((256, 256), 1, False), ((256, 256), 4, True),
                                           ((97, 61), 3, False)])
-def test_render_exact_bit_identical_cornell(product, orc, c0, size, spp, lca):
+def test_render_exact_bit_identical_cornell(product, orc, c0, size, spp, lca, engine):
     w, sc, cam = c0
     cam = dict(cam)
     if lca:
         cam["lca_delta"] = (-0.009, 0.0, 0.009)
     W, H = size
-    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+    with _ctx(product, W, H, product.RC_MATH_EXACT, engine) as ctx:
         ctx.upload(sc)
         ctx.render(cam, (1, 1.0), 0, spp)
         gpu = ctx.read_buffers()
@@ -64,10 +75,11 @@ def test_render_exact_bit_identical_cornell(product, orc, c0, size, spp, lca):
     _same_images(gpu, cpu)
 
 
-def test_render_exact_bit_identical_export_scene(product, orc, c1):
+@pytest.mark.parametrize("engine", ENGINES)
+def test_render_exact_bit_identical_export_scene(product, orc, c1, engine):
     w, sc, cam = c1
     W, H = 160, 90
-    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+    with _ctx(product, W, H, product.RC_MATH_EXACT, engine) as ctx:
         ctx.upload(sc)
         ctx.render(cam, (1, 1.0), 0, 3)
         gpu = ctx.read_buffers()
@@ -81,13 +93,14 @@ def test_render_exact_bit_identical_export_scene(product, orc, c1):
     assert cnt["error_word"] == 0
 
 
-def test_render_split_launches_equal_one_launch(product, c1):
+@pytest.mark.parametrize("engine", ENGINES)
+def test_render_split_launches_equal_one_launch(product, c1, engine):
     """n_spp frames in one launch == one launch per frame (same additions)."""
     w, sc, cam = c1
     W, H = 64, 48
     out = []
     for split in (False, True):
-        with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        with _ctx(product, W, H, product.RC_MATH_EXACT, engine) as ctx:
             ctx.upload(sc)
             if split:
                 for f in range(5):
@@ -99,11 +112,12 @@ def test_render_split_launches_equal_one_launch(product, c1):
     _same_images(out[0], out[1])
 
 
-def test_render_nee_off_and_clamp(product, orc, c1):
+@pytest.mark.parametrize("engine", ENGINES[:2])
+def test_render_nee_off_and_clamp(product, orc, c1, engine):
     w, sc, cam = c1
     W, H = 48, 32
     for settings in ((0, 1.0), (1, 20.0)):
-        with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        with _ctx(product, W, H, product.RC_MATH_EXACT, engine) as ctx:
             ctx.upload(sc)
             ctx.render(cam, settings, 0, 2)
             gpu = ctx.read_buffers()
@@ -111,12 +125,13 @@ def test_render_nee_off_and_clamp(product, orc, c1):
         _same_images(gpu, cpu)
 
 
-def test_render_fast_close_to_oracle(product, orc, c1):
+@pytest.mark.parametrize("engine", ENGINES[:2])
+def test_render_fast_close_to_oracle(product, orc, c1, engine):
     """Fast math reorders rounding, so a few paths take another branch; the
     per-pixel check is statistical and the image mean must agree."""
     w, sc, cam = c1
     W, H, spp = 160, 90, 4
-    with _ctx(product, W, H, product.RC_MATH_FAST) as ctx:
+    with _ctx(product, W, H, product.RC_MATH_FAST, engine) as ctx:
         ctx.upload(sc)
         ctx.render(cam, (1, 1.0), 0, spp)
         acc, gb, ga, var = ctx.read_buffers()
