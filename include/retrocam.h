@@ -164,7 +164,8 @@ typedef struct rc_counters {
 #define RC_KERNEL_WF_TRACE 6       /* wavefront: closest-hit + shadow traversal */
 #define RC_KERNEL_WF_SHADE 7       /* wavefront: one bounce of shading + NEE sample */
 #define RC_KERNEL_WF_ACCUMULATE 8  /* wavefront: in-order accumulation, G-buffer */
-#define RC_KERNEL_KINDS 9
+#define RC_KERNEL_PHOTON_LAYOUT 9  /* photon map: cell scan, scatter, heads/next */
+#define RC_KERNEL_KINDS 10
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */

@@ -85,7 +85,7 @@ class rc_counters(C.Structure):
 
 
 KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",
-                "wf_shade", "wf_accumulate")
+                "wf_shade", "wf_accumulate", "photon_layout")
 RC_ENGINE_MEGAKERNEL = 0
 RC_ENGINE_WAVEFRONT = 1
 

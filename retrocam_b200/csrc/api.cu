@@ -22,6 +22,7 @@ namespace rc {
 namespace exact {
 cudaError_t launch_render(const RenderArgs&, cudaStream_t);
 cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
+cudaError_t launch_photon_layout(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
@@ -33,6 +34,7 @@ cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 namespace fast {
 cudaError_t launch_render(const RenderArgs&, cudaStream_t);
 cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
+cudaError_t launch_photon_layout(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
@@ -67,7 +69,8 @@ struct rc_ctx {
     bool has_scene = false;
     DevBuf nodes, tri_isect, tri_shade, mats, lights, cdf;
     // SPPM
-    DevBuf photons, heads, next, counter;
+    DevBuf photons, heads, next, counter, cell_of, cell_count, cell_start, block_sums, seg_photon, seg_posw,
+        seg_powyz;
     int photon_cap = 0, hash_cap = 0, last_hash = 0, last_photons = 0;
     float sppm_radius = 0.05f;
     int sppm_iteration = 0;
@@ -95,7 +98,7 @@ struct rc_ctx {
 // Launch one kernel through `fn` (a launcher returning cudaError_t), with
 // optional event bracketing for rc_get_kernel_times.
 template <class F>
-static cudaError_t timed_launch(rc_ctx* ctx, int kind, F fn) {
+static cudaError_t timed_launch(rc_ctx* ctx, int kind, F fn, int kernels = 1) {
     cudaEvent_t a = nullptr, b = nullptr;
     if (ctx->timing) {
         cudaError_t e = cudaEventCreate(&a);
@@ -105,7 +108,7 @@ static cudaError_t timed_launch(rc_ctx* ctx, int kind, F fn) {
     }
     cudaError_t e = fn();
     if (e != cudaSuccess) return e;
-    ctx->launches++;
+    ctx->launches += kernels;
     if (ctx->timing) {
         e = cudaEventRecord(b, ctx->stream);
         if (e != cudaSuccess) return e;
@@ -254,7 +257,9 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                     (void*)ctx->out, (void*)ctx->ping, (void*)ctx->pong, (void*)ctx->counters})
         if (p) cudaFree(p);
     for (DevBuf* b : {&ctx->nodes, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
-                      &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter, &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
+                      &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter, &ctx->cell_of, &ctx->cell_count,
+                      &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw, &ctx->seg_powyz,
+                      &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
                       &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
                       &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen})
         release(*b);
@@ -635,16 +640,25 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     if (cap > ctx->photon_cap) {
         CK(ensure(ctx->photons, (size_t)cap * 3 * sizeof(float4)));
         CK(ensure(ctx->next, (size_t)cap * sizeof(int)));
+        CK(ensure(ctx->cell_of, (size_t)cap * sizeof(int)));
+        CK(ensure(ctx->seg_photon, (size_t)cap * sizeof(int)));
+        CK(ensure(ctx->seg_posw, (size_t)cap * sizeof(float4)));
+        CK(ensure(ctx->seg_powyz, (size_t)cap * sizeof(float2)));
         ctx->photon_cap = cap;
     }
     if (p->hash_size > ctx->hash_cap) {
         CK(ensure(ctx->heads, (size_t)p->hash_size * sizeof(int)));
+        CK(ensure(ctx->cell_count, (size_t)p->hash_size * sizeof(unsigned int)));
+        CK(ensure(ctx->cell_start, ((size_t)p->hash_size + 1) * sizeof(unsigned int)));
+        CK(ensure(ctx->block_sums, (((size_t)p->hash_size + 4095) / 4096) * sizeof(unsigned int)));
         ctx->hash_cap = p->hash_size;
     }
     CK(ensure(ctx->counter, sizeof(unsigned int)));
     // PhotonMap.clear(): heads = -1, counter = 0
     CK(cudaMemsetAsync(ctx->heads.ptr, 0xff, (size_t)p->hash_size * sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(ctx->counter.ptr, 0, sizeof(unsigned int), ctx->stream));
+    CK(cudaMemsetAsync(ctx->cell_count.ptr, 0, (size_t)p->hash_size * sizeof(unsigned int), ctx->stream));
+    CK(cudaMemsetAsync(ctx->cell_start.ptr, 0, ((size_t)p->hash_size + 1) * sizeof(unsigned int), ctx->stream));
     ctx->last_hash = p->hash_size;
     ctx->last_photons = p->photon_count;
     if (p->photon_count == 0 || ctx->scene.light_count == 0) return RC_OK;
@@ -654,15 +668,26 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     A.heads = (int*)ctx->heads.ptr;
     A.next = (int*)ctx->next.ptr;
     A.counter = (unsigned int*)ctx->counter.ptr;
+    A.cell_of = (int*)ctx->cell_of.ptr;
+    A.cell_count = (unsigned int*)ctx->cell_count.ptr;
+    A.cell_start = (unsigned int*)ctx->cell_start.ptr;
+    A.block_sums = (unsigned int*)ctx->block_sums.ptr;
+    A.seg_photon = (int*)ctx->seg_photon.ptr;
+    A.seg_posw = (float4*)ctx->seg_posw.ptr;
+    A.seg_powyz = (float2*)ctx->seg_powyz.ptr;
     A.photon_count = p->photon_count;
     A.hash_size = p->hash_size;
     A.radius = ctx->sppm_radius;
     A.seed = ctx->sppm_iteration * 7919 + 6271;
     A.counters = ctx->counters;
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
-    const cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_TRACE, [&] {
+    cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_TRACE, [&] {
         return ex ? exact::launch_photon_trace(A, ctx->stream) : fast::launch_photon_trace(A, ctx->stream);
     });
+    if (e != cudaSuccess) return launch_err(ctx, e, "photon trace");
+    e = timed_launch(ctx, RC_KERNEL_PHOTON_LAYOUT, [&] {
+        return ex ? exact::launch_photon_layout(A, ctx->stream) : fast::launch_photon_layout(A, ctx->stream);
+    }, 5);
     return launch_err(ctx, e, "photon trace");
 }
 
@@ -679,9 +704,9 @@ int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, f
     A.scene = ctx->scene;
     A.img = ctx->img;
     A.cam = cam_params(cam);
-    A.photons = (const float4*)ctx->photons.ptr;
-    A.heads = (const int*)ctx->heads.ptr;
-    A.next = (const int*)ctx->next.ptr;
+    A.cell_start = (const unsigned int*)ctx->cell_start.ptr;
+    A.seg_posw = (const float4*)ctx->seg_posw.ptr;
+    A.seg_powyz = (const float2*)ctx->seg_powyz.ptr;
     A.hash_size = p->hash_size;
     A.radius = ctx->sppm_radius;
     A.weight = weight;

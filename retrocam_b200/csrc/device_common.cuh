@@ -422,6 +422,134 @@ DI bool trace_shadow(const DeviceScene& S, const Ray& r, float max_dist, Guard& 
     return true;
 }
 
+#if !RC_EXACT
+// Fast-build traversals.  Interior steps and triangle tests run in separate
+// loops; a lane that reaches a leaf parks it and keeps descending until every
+// lane of the warp still descending holds a parked leaf, then the warp tests
+// triangles together, so interior and leaf work are not interleaved lane by
+// lane.  The nearer hit child is entered directly and only the farther one is
+// pushed.  The closest hit equals trace_closest's except where two triangles
+// tie exactly; the shadow answer is the same yes/no.
+struct TravNode {
+    int ref, cnt;   // cnt > 0: leaf with primitives [ref, ref+cnt)
+};
+
+DI bool pop_entry(const int2* stk, const float* stt, int& top, float cull, TravNode& n) {
+    while (top > 0) {
+        --top;
+        if (stt[top] > cull) continue;
+        n.ref = stk[top].x;
+        n.cnt = stk[top].y;
+        return true;
+    }
+    return false;
+}
+
+template <bool kAnyHit>
+DI bool traverse_ww(const DeviceScene& S, const Ray& r, float max_t, Guard& g, Hit& h) {
+    h.t = max_t;
+    h.prim = -1;
+    h.u = h.v = 0.0f;
+    float tmin;
+    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin) ||
+        tmin > h.t)
+        return false;
+    int2 stk[64];
+    float stt[64];
+    int top = 0;
+    TravNode node = {S.root_ref, S.root_count};
+    bool have_node = true;
+    TravNode leaf = {0, 0};
+    int steps = 0;
+    while (have_node || leaf.cnt > 0) {
+        while (have_node) {
+            if (node.cnt > 0) {
+                if (leaf.cnt > 0) break;  // already parked one: test it first
+                leaf = node;
+                have_node = pop_entry(stk, stt, top, h.t, node);
+            } else {
+                const NodeRec* nr = S.nodes + node.ref;
+                const float4 a = __ldg(&nr->a), b = __ldg(&nr->b), c = __ldg(&nr->c);
+                const int4 d = __ldg(&nr->d);
+                float tl, tr;
+                const bool hl = tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > h.t);
+                const bool hr = tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > h.t);
+                if (hl && hr) {
+                    const bool left_first = tl < tr;
+                    if (top < 62) {
+                        stk[top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
+                        stt[top++] = left_first ? tr : tl;
+                    }
+                    node.ref = left_first ? d.x : d.z;
+                    node.cnt = left_first ? d.y : d.w;
+                } else if (hl) {
+                    node.ref = d.x;
+                    node.cnt = d.y;
+                } else if (hr) {
+                    node.ref = d.z;
+                    node.cnt = d.w;
+                } else {
+                    have_node = pop_entry(stk, stt, top, h.t, node);
+                }
+            }
+            if (++steps > 2 * S.node_count) {
+                g.flags |= RC_GUARD_TRAVERSAL_CAP;
+                return h.prim >= 0;
+            }
+            if (__all_sync(__activemask(), leaf.cnt > 0)) break;
+        }
+        if (leaf.cnt > 0) {
+            for (int i = leaf.ref; i < leaf.ref + leaf.cnt; ++i) {
+                float t, u, v;
+                if (thit(g, r, S.tri_isect, i, t, u, v) && t < h.t) {
+                    if (kAnyHit) return true;
+                    h.t = t;
+                    h.u = u;
+                    h.v = v;
+                    h.prim = i;
+                }
+            }
+            leaf.cnt = 0;
+        }
+    }
+    return h.prim >= 0;
+}
+#endif
+
+// Closest hit and visibility as used by the kernels: the reference's
+// traversal order in the exact build, the warp-cooperative one in the fast
+// build.
+DI Hit closest_hit(const DeviceScene& S, const Ray& r, Guard& g) {
+#if RC_EXACT
+    return trace_closest(S, r, g);
+#else
+    Hit h;
+    traverse_ww<false>(S, r, 1e30f, g, h);
+    return h;
+#endif
+}
+
+template <bool kTestAtParent>
+DI bool unoccluded(const DeviceScene& S, const Ray& r, float max_dist, Guard& g) {
+#if RC_EXACT
+    return trace_shadow<kTestAtParent>(S, r, max_dist, g);
+#else
+    Hit h;
+    return !traverse_ww<true>(S, r, max_dist, g, h);
+#endif
+}
+
+// The photon passes' closest hit: the reference's unordered push order in
+// the exact build (it decides ties), the fast traversal otherwise.
+template <bool kTestAtParent>
+DI Hit photon_hit(const DeviceScene& S, const Ray& r, Guard& g) {
+#if RC_EXACT
+    return trace_unordered<kTestAtParent>(S, r, g);
+#else
+    return closest_hit(S, r, g);
+#endif
+}
+
 // ---------------------------------------------------------------------------
 // materials and sampling
 // ---------------------------------------------------------------------------
@@ -574,7 +702,7 @@ DI float3 sample_direct_light(const DeviceScene& S, float3 hp, float3 n, float3 
     const float area = l0.w;
     const float dist2_safe = gmax(dist2, area);
     cn.shadow++;
-    if (!trace_shadow<kShadowAtParent>(S, make_ray(hp + n * 2e-3f, sd), dist - 4e-3f, g)) return f3(0, 0, 0);
+    if (!unoccluded<kShadowAtParent>(S, make_ray(hp + n * 2e-3f, sd), dist - 4e-3f, g)) return f3(0, 0, 0);
     const float pdf = pick * (dist2_safe / (area * cos_light));
     if (pdf <= 0.0f) return f3(0, 0, 0);
     const float3 em = xyz(l3);
@@ -594,7 +722,7 @@ DI float3 trace_radiance(const DeviceScene& S, Ray ray, uint32_t& seed, int nee,
     cn.paths++;
     for (int bounce = 0; bounce < 6; ++bounce) {
         cn.closest++;
-        const Hit hit = trace_closest(S, ray, g);
+        const Hit hit = closest_hit(S, ray, g);
         if (hit.prim < 0) break;
         cn.hits++;
         const Surf sf = surface(S, ray, hit);

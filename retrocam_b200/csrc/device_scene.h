@@ -100,12 +100,24 @@ struct RenderArgs {
     DevCounters* counters;
 };
 
+// The photon map (scene/PhotonMap.java) plus its cell-sorted copy.  The trace
+// appends records and counts photons per hash cell; a scan of the counts and a
+// scatter lay each cell's photons out contiguously (cell_start, seg_*), and
+// the reference's heads/next chains are rebuilt from that order, so both
+// views list the same photons in the same order.
 struct PhotonArgs {
     DeviceScene scene;
     float4* photons;        // 3 float4 per photon (std430 record)
     int* heads;
     int* next;
     unsigned int* counter;
+    int* cell_of;           // hash cell of each stored photon
+    unsigned int* cell_count;   // hash_size counters, zero before the trace
+    unsigned int* cell_start;   // hash_size + 1 exclusive prefix sums
+    unsigned int* block_sums;   // scan scratch
+    int* seg_photon;        // photon index at each cell-sorted slot
+    float4* seg_posw;       // (position.xyz, power.x) per slot
+    float2* seg_powyz;      // (power.y, power.z) per slot
     int photon_count;
     int hash_size;
     float radius;
@@ -117,9 +129,9 @@ struct GatherArgs {
     DeviceScene scene;
     Images img;
     CamParams cam;
-    const float4* photons;
-    const int* heads;
-    const int* next;
+    const unsigned int* cell_start;
+    const float4* seg_posw;
+    const float2* seg_powyz;
     int hash_size;
     float radius;
     float weight;

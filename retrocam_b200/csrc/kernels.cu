@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(128) render_kernel(RenderArgs A) {
                 uint32_t gs = init_seed(px, py, 99991);
                 const Ray gr = generate_ray(cam, W, H, px, py, gs, 0.0f);
                 cn.closest++;
-                const Hit h = trace_closest(S, gr, g);
+                const Hit h = closest_hit(S, gr, g);
                 float4 gv = make_float4(0.0f, 1.0f, 0.0f, 1e4f);
                 if (h.prim >= 0) {
                     cn.hits++;
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(128) photon_trace_kernel(PhotonArgs A) {
         bool spec = false;
         for (int b = 0; b < 8; ++b) {
             ++rays;
-            const Hit hit = trace_unordered<kAtParent>(S, ray, g);
+            const Hit hit = photon_hit<kAtParent>(S, ray, g);
             if (hit.prim < 0) break;
             ++hits;
             const Surf sf = surface(S, ray, hit);
@@ -206,8 +206,11 @@ __global__ void __launch_bounds__(128) photon_trace_kernel(PhotonArgs A) {
             const int cy = (int)floorf(spos.y / A.radius);
             const int cz = (int)floorf(spos.z / A.radius);
             const int h = cell_hash(cx, cy, cz, A.hash_size);
-            const int old = atomicExch(A.heads + h, (int)idx);
-            A.next[idx] = old;
+            // the reference links the photon into its cell here with an
+            // atomicExchange on the head; the cell-sorted layout is built by
+            // the scan/scatter kernels below, and heads/next from it
+            A.cell_of[idx] = h;
+            atomicAdd(A.cell_count + h, 1u);
             A.photons[3 * idx + 0] = make_float4(spos.x, spos.y, spos.z, 0.0f);
             A.photons[3 * idx + 1] = make_float4(spow.x, spow.y, spow.z, 0.0f);
             A.photons[3 * idx + 2] = make_float4(sdir.x, sdir.y, sdir.z, 0.0f);
@@ -244,7 +247,7 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
         int hm = 0;
         for (int s = 0; s <= 6; ++s) {
             ++rays;
-            const Hit hit = trace_unordered<kAtParent>(S, ray, g);
+            const Hit hit = photon_hit<kAtParent>(S, ray, g);
             if (hit.prim < 0) break;
             ++hits;
             const Surf sf = surface(S, ray, hit);
@@ -277,18 +280,41 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
                 for (int dy = -1; dy <= 1; ++dy)
                     for (int dx = -1; dx <= 1; ++dx) {
                         const int h = cell_hash(ccx + dx, ccy + dy, ccz + dz, A.hash_size);
-                        int idx = __ldg(A.heads + h);
-                        int safety = 0;
-                        while (idx >= 0 && safety < 512) {
-                            const float4 pp = __ldg(A.photons + 3 * idx);
-                            const float3 d = hp - xyz(pp);
+                        // the chain of cell h, walked as the contiguous slots
+                        // [s0, s1) in chain order; `safety < 512` caps it
+                        const unsigned int s0 = __ldg(A.cell_start + h);
+                        const unsigned int s1 = __ldg(A.cell_start + h + 1);
+                        const unsigned int n = (s1 - s0) < 512u ? (s1 - s0) : 512u;
+                        // four independent loads in flight, then the four
+                        // photons in chain order (the sum order is unchanged)
+                        unsigned int k = 0;
+                        for (; k + 4 <= n; k += 4) {
+                            float4 pw[4];
+                            float2 yz[4];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                pw[q] = __ldg(A.seg_posw + s0 + k + q);
+                                yz[q] = __ldg(A.seg_powyz + s0 + k + q);
+                            }
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const float3 d = hp - xyz(pw[q]);
+                                const float d2 = dot(d, d);
+                                if (d2 <= r2) {
+                                    const float w = 1.0f - d2 / r2;
+                                    caustic = caustic + f3(pw[q].w, yz[q].x, yz[q].y) * w;
+                                }
+                            }
+                        }
+                        for (; k < n; ++k) {
+                            const float4 pw = __ldg(A.seg_posw + s0 + k);
+                            const float3 d = hp - xyz(pw);
                             const float d2 = dot(d, d);
                             if (d2 <= r2) {
                                 const float w = 1.0f - d2 / r2;
-                                caustic = caustic + xyz(__ldg(A.photons + 3 * idx + 1)) * w;
+                                const float2 yz = __ldg(A.seg_powyz + s0 + k);
+                                caustic = caustic + f3(pw.w, yz.x, yz.y) * w;
                             }
-                            idx = __ldg(A.next + idx);
-                            safety++;
                         }
                     }
             const float PI_G = 3.14159265358979f;
@@ -308,6 +334,107 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
     const unsigned int rsum = __reduce_add_sync(0xffffffffu, rays);
     if (lane == 0 && rsum) atomicAdd(&A.counters->gather_rays, (unsigned long long)rsum);
     flush_work(g, 0u, 0u, A.counters, true);
+}
+
+// ---------------------------------------------------------------------------
+// photon map: cell-sorted layout
+// ---------------------------------------------------------------------------
+// Exclusive scan of the per-cell counts into cell_start[0..hash_size], in
+// three passes: 4096 counts per 1024-thread block, a scan of the block sums
+// (one block, sequential over chunks of 1024), and the add-back.
+DI unsigned int block_exclusive_scan(unsigned int v, unsigned int* warp_sums, unsigned int* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned int w = (lane < (int)(blockDim.x >> 5)) ? warp_sums[lane] : 0u;
+        unsigned int z = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        if (lane < (int)(blockDim.x >> 5)) warp_sums[lane] = z - w;
+        if (lane == 31) *total = z;
+    }
+    __syncthreads();
+    const unsigned int r = warp_sums[warp] + x - v;
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(1024) cell_scan_blocks(const unsigned int* __restrict__ count,
+                                                          unsigned int* __restrict__ start,
+                                                          unsigned int* __restrict__ block_sums, int n) {
+    __shared__ unsigned int ws[32];
+    __shared__ unsigned int tot;
+    const int base = blockIdx.x * 4096 + threadIdx.x * 4;
+    unsigned int c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[k] = (base + k < n) ? count[base + k] : 0u;
+    const unsigned int sum = c[0] + c[1] + c[2] + c[3];
+    unsigned int off = block_exclusive_scan(sum, ws, &tot);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (base + k < n) start[base + k] = off;
+        off += c[k];
+    }
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) cell_scan_top(unsigned int* __restrict__ block_sums, int nblocks,
+                                                       unsigned int* __restrict__ start, int n) {
+    __shared__ unsigned int ws[32];
+    __shared__ unsigned int tot;
+    unsigned int carry = 0;
+    for (int b0 = 0; b0 < nblocks; b0 += 1024) {
+        const int i = b0 + threadIdx.x;
+        const unsigned int v = i < nblocks ? block_sums[i] : 0u;
+        const unsigned int x = block_exclusive_scan(v, ws, &tot);
+        if (i < nblocks) block_sums[i] = x + carry;
+        carry += tot;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) start[n] = carry;
+}
+
+__global__ void __launch_bounds__(1024) cell_scan_add(unsigned int* __restrict__ start,
+                                                       const unsigned int* __restrict__ block_sums, int n) {
+    const int i = blockIdx.x * 1024 + threadIdx.x;
+    if (i < n) start[i] += block_sums[i >> 12];
+}
+
+// Each stored photon takes a slot in its cell's segment (cell_count counts
+// back down to zero, ready for the next trace) and copies the fields the
+// gather reads into 24-byte records.
+__global__ void __launch_bounds__(256) photon_scatter(PhotonArgs A, const unsigned int* __restrict__ stored) {
+    const unsigned int n = *stored < (unsigned int)A.photon_count ? *stored : (unsigned int)A.photon_count;
+    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int h = A.cell_of[i];
+        const unsigned int slot = A.cell_start[h] + atomicSub(A.cell_count + h, 1u) - 1u;
+        const float4 pos = A.photons[3 * i], pw = A.photons[3 * i + 1];
+        A.seg_posw[slot] = make_float4(pos.x, pos.y, pos.z, pw.x);
+        A.seg_powyz[slot] = make_float2(pw.y, pw.z);
+        A.seg_photon[slot] = (int)i;
+    }
+}
+
+// heads/next of the reference's PhotonMap, in the segment order.
+__global__ void __launch_bounds__(256) photon_links(PhotonArgs A, const unsigned int* __restrict__ stored) {
+    const unsigned int n = *stored < (unsigned int)A.photon_count ? *stored : (unsigned int)A.photon_count;
+    for (unsigned int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        const int idx = A.seg_photon[s];
+        const int h = A.cell_of[idx];
+        const unsigned int end = A.cell_start[h + 1];
+        A.next[idx] = (s + 1 < end) ? A.seg_photon[s + 1] : -1;
+        if (s == A.cell_start[h]) A.heads[h] = idx;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -422,6 +549,20 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s) {
         photon_trace_kernel<true><<<blocks, 128, 0, s>>>(A);
     else
         photon_trace_kernel<false><<<blocks, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+// The cell-sorted layout of the map the trace just stored (4 launches).
+cudaError_t launch_photon_layout(const PhotonArgs& A, cudaStream_t s) {
+    const int n = A.hash_size;
+    const int nb = (n + 4095) / 4096;
+    cell_scan_blocks<<<nb, 1024, 0, s>>>(A.cell_count, A.cell_start, A.block_sums, n);
+    cell_scan_top<<<1, 1024, 0, s>>>(A.block_sums, nb, A.cell_start, n);
+    cell_scan_add<<<(n + 1023) / 1024, 1024, 0, s>>>(A.cell_start, A.block_sums, n);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    photon_scatter<<<sms * 4, 256, 0, s>>>(A, A.counter);
+    photon_links<<<sms * 4, 256, 0, s>>>(A, A.counter);
     return cudaGetLastError();
 }
 

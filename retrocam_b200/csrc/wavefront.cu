@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(128) wf_trace(WaveArgs A) {
         if (i < nr) {
             const int p = B.rq[cur][i];
             const Ray r = make_ray(xyz(B.o[p]), xyz(B.d[p]));
-            const Hit h = trace_closest(A.scene, r, g);
+            const Hit h = closest_hit(A.scene, r, g);
             B.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             ++closest;
         } else {
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(128) wf_trace(WaveArgs A) {
             const float4* rec = B.srec[prev] + 4 * k;
             const float4 so = rec[0], sd = rec[1], st = rec[2], sl = rec[3];
             const int p = __float_as_int(sd.w);
-            const bool vis = trace_shadow<kShadowAtParent>(A.scene, make_ray(xyz(so), xyz(sd)), so.w, g);
+            const bool vis = unoccluded<kShadowAtParent>(A.scene, make_ray(xyz(so), xyz(sd)), so.w, g);
             ++shadow;
             // radiance += throughput * sampleDirectLight(...), 0 when occluded
             const float3 L = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
                 uint32_t gs = init_seed(px, py, 99991);
                 const Ray gr = generate_ray(A.cam, W, H, px, py, gs, 0.0f);
                 ++closest;
-                const Hit h = trace_closest(A.scene, gr, g);
+                const Hit h = closest_hit(A.scene, gr, g);
                 float4 gv = make_float4(0.0f, 1.0f, 0.0f, 1e4f);
                 if (h.prim >= 0) {
                     ++ghits;
