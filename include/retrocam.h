@@ -169,7 +169,31 @@ typedef struct rc_counters {
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
-#define RC_ENGINE_WAVEFRONT 1   /* per-bounce kernels over compacted path queues */
+#define RC_ENGINE_WAVEFRONT 1   /* per-bounce kernels over compacted path queues;
+                                   fast math traces with a persistent kernel
+                                   that refills idle lanes with new rays */
+#define RC_ENGINE_WAVEFRONT_STATIC 2 /* as above, traced with a grid-stride loop */
+
+/* rc_tuning.wide_bvh bits: which rays traverse the 4-wide copy of the BVH
+ * (collapsed from the reference's binary tree at upload; fast math only --
+ * exact math always walks the binary tree in the reference's order). */
+#define RC_WIDE_PATHS 0x1    /* camera-path closest-hit and shadow rays */
+#define RC_WIDE_PHOTONS 0x2  /* photon-trace and gather rays */
+
+/* Launch-shape knobs of one context, picked by the autotuner
+ * (retrocam_b200/autotune.py) or by hand.  No counterpart in the reference,
+ * whose shaders have fixed local sizes.  Results do not depend on any knob in
+ * exact math; in fast math the traversal width changes the order of float
+ * operations of tied hits only.  Zero fields select the defaults. */
+typedef struct rc_tuning {
+    int32_t engine;        /* RC_ENGINE_*; default RC_ENGINE_WAVEFRONT */
+    int32_t chunk_paths;   /* wavefront paths in flight (queue capacity), 0 = 16M */
+    int32_t wide_bvh;      /* RC_WIDE_* bits; default 0 (the persistent trace of
+                              RC_ENGINE_WAVEFRONT walks the binary tree always) */
+    int32_t trace_block;   /* threads per block of the wavefront trace: 64, 128, 256 (0 = 128) */
+    int32_t shade_block;   /* threads per block of the wavefront shade: 64, 128, 256 (0 = 128) */
+    int32_t photon_block;  /* threads per block of the photon trace: 64, 128, 256 (0 = 128) */
+} rc_tuning;
 
 /* error_word bits. */
 #define RC_GUARD_TRAVERSAL_CAP 0x1u  /* a traversal exceeded its node-visit cap */
@@ -209,6 +233,10 @@ int rc_set_kernel_timing(rc_ctx* ctx, int enable);
  * chunk_paths bounds the wavefront's in-flight paths (path state is about
  * 200 bytes each); 0 picks the default. */
 int rc_set_engine(rc_ctx* ctx, int engine, int chunk_paths);
+/* Sets / reads all launch-shape knobs at once (rc_set_engine sets the first
+ * two).  RC_ERR_INVALID_ARG for a value outside the documented ranges. */
+int rc_set_tuning(rc_ctx* ctx, const rc_tuning* tuning);
+int rc_get_tuning(rc_ctx* ctx, rc_tuning* out);
 int rc_get_kernel_times(rc_ctx* ctx, double* ms_out, uint64_t* launches_out);
 int rc_abi_version(void);
 
@@ -354,6 +382,32 @@ int rc_render_frame(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settin
                     int spp, const rc_sppm_params* sppm, float sppm_initial_radius,
                     int sppm_iterations, const rc_atrous_params* atrous,
                     float* out_rgba);
+
+/* ---------------------------------------------------------------------------
+ * Batched export frames (export/RenderPipeline.java:149-239 per frame, the
+ * video-export loop over keyframed cameras)
+ * ------------------------------------------------------------------------- */
+
+/* One frame of a batch: its camera (keyframes already evaluated), samples
+ * per pixel and SPPM iterations (0 = no SPPM; <= spp). */
+typedef struct rc_frame_desc {
+    rc_camera camera;
+    int32_t spp;
+    int32_t sppm_iterations;
+} rc_frame_desc;
+
+/* Renders n_frames frames of uneven cost back to back, each exactly as
+ * rc_render_frame would, and writes the finished (denoised) frames to
+ * out_frames (n_frames*W*H*4 floats, host; NULL keeps them on the device).
+ * Every buffer the sequence needs is sized before the first frame.  With
+ * use_graph != 0 the whole sequence is captured once into a CUDA graph and
+ * replayed on later calls with the same frames and settings, so the host
+ * issues one launch per batch.  Several contexts on their own streams may
+ * render disjoint batches concurrently. */
+int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames,
+                     const rc_settings* settings, const rc_sppm_params* sppm,
+                     float sppm_initial_radius, const rc_atrous_params* atrous,
+                     float* out_frames, int use_graph);
 
 /* ---------------------------------------------------------------------------
  * Read-back and counters

@@ -75,6 +75,14 @@ class rc_atrous_params(C.Structure):
                 ("exposure", C.c_float)]
 
 
+class rc_tuning(C.Structure):
+    _fields_ = [("engine", C.c_int32), ("chunk_paths", C.c_int32), ("wide_bvh", C.c_int32),
+                ("trace_block", C.c_int32), ("shade_block", C.c_int32), ("photon_block", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class rc_counters(C.Structure):
     _fields_ = [("camera_paths", C.c_uint64), ("closest_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("photon_rays", C.c_uint64), ("gather_rays", C.c_uint64), ("photons_stored", C.c_uint64),
@@ -88,6 +96,9 @@ KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize"
                 "wf_shade", "wf_accumulate", "photon_layout")
 RC_ENGINE_MEGAKERNEL = 0
 RC_ENGINE_WAVEFRONT = 1
+RC_ENGINE_WAVEFRONT_STATIC = 2
+RC_WIDE_PATHS = 0x1
+RC_WIDE_PHOTONS = 0x2
 
 
 _VP, _I, _F = C.c_void_p, C.c_int, C.c_float
@@ -102,6 +113,9 @@ _SIGNATURES = {
     "rc_set_kernel_timing": (_I, [_VP, _I]),
     "rc_get_kernel_times": (_I, [_VP, _VP, _VP]),
     "rc_set_engine": (_I, [_VP, _I, _I]),
+    "rc_set_tuning": (_I, [_VP, _VP]),
+    "rc_get_tuning": (_I, [_VP, _VP]),
+    "rc_render_frames": (_I, [_VP, _VP, _I, _VP, _VP, _F, _VP, _VP, _I]),
     "rc_tessellate_box": (_I, [_F] * 6 + [_I] + [_F] * 3 + [_VP]),
     "rc_tessellate_sphere": (_I, [_F] * 4 + [_I, _I, _I] + [_F] * 3 + [_VP, _I, C.POINTER(_I)]),
     "rc_triangles_from_positions": (_I, [_VP, _I, _I, _VP]),
@@ -360,6 +374,21 @@ class Context:
 
     def set_engine(self, engine: int, chunk_paths: int = 0):
         self.check(lib().rc_set_engine(self.h, engine, chunk_paths))
+
+    def set_tuning(self, **knobs):
+        """Sets launch-shape knobs (rc_tuning field names); unnamed ones keep
+        their current values."""
+        t = self.tuning()
+        for k, v in knobs.items():
+            if k not in t:
+                raise KeyError(k)
+            t[k] = int(v)
+        self.check(lib().rc_set_tuning(self.h, C.byref(rc_tuning(**t))))
+
+    def tuning(self) -> dict:
+        t = rc_tuning()
+        self.check(lib().rc_get_tuning(self.h, C.byref(t)))
+        return t.as_dict()
 
     def set_kernel_timing(self, on: bool):
         self.check(lib().rc_set_kernel_timing(self.h, 1 if on else 0))

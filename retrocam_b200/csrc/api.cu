@@ -21,26 +21,26 @@
 namespace rc {
 namespace exact {
 cudaError_t launch_render(const RenderArgs&, cudaStream_t);
-cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
+cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t, int block);
 cudaError_t launch_photon_layout(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
 cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
-cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t);
-cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
+cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace exact
 namespace fast {
 cudaError_t launch_render(const RenderArgs&, cudaStream_t);
-cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t);
+cudaError_t launch_photon_trace(const PhotonArgs&, cudaStream_t, int block);
 cudaError_t launch_photon_layout(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
 cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
-cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t);
-cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t);
+cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
+cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace fast
 }  // namespace rc
@@ -67,7 +67,7 @@ struct rc_ctx {
     // scene
     DeviceScene scene;
     bool has_scene = false;
-    DevBuf nodes, tri_isect, tri_shade, mats, lights, cdf;
+    DevBuf nodes, nodes4, tri_isect, tri_shade, mats, lights, cdf;
     // SPPM
     DevBuf photons, heads, next, counter, cell_of, cell_count, cell_start, block_sums, seg_photon, seg_posw,
         seg_powyz;
@@ -89,9 +89,18 @@ struct rc_ctx {
     // path-tracer engine and wavefront path state
     int engine = RC_ENGINE_WAVEFRONT;
     int chunk_paths = 0;   // 0: default
+    int wide_bvh = 0;
+    int trace_block = 128, shade_block = 128, photon_block = 128;
     DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
         wf_qlen;
     int wf_capacity = 0;
+    // batched frames (rc_render_frames) and their captured graph
+    DevBuf frames;
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_key = 0;
+    unsigned long long graph_launches = 0;
+    int graph_total_samples = 0, graph_iteration = 0;
+    float graph_radius = 0.0f;
     std::string err;
 };
 
@@ -256,13 +265,14 @@ int rc_ctx_destroy(rc_ctx* ctx) {
     for (void* p : {(void*)ctx->img.accum, (void*)ctx->img.gbuf, (void*)ctx->img.galb, (void*)ctx->img.var,
                     (void*)ctx->out, (void*)ctx->ping, (void*)ctx->pong, (void*)ctx->counters})
         if (p) cudaFree(p);
-    for (DevBuf* b : {&ctx->nodes, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
+    for (DevBuf* b : {&ctx->nodes, &ctx->nodes4, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
                       &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter, &ctx->cell_of, &ctx->cell_count,
                       &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw, &ctx->seg_powyz,
                       &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
                       &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
-                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen})
+                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->frames})
         release(*b);
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return RC_OK;
@@ -299,6 +309,77 @@ int rc_synchronize(rc_ctx* ctx) {
     if (word) return fail(ctx, RC_ERR_DEVICE_GUARD, "kernel guard raised (error word 0x%x)", word);
     return RC_OK;
 }
+
+}  // extern "C"
+
+// Collapses the binary BVH below interior node `bin` into 4-wide nodes,
+// pre-order, returning the index of the node made for `bin`.  A node takes
+// its two children and keeps opening the interior child of largest surface
+// area until it holds four.
+static float node_area(const rc_bvh_node& n) {
+    const float dx = n.aabb_max[0] - n.aabb_min[0], dy = n.aabb_max[1] - n.aabb_min[1];
+    const float dz = n.aabb_max[2] - n.aabb_min[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+static int collapse4(const rc_bvh_node* nodes, int bin, std::vector<Node4>& out) {
+    int kids[4] = {nodes[bin].left_child, nodes[bin].right_child, -1, -1};
+    int n = 2;
+    while (n < 4) {
+        int best = -1;
+        float best_area = -1.0f;
+        for (int k = 0; k < n; ++k) {
+            const rc_bvh_node& c = nodes[kids[k]];
+            if (c.prim_count <= 0 && node_area(c) > best_area) {
+                best_area = node_area(c);
+                best = k;
+            }
+        }
+        if (best < 0) break;
+        const rc_bvh_node& c = nodes[kids[best]];
+        kids[best] = c.left_child;
+        kids[n++] = c.right_child;
+    }
+    const int self = (int)out.size();
+    out.push_back(Node4());
+    float lo[3][4], hi[3][4];
+    int ref[4], cnt[4];
+    for (int k = 0; k < 4; ++k) {
+        if (k < n) {
+            const rc_bvh_node& c = nodes[kids[k]];
+            for (int a = 0; a < 3; ++a) {
+                lo[a][k] = c.aabb_min[a];
+                hi[a][k] = c.aabb_max[a];
+            }
+            if (c.prim_count > 0) {
+                ref[k] = c.prim_start;
+                cnt[k] = c.prim_count;
+            } else {
+                ref[k] = collapse4(nodes, kids[k], out);
+                cnt[k] = 0;
+            }
+        } else {
+            for (int a = 0; a < 3; ++a) {
+                lo[a][k] = 0.0f;
+                hi[a][k] = 0.0f;
+            }
+            ref[k] = 0;
+            cnt[k] = -1;
+        }
+    }
+    Node4& w = out[self];
+    w.lox = make_float4(lo[0][0], lo[0][1], lo[0][2], lo[0][3]);
+    w.hix = make_float4(hi[0][0], hi[0][1], hi[0][2], hi[0][3]);
+    w.loy = make_float4(lo[1][0], lo[1][1], lo[1][2], lo[1][3]);
+    w.hiy = make_float4(hi[1][0], hi[1][1], hi[1][2], hi[1][3]);
+    w.loz = make_float4(lo[2][0], lo[2][1], lo[2][2], lo[2][3]);
+    w.hiz = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
+    w.ref = make_int4(ref[0], ref[1], ref[2], ref[3]);
+    w.cnt = make_int4(cnt[0], cnt[1], cnt[2], cnt[3]);
+    return self;
+}
+
+extern "C" {
 
 int rc_ctx_set_stream(rc_ctx* ctx, void* cuda_stream) {
     if (!ctx) return RC_ERR_INVALID_ARG;
@@ -388,6 +469,10 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
         r.d = make_int4(L.prim_count > 0 ? L.prim_start : n.left_child, L.prim_count,
                         R.prim_count > 0 ? R.prim_start : n.right_child, R.prim_count);
     }
+    // 4-wide copy for the fast build's traversal; a tree deeper than any SAH
+    // build makes keeps the binary traversal (the collapse recurses per level).
+    std::vector<Node4> wide;
+    if (tri_count > 0 && nodes[0].prim_count <= 0 && max_depth <= 256) collapse4(nodes, 0, wide);
     std::vector<float4> isect(3 * (size_t)tri_count), shade(3 * (size_t)tri_count);
     for (int i = 0; i < tri_count; ++i) {
         const rc_triangle& t = tris[i];
@@ -408,6 +493,8 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     CK(cudaSetDevice(ctx->device));
     CK(cudaStreamSynchronize(ctx->stream));  // buffers may be in use by queued work
     CK(ensure(ctx->nodes, recs.size() * sizeof(NodeRec)));
+    CK(ensure(ctx->nodes4, std::max<size_t>(sizeof(Node4), wide.size() * sizeof(Node4))));
+    if (!wide.empty()) CK(copy_h2d(ctx, ctx->nodes4.ptr, wide.data(), wide.size() * sizeof(Node4)));
     CK(ensure(ctx->tri_isect, std::max<size_t>(16, isect.size() * sizeof(float4))));
     CK(ensure(ctx->tri_shade, std::max<size_t>(16, shade.size() * sizeof(float4))));
     CK(ensure(ctx->mats, (size_t)material_count * sizeof(rc_material)));
@@ -425,6 +512,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     CK(cudaStreamSynchronize(ctx->stream));  // host staging vectors go out of scope
     DeviceScene& S = ctx->scene;
     S.nodes = (const NodeRec*)ctx->nodes.ptr;
+    S.nodes4 = wide.empty() ? nullptr : (const Node4*)ctx->nodes4.ptr;
     S.tri_isect = (const float4*)ctx->tri_isect.ptr;
     S.tri_shade = (const float4*)ctx->tri_shade.ptr;
     S.materials = (const float4*)ctx->mats.ptr;
@@ -460,27 +548,73 @@ static int launch_err(rc_ctx* ctx, cudaError_t e, const char* what) {
 
 int rc_set_engine(rc_ctx* ctx, int engine, int chunk_paths) {
     if (!ctx) return RC_ERR_INVALID_ARG;
-    if ((engine != RC_ENGINE_MEGAKERNEL && engine != RC_ENGINE_WAVEFRONT) || chunk_paths < 0)
+    if ((engine != RC_ENGINE_MEGAKERNEL && engine != RC_ENGINE_WAVEFRONT && engine != RC_ENGINE_WAVEFRONT_STATIC) ||
+        chunk_paths < 0)
         return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_engine: bad engine %d or chunk %d", engine, chunk_paths);
     ctx->engine = engine;
     ctx->chunk_paths = chunk_paths;
     return RC_OK;
 }
 
+static bool valid_block(int b) { return b == 0 || b == 64 || b == 128 || b == 256; }
+
+int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!t) return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_tuning: null tuning");
+    if ((t->engine != RC_ENGINE_MEGAKERNEL && t->engine != RC_ENGINE_WAVEFRONT &&
+         t->engine != RC_ENGINE_WAVEFRONT_STATIC) ||
+        t->chunk_paths < 0 || (t->wide_bvh & ~(RC_WIDE_PATHS | RC_WIDE_PHOTONS)) || !valid_block(t->trace_block) ||
+        !valid_block(t->shade_block) || !valid_block(t->photon_block))
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d", t->engine,
+                    t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block);
+    ctx->engine = t->engine;
+    ctx->chunk_paths = t->chunk_paths;
+    ctx->wide_bvh = t->wide_bvh;
+    ctx->trace_block = t->trace_block ? t->trace_block : 128;
+    ctx->shade_block = t->shade_block ? t->shade_block : 128;
+    ctx->photon_block = t->photon_block ? t->photon_block : 128;
+    return RC_OK;
+}
+
+int rc_get_tuning(rc_ctx* ctx, rc_tuning* out) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!out) return fail(ctx, RC_ERR_INVALID_ARG, "rc_get_tuning: null output");
+    out->engine = ctx->engine;
+    out->chunk_paths = ctx->chunk_paths;
+    out->wide_bvh = ctx->wide_bvh;
+    out->trace_block = ctx->trace_block;
+    out->shade_block = ctx->shade_block;
+    out->photon_block = ctx->photon_block;
+    return RC_OK;
+}
+
+// The scene as one class of rays sees it: without the 4-wide nodes unless the
+// context's wide_bvh bit for that class is set.
+static DeviceScene scene_for(const rc_ctx* ctx, int wide_bit) {
+    DeviceScene S = ctx->scene;
+    if (!(ctx->wide_bvh & wide_bit)) S.nodes4 = nullptr;
+    return S;
+}
+
 // Default wavefront chunk: every sample of the call, up to 16M paths.
 static const int kDefaultChunkPaths = 16 << 20;
 
-static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
-    const int W = ctx->width, H = ctx->height;
-    const int tiles_x = (W + 7) / 8, tiles_y = (H + 3) / 4;
-    const int npix = tiles_x * tiles_y * 32;
-    // the device decides LCA with the same float expression
-    const bool lca = (fabsf(R.cam.lca[0]) + fabsf(R.cam.lca[2])) > 1e-4f;
-    const int C = lca ? 3 : 1;
-    const long per_sample = (long)npix * C;
+// Paths in flight for a call of n_spp samples with or without lens channels.
+static long wavefront_capacity(const rc_ctx* ctx, int n_spp, bool lca, int* samples_per_chunk) {
+    const int tiles_x = (ctx->width + 7) / 8, tiles_y = (ctx->height + 3) / 4;
+    const long per_sample = (long)tiles_x * tiles_y * 32 * (lca ? 3 : 1);
     const long cap_paths = ctx->chunk_paths > 0 ? ctx->chunk_paths : kDefaultChunkPaths;
-    int ns = (int)std::max<long>(1, std::min<long>(R.n_spp, cap_paths / per_sample));
-    const long cap = per_sample * ns;
+    const int ns = (int)std::max<long>(1, std::min<long>(n_spp, cap_paths / per_sample));
+    if (samples_per_chunk) *samples_per_chunk = ns;
+    return per_sample * ns;
+}
+
+static bool lca_active(const CamParams& c) {
+    // the device decides LCA with the same float expression
+    return (fabsf(c.lca[0]) + fabsf(c.lca[2])) > 1e-4f;
+}
+
+static int wavefront_reserve(rc_ctx* ctx, long cap) {
     if (cap > ctx->wf_capacity) {
         CK(cudaStreamSynchronize(ctx->stream));
         const size_t n = (size_t)cap;
@@ -497,9 +631,23 @@ static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
         CK(ensure(ctx->wf_sq1, n * 4));
         CK(ensure(ctx->wf_srec0, n * 64));
         CK(ensure(ctx->wf_srec1, n * 64));
-        CK(ensure(ctx->wf_qlen, 4 * sizeof(unsigned int)));
+        CK(ensure(ctx->wf_qlen, 8 * sizeof(unsigned int)));
         ctx->wf_capacity = (int)cap;
     }
+    return RC_OK;
+}
+
+static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
+    const int W = ctx->width, H = ctx->height;
+    const int tiles_x = (W + 7) / 8, tiles_y = (H + 3) / 4;
+    const int npix = tiles_x * tiles_y * 32;
+    const bool lca = lca_active(R.cam);
+    const int C = lca ? 3 : 1;
+    const long per_sample = (long)npix * C;
+    int ns = 1;
+    const long cap = wavefront_capacity(ctx, R.n_spp, lca, &ns);
+    const int rr = wavefront_reserve(ctx, cap);
+    if (rr != RC_OK) return rr;
     WaveArgs A;
     A.scene = R.scene;
     A.img = R.img;
@@ -526,6 +674,7 @@ static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
     A.tiles_x = tiles_x;
     A.npix = npix;
     A.counters = R.counters;
+    A.dynamic_fetch = ctx->engine == RC_ENGINE_WAVEFRONT ? 1 : 0;
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
     for (int s0 = 0; s0 < R.n_spp; s0 += ns) {
         A.first_frame = R.first_frame + s0;
@@ -539,12 +688,14 @@ static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
         for (int b = 0; b <= 6; ++b) {
             A.bounce = b;
             e = timed_launch(ctx, RC_KERNEL_WF_TRACE, [&] {
-                return ex ? exact::launch_wf_trace(A, ctx->stream) : fast::launch_wf_trace(A, ctx->stream);
+                return ex ? exact::launch_wf_trace(A, ctx->stream, ctx->trace_block)
+                          : fast::launch_wf_trace(A, ctx->stream, ctx->trace_block);
             });
             if (e != cudaSuccess) return launch_err(ctx, e, "wavefront trace");
             if (b == 6) break;
             e = timed_launch(ctx, RC_KERNEL_WF_SHADE, [&] {
-                return ex ? exact::launch_wf_shade(A, ctx->stream) : fast::launch_wf_shade(A, ctx->stream);
+                return ex ? exact::launch_wf_shade(A, ctx->stream, ctx->shade_block)
+                          : fast::launch_wf_shade(A, ctx->stream, ctx->shade_block);
             });
             if (e != cudaSuccess) return launch_err(ctx, e, "wavefront shade");
         }
@@ -564,7 +715,7 @@ int rc_render(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, in
     if (n_spp == 0) return RC_OK;
     CK(cudaSetDevice(ctx->device));
     RenderArgs A;
-    A.scene = ctx->scene;
+    A.scene = scene_for(ctx, RC_WIDE_PATHS);
     A.img = ctx->img;
     A.cam = cam_params(cam);
     A.nee_enabled = settings->nee_enabled;
@@ -572,7 +723,7 @@ int rc_render(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, in
     A.first_frame = first_frame;
     A.n_spp = n_spp;
     A.counters = ctx->counters;
-    if (ctx->engine == RC_ENGINE_WAVEFRONT) {
+    if (ctx->engine == RC_ENGINE_WAVEFRONT || ctx->engine == RC_ENGINE_WAVEFRONT_STATIC) {
         const int r = wavefront_render(ctx, A);
         if (r != RC_OK) return r;
     } else {
@@ -629,12 +780,8 @@ static int check_sppm(rc_ctx* ctx, const rc_sppm_params* p) {
     return RC_OK;
 }
 
-int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
-    if (!ctx) return RC_ERR_INVALID_ARG;
-    int r = check_sppm(ctx, p);
-    if (r != RC_OK) return r;
-    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_sppm_trace: no scene uploaded");
-    CK(cudaSetDevice(ctx->device));
+// Sizes the photon map for `photons` photons and a hash of `hash_size` cells.
+static int photon_reserve(rc_ctx* ctx, const rc_sppm_params* p) {
     const int cap = p->photon_count > 0 ? p->photon_count : 1;
     if (cap > ctx->photon_cap || p->hash_size > ctx->hash_cap) CK(cudaStreamSynchronize(ctx->stream));
     if (cap > ctx->photon_cap) {
@@ -654,6 +801,16 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
         ctx->hash_cap = p->hash_size;
     }
     CK(ensure(ctx->counter, sizeof(unsigned int)));
+    return RC_OK;
+}
+
+int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    int r = check_sppm(ctx, p);
+    if (r != RC_OK) return r;
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_sppm_trace: no scene uploaded");
+    CK(cudaSetDevice(ctx->device));
+    if ((r = photon_reserve(ctx, p)) != RC_OK) return r;
     // PhotonMap.clear(): heads = -1, counter = 0
     CK(cudaMemsetAsync(ctx->heads.ptr, 0xff, (size_t)p->hash_size * sizeof(int), ctx->stream));
     CK(cudaMemsetAsync(ctx->counter.ptr, 0, sizeof(unsigned int), ctx->stream));
@@ -663,7 +820,7 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     ctx->last_photons = p->photon_count;
     if (p->photon_count == 0 || ctx->scene.light_count == 0) return RC_OK;
     PhotonArgs A;
-    A.scene = ctx->scene;
+    A.scene = scene_for(ctx, RC_WIDE_PHOTONS);
     A.photons = (float4*)ctx->photons.ptr;
     A.heads = (int*)ctx->heads.ptr;
     A.next = (int*)ctx->next.ptr;
@@ -682,7 +839,8 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     A.counters = ctx->counters;
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
     cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_TRACE, [&] {
-        return ex ? exact::launch_photon_trace(A, ctx->stream) : fast::launch_photon_trace(A, ctx->stream);
+        return ex ? exact::launch_photon_trace(A, ctx->stream, ctx->photon_block)
+                  : fast::launch_photon_trace(A, ctx->stream, ctx->photon_block);
     });
     if (e != cudaSuccess) return launch_err(ctx, e, "photon trace");
     e = timed_launch(ctx, RC_KERNEL_PHOTON_LAYOUT, [&] {
@@ -701,7 +859,7 @@ int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, f
         return fail(ctx, RC_ERR_INVALID_ARG, "rc_sppm_gather: no photon map traced with hash_size %d", p->hash_size);
     CK(cudaSetDevice(ctx->device));
     GatherArgs A;
-    A.scene = ctx->scene;
+    A.scene = scene_for(ctx, RC_WIDE_PHOTONS);
     A.img = ctx->img;
     A.cam = cam_params(cam);
     A.cell_start = (const unsigned int*)ctx->cell_start.ptr;
@@ -872,6 +1030,125 @@ int rc_reset_counters(rc_ctx* ctx) {
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemsetAsync(ctx->counters, 0, sizeof(DevCounters), ctx->stream));
     ctx->launches = ctx->h2d = ctx->d2h = 0;
+    return RC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched export frames (keyframed animations)
+// ---------------------------------------------------------------------------
+static uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+    const unsigned char* c = (const unsigned char*)p;
+    for (size_t i = 0; i < n; ++i) {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, const rc_settings* settings,
+                     const rc_sppm_params* sppm, float sppm_initial_radius, const rc_atrous_params* atrous,
+                     float* out_frames, int use_graph) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!frames || n_frames < 1 || !settings || !atrous)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_render_frames: bad arguments");
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_render_frames: no scene uploaded");
+    for (int f = 0; f < n_frames; ++f) {
+        const rc_frame_desc& d = frames[f];
+        if (d.spp < 1 || d.sppm_iterations < 0 || d.sppm_iterations > d.spp || (d.sppm_iterations > 0 && !sppm))
+            return fail(ctx, RC_ERR_INVALID_ARG, "rc_render_frames: frame %d: bad spp/iterations", f);
+    }
+    CK(cudaSetDevice(ctx->device));
+    const size_t px = (size_t)ctx->width * ctx->height;
+    // ---- reserve every buffer the sequence touches (no allocation may
+    //      happen while the stream is being captured) ----
+    long cap = 0;
+    bool any_sppm = false;
+    for (int f = 0; f < n_frames; ++f) {
+        const rc_frame_desc& d = frames[f];
+        const int it = d.sppm_iterations;
+        const int block = it > 0 ? (d.spp + it - 1) / it : d.spp;
+        cap = std::max(cap, wavefront_capacity(ctx, block, lca_active(cam_params(&d.camera)), nullptr));
+        any_sppm = any_sppm || (it > 0);
+    }
+    if (ctx->engine != RC_ENGINE_MEGAKERNEL) {
+        const int r = wavefront_reserve(ctx, cap);
+        if (r != RC_OK) return r;
+    }
+    if (any_sppm) {
+        int r = check_sppm(ctx, sppm);
+        if (r == RC_OK) r = photon_reserve(ctx, sppm);
+        if (r != RC_OK) return r;
+    }
+    CK(ensure(ctx->frames, (size_t)n_frames * px * sizeof(float4)));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // ---- the sequence ----
+    auto sequence = [&]() -> int {
+        for (int f = 0; f < n_frames; ++f) {
+            const rc_frame_desc& d = frames[f];
+            int r = rc_render_frame(ctx, &d.camera, settings, d.spp, sppm, sppm_initial_radius, d.sppm_iterations,
+                                    atrous, nullptr);
+            if (r != RC_OK) return r;
+            cudaError_t e = cudaMemcpyAsync((float4*)ctx->frames.ptr + (size_t)f * px, ctx->result,
+                                            px * sizeof(float4), cudaMemcpyDeviceToDevice, ctx->stream);
+            if (e != cudaSuccess) return fail(ctx, RC_ERR_CUDA, "frame copy: %s", cudaGetErrorString(e));
+        }
+        return RC_OK;
+    };
+    if (!use_graph) {
+        const int r = sequence();
+        if (r != RC_OK) return r;
+    } else {
+        uint64_t key = 1469598103934665603ull;
+        key = fnv1a(key, frames, sizeof(rc_frame_desc) * (size_t)n_frames);
+        key = fnv1a(key, settings, sizeof(*settings));
+        if (sppm) key = fnv1a(key, sppm, sizeof(*sppm));
+        key = fnv1a(key, &sppm_initial_radius, sizeof(float));
+        key = fnv1a(key, atrous, sizeof(*atrous));
+        key = fnv1a(key, &ctx->engine, sizeof(int));
+        key = fnv1a(key, &ctx->math_mode, sizeof(int));
+        key = fnv1a(key, &ctx->stream, sizeof(void*));
+        key = fnv1a(key, &ctx->frames.ptr, sizeof(void*));
+        if (!ctx->graph_exec || ctx->graph_key != key) {
+            if (ctx->graph_exec) {
+                cudaGraphExecDestroy(ctx->graph_exec);
+                ctx->graph_exec = nullptr;
+            }
+            const bool timing = ctx->timing;
+            ctx->timing = false;  // event pairs are not recorded into the graph
+            const unsigned long long launches0 = ctx->launches;
+            CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+            const int r = sequence();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+            ctx->timing = timing;
+            if (r != RC_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return r;
+            }
+            if (ec != cudaSuccess) return fail(ctx, RC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ec));
+            const cudaError_t ei = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (ei != cudaSuccess) {
+                ctx->graph_exec = nullptr;
+                return fail(ctx, RC_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(ei));
+            }
+            ctx->graph_key = key;
+            ctx->graph_launches = ctx->launches - launches0;
+            ctx->launches = launches0;
+            ctx->graph_total_samples = ctx->total_samples;
+            ctx->graph_radius = ctx->sppm_radius;
+            ctx->graph_iteration = ctx->sppm_iteration;
+        }
+        CK(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+        ctx->launches += ctx->graph_launches;
+        ctx->total_samples = ctx->graph_total_samples;
+        ctx->sppm_radius = ctx->graph_radius;
+        ctx->sppm_iteration = ctx->graph_iteration;
+    }
+    if (out_frames) {
+        CK(copy_d2h(ctx, out_frames, ctx->frames.ptr, (size_t)n_frames * px * sizeof(float4)));
+        return rc_synchronize(ctx);
+    }
     return RC_OK;
 }
 

@@ -514,17 +514,122 @@ DI bool traverse_ww(const DeviceScene& S, const Ray& r, float max_t, Guard& g, H
     }
     return h.prim >= 0;
 }
+
+DI void cswap(unsigned int& a, unsigned int& b) {
+    const unsigned int lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+
+// 4-wide traversal over Node4 (same leaf parking as traverse_ww).  The hit
+// children of a node are ordered by entry distance with a 5-comparator
+// network on keys (distance bits with the slot in the low two bits; misses
+// and empty slots, count < 0, sort last); the nearest is entered and the rest
+// pushed far to near.  Up to three pushes per level: the stack holds 96
+// entries, and a push that would overflow it raises RC_GUARD_TRAVERSAL_CAP.
+constexpr int kStack4 = 96;
+
+template <bool kAnyHit>
+DI bool traverse4(const DeviceScene& S, const Ray& r, float max_t, Guard& g, Hit& h) {
+    h.t = max_t;
+    h.prim = -1;
+    h.u = h.v = 0.0f;
+    float tmin;
+    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin) ||
+        tmin > h.t)
+        return false;
+    int2 stk[kStack4];
+    float stt[kStack4];
+    int top = 0;
+    TravNode node = {S.root_count > 0 ? S.root_ref : 0, S.root_count};
+    bool have_node = true;
+    TravNode leaf = {0, 0};
+    int steps = 0;
+    while (have_node || leaf.cnt > 0) {
+        while (have_node) {
+            if (node.cnt > 0) {
+                if (leaf.cnt > 0) break;
+                leaf = node;
+                have_node = pop_entry(stk, stt, top, h.t, node);
+            } else {
+                const Node4* n4 = S.nodes4 + node.ref;
+                const float4 lx = __ldg(&n4->lox), hx = __ldg(&n4->hix), ly = __ldg(&n4->loy);
+                const float4 hy = __ldg(&n4->hiy), lz = __ldg(&n4->loz), hz = __ldg(&n4->hiz);
+                const int4 cr = __ldg(&n4->ref), cc = __ldg(&n4->cnt);
+                float t[4];
+                unsigned int key[4];
+                const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
+                const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
+                const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+                const int CR[4] = {cr.x, cr.y, cr.z, cr.w}, CC[4] = {cc.x, cc.y, cc.z, cc.w};
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const bool hit = CC[k] >= 0 && tslab(g, r, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k], t[k]) &&
+                                     !(t[k] > h.t);
+                    const float tk = fmaxf(t[k], 0.0f);
+                    key[k] = hit ? ((__float_as_uint(tk) & ~3u) | (unsigned int)k) : 0xffffffffu;
+                }
+                cswap(key[0], key[1]);
+                cswap(key[2], key[3]);
+                cswap(key[0], key[2]);
+                cswap(key[1], key[3]);
+                cswap(key[1], key[2]);
+                if (key[0] == 0xffffffffu) {
+                    have_node = pop_entry(stk, stt, top, h.t, node);
+                } else {
+#pragma unroll
+                    for (int k = 3; k >= 1; --k) {
+                        if (key[k] != 0xffffffffu) {
+                            if (top < kStack4) {
+                                const int s = key[k] & 3u;
+                                stk[top] = make_int2(CR[s], CC[s]);
+                                stt[top++] = t[s];
+                            } else {
+                                g.flags |= RC_GUARD_TRAVERSAL_CAP;
+                            }
+                        }
+                    }
+                    const int s0 = key[0] & 3u;
+                    node.ref = CR[s0];
+                    node.cnt = CC[s0];
+                }
+            }
+            if (++steps > 2 * S.node_count + 64) {
+                g.flags |= RC_GUARD_TRAVERSAL_CAP;
+                return h.prim >= 0;
+            }
+            if (__all_sync(__activemask(), leaf.cnt > 0)) break;
+        }
+        if (leaf.cnt > 0) {
+            for (int i = leaf.ref; i < leaf.ref + leaf.cnt; ++i) {
+                float tt, u, v;
+                if (thit(g, r, S.tri_isect, i, tt, u, v) && tt < h.t) {
+                    if (kAnyHit) return true;
+                    h.t = tt;
+                    h.u = u;
+                    h.v = v;
+                    h.prim = i;
+                }
+            }
+            leaf.cnt = 0;
+        }
+    }
+    return h.prim >= 0;
+}
 #endif
 
 // Closest hit and visibility as used by the kernels: the reference's
-// traversal order in the exact build, the warp-cooperative one in the fast
-// build.
+// traversal order in the exact build; in the fast build the 4-wide
+// traversal when the scene has 4-wide nodes, else the binary one.
 DI Hit closest_hit(const DeviceScene& S, const Ray& r, Guard& g) {
 #if RC_EXACT
     return trace_closest(S, r, g);
 #else
     Hit h;
-    traverse_ww<false>(S, r, 1e30f, g, h);
+    if (S.nodes4)
+        traverse4<false>(S, r, 1e30f, g, h);
+    else
+        traverse_ww<false>(S, r, 1e30f, g, h);
     return h;
 #endif
 }
@@ -535,6 +640,7 @@ DI bool unoccluded(const DeviceScene& S, const Ray& r, float max_dist, Guard& g)
     return trace_shadow<kTestAtParent>(S, r, max_dist, g);
 #else
     Hit h;
+    if (S.nodes4) return !traverse4<true>(S, r, max_dist, g, h);
     return !traverse_ww<true>(S, r, max_dist, g, h);
 #endif
 }

@@ -34,8 +34,20 @@ struct NodeRec {
     int4 d;
 };
 
+// 4-wide node of the fast build's traversal (128 B, two cache lines): the
+// boxes of up to four children as SoA lanes, and per child (ref, count) with
+// ref a Node4 index when count == 0 and a primitive start otherwise.  Unused
+// slots have count -1 (and a zero box) and are never tested.
+// Built on the host by collapsing the reference's binary BVH; the triangles
+// and their order are unchanged.
+struct Node4 {
+    float4 lox, hix, loy, hiy, loz, hiz;
+    int4 ref, cnt;
+};
+
 struct DeviceScene {
     const NodeRec* nodes = nullptr;
+    const Node4* nodes4 = nullptr;       // root at index 0 unless the root is a leaf
     const float4* tri_isect = nullptr;   // 3 per triangle
     const float4* tri_shade = nullptr;   // 3 per triangle
     const float4* materials = nullptr;   // 4 per material
@@ -193,6 +205,7 @@ struct WaveArgs {
     int npix;          // tiles * 32
     int paths;         // npix * channels * n_samples
     int bounce;
+    int dynamic_fetch; // fast build: persistent trace kernel with ray refill
     DevCounters* counters;
 };
 

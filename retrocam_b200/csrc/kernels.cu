@@ -112,7 +112,7 @@ DI float fresnel_schlick(float cos_theta, float ior) {
 // appended with a warp-aggregated 32-bit atomicAdd on the counter and linked
 // into their cell with a 32-bit atomicExch on the cell head.
 template <bool kAtParent>
-__global__ void __launch_bounds__(128) photon_trace_kernel(PhotonArgs A) {
+__global__ void __launch_bounds__(256) photon_trace_kernel(PhotonArgs A) {
     const int gid = blockIdx.x * blockDim.x + threadIdx.x;
     const DeviceScene& S = A.scene;
     Guard g = {0u, 0u, 0u};
@@ -542,13 +542,14 @@ cudaError_t launch_render(const RenderArgs& A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s) {
-    const int blocks = (A.photon_count + 127) / 128;
+cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) {
+    const int b = block <= 64 ? 64 : (block <= 128 ? 128 : 256);
+    const int blocks = (A.photon_count + b - 1) / b;
     if (blocks == 0) return cudaSuccess;
     if (A.scene.depth <= 60)
-        photon_trace_kernel<true><<<blocks, 128, 0, s>>>(A);
+        photon_trace_kernel<true><<<blocks, b, 0, s>>>(A);
     else
-        photon_trace_kernel<false><<<blocks, 128, 0, s>>>(A);
+        photon_trace_kernel<false><<<blocks, b, 0, s>>>(A);
     return cudaGetLastError();
 }
 

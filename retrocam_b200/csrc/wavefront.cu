@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
 // Closest-hit traversal of ray queue rq[bounce&1] followed (same index
 // space) by the visibility tests of shadow queue sq[(bounce+1)&1].
 template <bool kShadowAtParent>
-__global__ void __launch_bounds__(128) wf_trace(WaveArgs A) {
+__global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const int cur = A.bounce & 1;
     const int prev = cur ^ 1;
@@ -138,7 +138,7 @@ __global__ void __launch_bounds__(128) wf_trace(WaveArgs A) {
 
 // One bounce of pathtrace.comp's traceRadiance for every path in ray queue
 // rq[bounce&1] whose closest hit wf_trace has stored.
-__global__ void __launch_bounds__(128) wf_shade(WaveArgs A) {
+__global__ void __launch_bounds__(256) wf_shade(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
     const int cur = A.bounce & 1;
@@ -146,6 +146,7 @@ __global__ void __launch_bounds__(128) wf_shade(WaveArgs A) {
     const int b = A.bounce;
     const bool last = b == 5;
     const unsigned int n = B.qlen[cur];
+    if (blockIdx.x == 0 && threadIdx.x == 0) B.qlen[4] = 0u;  // work counter of the next trace
     uint32_t hits = 0, lights = 0;
     for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int p = B.rq[cur][i];
@@ -418,41 +419,241 @@ static int grid_for(const void* fn, int block) {
     return sms * (per > 0 ? per : 1);
 }
 
+#if !RC_EXACT
+// Persistent trace with dynamic ray fetch (fast build).  Each lane owns one
+// ray at a time and advances it one traversal step per loop iteration: an
+// interior node, parking a reached leaf, or the triangles of a parked leaf
+// (taken together once every busy lane of the warp has parked one).  When
+// fewer than kRefill lanes are still busy, the idle lanes take the next rays
+// from the work counter (one atomicAdd per warp), so a warp is not held by
+// its slowest ray.  Same rays and results as wf_trace; only the schedule
+// differs.
+constexpr int kRefill = 20;
+
+struct LaneRay {
+    Ray r;
+    Hit h;
+    TravNode node, leaf;
+    bool have_node;
+    bool any;      // shadow ray
+    int item;      // work index, -1 idle, -2 no more work
+    int top;
+};
+
+__global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
+    const WaveBuffers& B = A.wb;
+    const DeviceScene& S = A.scene;
+    const int cur = A.bounce & 1;
+    const int prev = cur ^ 1;
+    const unsigned int nr = A.bounce < 6 ? B.qlen[cur] : 0u;
+    const unsigned int ns = B.qlen[2 + prev];
+    const unsigned int total = nr + ns;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        B.qlen[prev] = 0u;
+        B.qlen[2 + cur] = 0u;
+    }
+    const unsigned int FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    Guard g = {0u, 0u, 0u};
+    uint32_t closest = 0, shadow = 0;
+    int2 stk[64];
+    float stt[64];
+    LaneRay L;
+    L.item = -1;
+    L.top = 0;
+    L.have_node = false;
+    L.leaf.cnt = 0;
+    L.any = false;
+    int steps = 0;
+    while (true) {
+        // ---- refill idle lanes ----
+        const unsigned int idle = __ballot_sync(FULL, L.item == -1);
+        if (idle) {
+            const int leader = __ffs(idle) - 1;
+            unsigned int base = 0;
+            if (lane == leader) base = atomicAdd(B.qlen + 4, (unsigned int)__popc(idle));
+            base = __shfl_sync(FULL, base, leader);
+            if (L.item == -1) {
+                const unsigned int i = base + __popc(idle & ((1u << lane) - 1u));
+                L.item = i < total ? (int)i : -2;
+                if (L.item >= 0) {
+                    float tmax = 1e30f;
+                    if ((unsigned int)L.item < nr) {
+                        const int p = B.rq[cur][L.item];
+                        L.r = make_ray(xyz(B.o[p]), xyz(B.d[p]));
+                        L.any = false;
+                        ++closest;
+                    } else {
+                        const float4* rec = B.srec[prev] + 4 * (L.item - (int)nr);
+                        const float4 so = rec[0], sd = rec[1];
+                        L.r = make_ray(xyz(so), xyz(sd));
+                        tmax = so.w;
+                        L.any = true;
+                        ++shadow;
+                    }
+                    L.h.t = tmax;
+                    L.h.prim = -1;
+                    L.h.u = L.h.v = 0.0f;
+                    L.top = 0;
+                    L.leaf.cnt = 0;
+                    L.node.ref = S.root_ref;
+                    L.node.cnt = S.root_count;
+                    float tmin;
+                    L.have_node = tslab(g, L.r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0],
+                                        S.root_max[1], S.root_max[2], tmin) && !(tmin > L.h.t);
+                    steps = 0;
+                }
+            }
+        }
+        if (__all_sync(FULL, L.item == -2)) break;
+        // ---- advance the rays ----
+        while (true) {
+            bool busy = L.item >= 0;
+            const unsigned int act = __ballot_sync(FULL, busy);
+            const unsigned int parked = __ballot_sync(FULL, busy && L.leaf.cnt > 0);
+            if (busy) {
+                bool done = false;
+                const bool do_leaf = L.leaf.cnt > 0 && (parked == act || !L.have_node || L.node.cnt > 0);
+                if (do_leaf) {
+                    for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
+                        float t, u, v;
+                        if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
+                            L.h.t = t;
+                            L.h.u = u;
+                            L.h.v = v;
+                            L.h.prim = i;
+                            if (L.any) {
+                                done = true;
+                                break;
+                            }
+                        }
+                    }
+                    L.leaf.cnt = 0;
+                } else if (L.have_node) {
+                    if (L.node.cnt > 0) {
+                        L.leaf = L.node;
+                        L.have_node = pop_entry(stk, stt, L.top, L.h.t, L.node);
+                    } else {
+                        const NodeRec* nrec = S.nodes + L.node.ref;
+                        const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
+                        const int4 d = __ldg(&nrec->d);
+                        float tl, tr;
+                        const bool hl = tslab(g, L.r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > L.h.t);
+                        const bool hr = tslab(g, L.r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > L.h.t);
+                        if (hl && hr) {
+                            const bool left_first = tl < tr;
+                            if (L.top < 62) {
+                                stk[L.top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
+                                stt[L.top++] = left_first ? tr : tl;
+                            }
+                            L.node.ref = left_first ? d.x : d.z;
+                            L.node.cnt = left_first ? d.y : d.w;
+                        } else if (hl) {
+                            L.node.ref = d.x;
+                            L.node.cnt = d.y;
+                        } else if (hr) {
+                            L.node.ref = d.z;
+                            L.node.cnt = d.w;
+                        } else {
+                            L.have_node = pop_entry(stk, stt, L.top, L.h.t, L.node);
+                        }
+                    }
+                }
+                if (!L.have_node && L.leaf.cnt == 0) done = true;
+                if (++steps > 4 * S.node_count + 64) {
+                    g.flags |= RC_GUARD_TRAVERSAL_CAP;
+                    done = true;
+                }
+                if (done) {
+                    const int item = L.item;
+                    if ((unsigned int)item < nr) {
+                        const int p = B.rq[cur][item];
+                        B.hit[p] = make_float4(L.h.t, L.h.u, L.h.v, __int_as_float(L.h.prim));
+                    } else {
+                        const float4* rec = B.srec[prev] + 4 * (item - (int)nr);
+                        const float4 sd = rec[1], st = rec[2], sl = rec[3];
+                        const int p = __float_as_int(sd.w);
+                        const bool vis = L.h.prim < 0;
+                        const float3 Lc = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
+                        const float3 rr = xyz(B.rad[p]) + xyz(st) * Lc;
+                        B.rad[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
+                        if (__float_as_int(st.w) != 0) B.res[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
+                    }
+                    L.item = -1;
+                    busy = false;
+                }
+            }
+            const unsigned int still = __ballot_sync(FULL, busy);
+            if (__popc(still) < kRefill) break;
+        }
+    }
+    const unsigned int c = __reduce_add_sync(FULL, closest);
+    const unsigned int s = __reduce_add_sync(FULL, shadow);
+    const unsigned int n = __reduce_add_sync(FULL, g.nodes);
+    const unsigned int t = __reduce_add_sync(FULL, g.tris);
+    const unsigned int gf = __reduce_or_sync(FULL, g.flags);
+    if (lane == 0) {
+        if (c) atomicAdd(&A.counters->closest_rays, (unsigned long long)c);
+        if (s) atomicAdd(&A.counters->shadow_rays, (unsigned long long)s);
+        if (n) atomicAdd(&A.counters->node_tests, (unsigned long long)n);
+        if (t) atomicAdd(&A.counters->tri_tests, (unsigned long long)t);
+        if (gf) atomicOr(&A.counters->error_word, gf);
+    }
+}
+#endif
+
 // Launchers; the chunk sequence (generate, 7 x trace, 6 x shade interleaved,
 // accumulate) is driven from api.cu so each launch can be timed.  Grids are
-// sized once to fill every SM (grid-stride kernels).
+// sized to fill every SM (grid-stride and persistent kernels), once per
+// kernel and block size (64, 128 or 256 threads).
 struct WfGrids {
-    int gen = 0, trace0 = 0, trace1 = 0, shade = 0, acc = 0;
+    int gen = 0, acc = 0;
+    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, dyn[3] = {};
 };
+static int block_class(int block) { return block <= 64 ? 0 : (block <= 128 ? 1 : 2); }
 static WfGrids& grids() {
     static WfGrids g;
     if (!g.gen) {
         g.gen = grid_for((const void*)wf_generate, 256);
-        g.trace0 = grid_for((const void*)wf_trace<false>, 128);
-        g.trace1 = grid_for((const void*)wf_trace<true>, 128);
-        g.shade = grid_for((const void*)wf_shade, 128);
         g.acc = grid_for((const void*)wf_accumulate, 128);
+        for (int c = 0; c < 3; ++c) {
+            const int b = 64 << c;
+            g.trace0[c] = grid_for((const void*)wf_trace<false>, b);
+            g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
+            g.shade[c] = grid_for((const void*)wf_shade, b);
+#if !RC_EXACT
+            g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
+#endif
+        }
     }
     return g;
 }
 
 cudaError_t launch_wf_generate(const WaveArgs& A, cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(A.wb.qlen, 0, 4 * sizeof(unsigned int), s);
+    cudaError_t e = cudaMemsetAsync(A.wb.qlen, 0, 8 * sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
     wf_generate<<<grids().gen, 256, 0, s>>>(A);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s) {
+cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
+    const int c = block_class(block), b = 64 << c;
+#if !RC_EXACT
+    if (A.dynamic_fetch) {
+        wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
+        return cudaGetLastError();
+    }
+#endif
     if (A.scene.depth <= 28)
-        wf_trace<true><<<grids().trace1, 128, 0, s>>>(A);
+        wf_trace<true><<<grids().trace1[c], b, 0, s>>>(A);
     else
-        wf_trace<false><<<grids().trace0, 128, 0, s>>>(A);
+        wf_trace<false><<<grids().trace0[c], b, 0, s>>>(A);
     return cudaGetLastError();
 }
 
-cudaError_t launch_wf_shade(const WaveArgs& A, cudaStream_t s) {
-    wf_shade<<<grids().shade, 128, 0, s>>>(A);
+cudaError_t launch_wf_shade(const WaveArgs& A, cudaStream_t s, int block) {
+    const int c = block_class(block);
+    wf_shade<<<grids().shade[c], 64 << c, 0, s>>>(A);
     return cudaGetLastError();
 }
 

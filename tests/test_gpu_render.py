@@ -24,7 +24,7 @@ def _scene(product, orc, workload):
     return w, sc, cam
 
 
-ENGINES = ("megakernel", "wavefront", "wavefront_small_chunks")
+ENGINES = ("megakernel", "wavefront", "wavefront_small_chunks", "wavefront_static")
 
 
 def _ctx(product, W, H, mode, engine="wavefront"):
@@ -33,9 +33,98 @@ def _ctx(product, W, H, mode, engine="wavefront"):
         ctx.set_engine(product.RC_ENGINE_MEGAKERNEL)
     elif engine == "wavefront_small_chunks":
         ctx.set_engine(product.RC_ENGINE_WAVEFRONT, 5000)   # several chunks per call
+    elif engine == "wavefront_static":
+        ctx.set_engine(product.RC_ENGINE_WAVEFRONT_STATIC)
     else:
         ctx.set_engine(product.RC_ENGINE_WAVEFRONT)
     return ctx
+
+
+def test_fast_dynamic_fetch_matches_static_schedule(product, c1):
+    """The persistent refill trace (fast build) visits the same rays as the
+    grid-stride one; only exact ties between triangles may resolve another
+    way, so almost every pixel is bit-identical."""
+    w, sc, cam = c1
+    out = []
+    for engine in ("wavefront", "wavefront_static"):
+        with _ctx(product, 160, 90, product.RC_MATH_FAST, engine) as ctx:
+            ctx.upload(sc)
+            ctx.render(cam, (1, 1.0), 0, 4)
+            out.append(ctx.read_buffers()[0])
+            assert ctx.counters()["error_word"] == 0
+    same = np.all(bits(out[0]) == bits(out[1]), axis=-1).mean()
+    assert same > 0.995, same
+
+
+def test_tuning_roundtrip_and_validation(product):
+    with product.Context(64, 64, 0, product.RC_MATH_FAST) as ctx:
+        t = ctx.tuning()
+        assert t == {"engine": product.RC_ENGINE_WAVEFRONT, "chunk_paths": 0, "wide_bvh": 0,
+                     "trace_block": 128, "shade_block": 128, "photon_block": 128}
+        ctx.set_tuning(engine=product.RC_ENGINE_WAVEFRONT_STATIC, wide_bvh=3, trace_block=256, shade_block=64)
+        t = ctx.tuning()
+        assert (t["engine"], t["wide_bvh"], t["trace_block"], t["shade_block"]) == (2, 3, 256, 64)
+        for bad in ({"engine": 7}, {"chunk_paths": -1}, {"wide_bvh": 4}, {"trace_block": 96},
+                    {"photon_block": 512}):
+            with pytest.raises(product.RetroCamError) as e:
+                ctx.set_tuning(**bad)
+            assert e.value.code == product.RC_ERR_INVALID_ARG
+        assert ctx.tuning() == t   # a rejected call changes nothing
+
+
+def test_exact_results_independent_of_tuning(product, orc, c1):
+    """Exact math walks the binary tree in the reference's order whatever the
+    knobs say, so every launch shape gives the oracle's bits."""
+    w, sc, cam = c1
+    W, H = 96, 64
+    cpu, _ = orc.render(sc, cam, (1, 1.0), W, H, 0, 2)
+    for knobs in ({"wide_bvh": 3, "trace_block": 64, "shade_block": 256},
+                  {"engine": product.RC_ENGINE_WAVEFRONT_STATIC, "trace_block": 256, "shade_block": 64},
+                  {"engine": product.RC_ENGINE_MEGAKERNEL, "wide_bvh": 3}):
+        with product.Context(W, H, 0, product.RC_MATH_EXACT) as ctx:
+            ctx.set_tuning(**knobs)
+            ctx.upload(sc)
+            ctx.render(cam, (1, 1.0), 0, 2)
+            _same_images(ctx.read_buffers(), cpu)
+
+
+@pytest.mark.parametrize("engine", ("megakernel", "wavefront", "wavefront_static"))
+def test_fast_wide_bvh_matches_binary(product, c1, engine):
+    """The 4-wide traversal finds the same nearest triangle as the binary one
+    (ties between triangles at one distance aside), so nearly every pixel is
+    bit-identical; block sizes change nothing."""
+    w, sc, cam = c1
+    out = []
+    for wide, block in ((0, 128), (product.RC_WIDE_PATHS, 128), (product.RC_WIDE_PATHS, 256), (0, 64)):
+        with _ctx(product, 160, 90, product.RC_MATH_FAST, engine) as ctx:
+            ctx.set_tuning(wide_bvh=wide, trace_block=block, shade_block=block)
+            ctx.upload(sc)
+            ctx.render(cam, (1, 1.0), 0, 4)
+            out.append(ctx.read_buffers()[0])
+            assert ctx.counters()["error_word"] == 0
+    for o in out[1:]:
+        same = np.all(bits(o) == bits(out[0]), axis=-1).mean()
+        assert same > 0.995, same
+
+
+def test_fast_wide_bvh_photon_map(product, c1):
+    """Photon trace through the 4-wide tree stores the same photons as
+    through the binary tree (compared as sorted records)."""
+    w, sc, cam = c1
+    maps = []
+    for wide in (0, product.RC_WIDE_PHOTONS):
+        with product.Context(64, 64, 0, product.RC_MATH_FAST) as ctx:
+            ctx.set_tuning(wide_bvh=wide, photon_block=64 if wide else 256)
+            ctx.upload(sc)
+            ctx.sppm_reset(0.02)
+            ctx.sppm_trace(200_000, 1 << 18)
+            ph, heads, nxt, n = ctx.read_photon_map(200_000, 1 << 18)
+            maps.append(_photon_records(ph, n))
+            assert ctx.counters()["error_word"] == 0
+    a, b = maps
+    assert abs(len(a) - len(b)) <= max(2, len(a) // 1000)
+    k = min(len(a), len(b))
+    assert np.mean(np.all(bits(a[:k]) == bits(b[:k]), axis=-1)) > 0.99
 
 
 @pytest.fixture(scope="module")
@@ -125,7 +214,7 @@ def test_render_nee_off_and_clamp(product, orc, c1, engine):
         _same_images(gpu, cpu)
 
 
-@pytest.mark.parametrize("engine", ENGINES[:2])
+@pytest.mark.parametrize("engine", ("megakernel", "wavefront", "wavefront_static"))
 def test_render_fast_close_to_oracle(product, orc, c1, engine):
     """Fast math reorders rounding, so a few paths take another branch; the
     per-pixel check is statistical and the image mean must agree."""
