@@ -85,7 +85,9 @@ def parse_args(argv=None):
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="export_frame")
     ap.add_argument("--math", default="fast", choices=["fast", "exact"])
-    ap.add_argument("--engine", default="wavefront", choices=["wavefront", "megakernel"])
+    ap.add_argument("--engine", default="auto", choices=["auto", "wavefront", "wavefront_static", "megakernel"],
+                    help="auto: the autotuner's launch shape for this GPU and workload (cached)")
+    ap.add_argument("--retune", action="store_true", help="with --engine auto: tune again, ignore the cache")
     ap.add_argument("--chunk-paths", type=int, default=0, help="wavefront paths in flight (0: default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
@@ -380,8 +382,6 @@ def run_b200(args):
     cam = api.workload_camera(w)
     mode = api.RC_MATH_EXACT if args.math == "exact" else api.RC_MATH_FAST
     ctx = api.Context(w.width, w.height, local_rank, mode)
-    ctx.set_engine(api.RC_ENGINE_WAVEFRONT if args.engine == "wavefront" else api.RC_ENGINE_MEGAKERNEL,
-                   args.chunk_paths)
     stream = torch.cuda.Stream(device=device)
     ctx.set_stream(stream.cuda_stream)
     ctx.upload(sc)
@@ -389,6 +389,16 @@ def run_b200(args):
     iters = w.sppm.iterations if w.sppm is not None else 0
     r0 = w.sppm.r0 if w.sppm is not None else 0.05
     samples_per_step = w.width * w.height * w.spp
+    if args.engine == "auto":
+        from retrocam_b200 import autotune
+        key = autotune.cache_key(torch.cuda.get_device_name(device), w.width, w.height, mode,
+                                 autotune.scene_signature(sc))
+        autotune.tuned(ctx, key, lambda: ctx.render_frame(cam, settings, w.spp, sppm, r0, iters, atrous,
+                                                          read=False), retune=args.retune)
+    else:
+        ctx.set_engine({"wavefront": api.RC_ENGINE_WAVEFRONT, "wavefront_static": api.RC_ENGINE_WAVEFRONT_STATIC,
+                        "megakernel": api.RC_ENGINE_MEGAKERNEL}[args.engine], args.chunk_paths)
+    tuning = ctx.tuning()
 
     def step(read=False, out=None):
         if out is None:
@@ -468,7 +478,7 @@ def run_b200(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, no dataset)",
-        "config": workload_config(w, args),
+        "config": dict(workload_config(w, args), tuning=tuning),
         "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
