@@ -165,7 +165,8 @@ typedef struct rc_counters {
 #define RC_KERNEL_WF_SHADE 7       /* wavefront: one bounce of shading + NEE sample */
 #define RC_KERNEL_WF_ACCUMULATE 8  /* wavefront: in-order accumulation, G-buffer */
 #define RC_KERNEL_PHOTON_LAYOUT 9  /* photon map: cell scan, scatter, heads/next */
-#define RC_KERNEL_KINDS 10
+#define RC_KERNEL_KPCNN 10         /* learned denoiser: features, 4 convolutions, filter */
+#define RC_KERNEL_KINDS 11
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
@@ -200,6 +201,7 @@ typedef struct rc_tuning {
 #define RC_GUARD_BAD_INDEX 0x2u      /* a node/primitive/material index was out of range */
 #define RC_GUARD_CHAIN_CAP 0x4u      /* reserved: gather chain cap (512) is a
                                         reference semantic, not an error */
+#define RC_GUARD_MMA_WAIT 0x8u       /* a tensor-core kernel's bounded wait gave up */
 
 /* Math modes of the kernels. */
 #define RC_MATH_FAST 0   /* FMA contraction, CUDA intrinsics; checked by tolerance */
@@ -408,6 +410,55 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames,
                      const rc_settings* settings, const rc_sppm_params* sppm,
                      float sppm_initial_radius, const rc_atrous_params* atrous,
                      float* out_frames, int use_graph);
+
+/* ---------------------------------------------------------------------------
+ * Learned denoiser (kernel-predicting CNN).  No counterpart in the
+ * reference, which has only the à-trous filter; the entry point sits beside
+ * rc_denoise_atrous (post/AtrousDenoiser.java:60) with the same inputs.
+ *
+ * Network: features (log1p radiance, albedo, normal, depth t/(1+t); 10
+ * channels padded to 16) -> 3 x [conv3x3 32 ch + ReLU] -> conv3x3 head of 25
+ * logits -> per-pixel softmax -> 5x5 filter (edge clamped) of the mean
+ * radiance.  BF16 weights and activations, FP32 accumulation (tcgen05).
+ *
+ * Parameters are one FP32 vector of RC_KPCNN_PARAMS floats: for layers 1, 2,
+ * 3 and the head in turn, W[tap][co][ci] (tap = 3*dy + dx over the 3x3
+ * window, co < 32, ci < 16 for layer 1 and < 32 otherwise; head co >= 25 and
+ * layer-1 ci >= 10 must be zero) followed by bias[32].
+ * ------------------------------------------------------------------------- */
+#define RC_KPCNN_PARAMS 32384
+
+typedef struct rc_kpcnn {
+    const float* params;   /* host, RC_KPCNN_PARAMS floats */
+    int32_t param_count;   /* must equal RC_KPCNN_PARAMS */
+} rc_kpcnn;
+
+/* Denoises the context's current accumulation (accum / N with the G-buffer
+ * and albedo as features) into the context's output frame; copies it to
+ * out_rgba (W*H*4 floats) when non-NULL.  Uploads the parameters each call. */
+int rc_denoise_learned(rc_ctx* ctx, const rc_kpcnn* weights, float* out_rgba);
+
+/* Building blocks on caller-owned DEVICE buffers (training and tests), on
+ * the given CUDA stream (NULL = legacy default).  Layouts as in kpcnn.cu:
+ * NHWC bf16 activations (16 or 32 channels), packed bf16 weights
+ * [tap][ci/8][co][8], float4 radiance.  `err` is a device word that
+ * receives a nonzero bit when a kernel's bounded wait gave up. */
+int rc_kp_conv3x3(const void* in, int cin, const void* wpk, const float* bias, void* out, int out_f32,
+                  int relu, const void* mask, int n, int h, int w, unsigned int* err, void* stream);
+int rc_kp_wgrad(const void* x, int cin, const void* dy, float* dw, float* db, int n, int h, int w,
+                unsigned int* err, void* stream);
+int rc_kp_head(const float* logits, const void* color, const void* target, void* out, void* dlogits,
+               double* loss, float grad_scale, int n, int h, int w, void* stream);
+/* packed7: w1, w2, w3, head (forward) and w2, w3, head (backward-data). */
+int rc_kp_pack(const float* params, void* const* packed7, void* stream);
+int rc_kp_adam(float* params, float* grads, float* m, float* v, int count, float lr, float beta1, float beta2,
+               float eps, int step, void* stream);
+int rc_kp_crop(const void* feat_all, const void* color_all, const void* target_all, const int* src,
+               const int* tgt, const int* oy, const int* ox, int batch, int H, int W, int size, void* feat,
+               void* color, void* target, void* stream);
+/* The network input of the context's current images: feat (W*H*16 bf16)
+ * and mean radiance (W*H float4), device buffers, on the context's stream. */
+int rc_kp_features(rc_ctx* ctx, void* feat, void* color);
 
 /* ---------------------------------------------------------------------------
  * Read-back and counters

@@ -93,7 +93,7 @@ class rc_counters(C.Structure):
 
 
 KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",
-                "wf_shade", "wf_accumulate", "photon_layout")
+                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn")
 RC_ENGINE_MEGAKERNEL = 0
 RC_ENGINE_WAVEFRONT = 1
 RC_ENGINE_WAVEFRONT_STATIC = 2
@@ -141,7 +141,22 @@ _SIGNATURES = {
     "rc_read_photon_map": (_I, [_VP, _VP, _I, _VP, _I, _VP, _VP]),
     "rc_get_counters": (_I, [_VP, _VP]),
     "rc_reset_counters": (_I, [_VP]),
+    "rc_denoise_learned": (_I, [_VP, _VP, _VP]),
+    "rc_kp_features": (_I, [_VP, _VP, _VP]),
+    "rc_kp_conv3x3": (_I, [_VP, _I, _VP, _VP, _VP, _I, _I, _VP, _I, _I, _I, _VP, _VP]),
+    "rc_kp_wgrad": (_I, [_VP, _I, _VP, _VP, _VP, _I, _I, _I, _VP, _VP]),
+    "rc_kp_head": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _F, _I, _I, _I, _VP]),
+    "rc_kp_pack": (_I, [_VP, _VP, _VP]),
+    "rc_kp_adam": (_I, [_VP, _VP, _VP, _VP, _I, _F, _F, _F, _F, _I, _VP]),
+    "rc_kp_crop": (_I, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I, _I, _I, _I, _VP, _VP, _VP, _VP]),
 }
+
+RC_KPCNN_PARAMS = 32384
+RC_GUARD_MMA_WAIT = 0x8
+
+
+class rc_kpcnn(C.Structure):
+    _fields_ = [("params", C.c_void_p), ("param_count", C.c_int32)]
 
 _lib = None
 
@@ -326,6 +341,18 @@ class Context:
         out = np.zeros((self.height, self.width, 4), np.float32) if read else None
         self.check(lib().rc_denoise_atrous(self.h, C.byref(params), _p(out)))
         return out
+
+    def denoise_learned(self, params: np.ndarray, read=True):
+        """rc_denoise_learned with a float32 parameter vector (RC_KPCNN_PARAMS)."""
+        params = np.ascontiguousarray(params, np.float32)
+        out = np.zeros((self.height, self.width, 4), np.float32) if read else None
+        w = rc_kpcnn(params.ctypes.data, params.size)
+        self.check(lib().rc_denoise_learned(self.h, C.byref(w), _p(out)))
+        return out
+
+    def kp_features(self, feat_ptr: int, color_ptr: int):
+        """Network input of the current images into device buffers."""
+        self.check(lib().rc_kp_features(self.h, C.c_void_p(feat_ptr), C.c_void_p(color_ptr)))
 
     def render_frame(self, cam, settings, spp, sppm: rc_sppm_params | None, r0, sppm_iters,
                      atrous: rc_atrous_params, read=True):

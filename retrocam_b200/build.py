@@ -3,6 +3,8 @@
   kernels.cu  x2  -DRC_EXACT=1 -fmad=false  (bit-exact math, rc::exact)
                   -DRC_EXACT=0              (fast math, rc::fast)
   api.cu          C ABI, device half
+  noalloc.cu      allocation-free à-trous entry point
+  kpcnn.cu        learned denoiser (tcgen05 BF16 convolutions)
   host_scene.cpp  C ABI, host half (-ffp-contract=off: Java float rules)
 
 The CUDA runtime is linked statically so the library needs only the driver.
@@ -67,7 +69,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 o = os.path.join(BUILD, f"{src}_{name.split('_')[1]}.o")
                 _run(common + flags + ["-c", os.path.join(CSRC, src + ".cu"), "-o", o], log)
                 objs.append(o)
-        for name in ("api", "noalloc"):
+        for name in ("api", "noalloc", "kpcnn"):
             o = os.path.join(BUILD, name + ".o")
             _run(common + ["-c", os.path.join(CSRC, name + ".cu"), "-o", o], log)
             objs.append(o)

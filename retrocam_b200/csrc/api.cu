@@ -4,6 +4,7 @@
 // uploaded scene in the kernels' layout (device_scene.h), the SPPM photon map
 // and a block of device counters.  Calls are asynchronous on the context's
 // stream unless they return data to the host.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>
@@ -43,6 +44,14 @@ cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace fast
+namespace kp {
+cudaError_t launch_features(const float4* accum, const ushort4* gbuf, const ushort4* galb, __nv_bfloat16* feat,
+                            float4* color, int count, cudaStream_t s);
+size_t packed_bytes();
+cudaError_t run_inference(const float* params, void* packed, const float4* accum, const ushort4* gbuf,
+                          const ushort4* galb, void* feat, void* act0, void* act1, float* logits, float4* color,
+                          float4* out, int W, int H, unsigned int* err, cudaStream_t s);
+}  // namespace kp
 }  // namespace rc
 
 using namespace rc;
@@ -96,6 +105,8 @@ struct rc_ctx {
     int wf_capacity = 0;
     // batched frames (rc_render_frames) and their captured graph
     DevBuf frames;
+    // learned denoiser scratch
+    DevBuf kp_feat, kp_act0, kp_act1, kp_logits, kp_color, kp_params, kp_packed;
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_key = 0;
     unsigned long long graph_launches = 0;
@@ -270,7 +281,9 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw, &ctx->seg_powyz,
                       &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
                       &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
-                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->frames})
+                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->frames,
+                      &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
+                      &ctx->kp_params, &ctx->kp_packed})
         release(*b);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -924,6 +937,49 @@ int rc_denoise_atrous(rc_ctx* ctx, const rc_atrous_params* p, float* out_rgba) {
         });
         if (e != cudaSuccess) return launch_err(ctx, e, "normalize");
     }
+    ctx->result = ctx->out;
+    if (out_rgba) return rc_read_output(ctx, out_rgba);
+    return RC_OK;
+}
+
+int rc_kp_features(rc_ctx* ctx, void* feat, void* color) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!feat || !color) return fail(ctx, RC_ERR_INVALID_ARG, "rc_kp_features: null buffer");
+    CK(cudaSetDevice(ctx->device));
+    const cudaError_t e = timed_launch(ctx, RC_KERNEL_KPCNN, [&] {
+        return kp::launch_features(ctx->img.accum, ctx->img.gbuf, ctx->img.galb, static_cast<__nv_bfloat16*>(feat),
+                                   static_cast<float4*>(color), ctx->width * ctx->height, ctx->stream);
+    });
+    if (e != cudaSuccess) return launch_err(ctx, e, "kpcnn features");
+    return RC_OK;
+}
+
+int rc_denoise_learned(rc_ctx* ctx, const rc_kpcnn* weights, float* out_rgba) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (!weights || !weights->params || weights->param_count != RC_KPCNN_PARAMS)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_denoise_learned: need %d parameters", RC_KPCNN_PARAMS);
+    CK(cudaSetDevice(ctx->device));
+    const size_t px = (size_t)ctx->width * ctx->height;
+    if (ctx->kp_params.bytes < RC_KPCNN_PARAMS * sizeof(float) || ctx->kp_logits.bytes < px * 128)
+        CK(cudaStreamSynchronize(ctx->stream));
+    CK(ensure(ctx->kp_feat, px * 32));
+    CK(ensure(ctx->kp_act0, px * 64));
+    CK(ensure(ctx->kp_act1, px * 64));
+    CK(ensure(ctx->kp_logits, px * 128));
+    CK(ensure(ctx->kp_color, px * 16));
+    CK(ensure(ctx->kp_params, RC_KPCNN_PARAMS * sizeof(float)));
+    CK(ensure(ctx->kp_packed, kp::packed_bytes()));
+    CK(copy_h2d(ctx, ctx->kp_params.ptr, weights->params, RC_KPCNN_PARAMS * sizeof(float)));
+    const cudaError_t e = timed_launch(
+        ctx, RC_KERNEL_KPCNN,
+        [&] {
+            return kp::run_inference((const float*)ctx->kp_params.ptr, ctx->kp_packed.ptr, ctx->img.accum,
+                                     ctx->img.gbuf, ctx->img.galb, ctx->kp_feat.ptr, ctx->kp_act0.ptr,
+                                     ctx->kp_act1.ptr, (float*)ctx->kp_logits.ptr, (float4*)ctx->kp_color.ptr,
+                                     ctx->out, ctx->width, ctx->height, &ctx->counters->error_word, ctx->stream);
+        },
+        7);
+    if (e != cudaSuccess) return launch_err(ctx, e, "kpcnn");
     ctx->result = ctx->out;
     if (out_rgba) return rc_read_output(ctx, out_rgba);
     return RC_OK;

@@ -1,0 +1,652 @@
+// kpcnn.cu -- the learned denoiser: a kernel-predicting CNN (3 x conv3x3
+// with 32 channels and ReLU, a 3x3 head of 25 logits, a per-pixel softmax
+// 5x5 filter applied to the noisy radiance), with BF16 operands and FP32
+// accumulation on the tcgen05 tensor cores, for inference and training.
+// The reference has no learned denoiser; this is new work beside its
+// à-trous filter (post/atrous_denoise.frag), which stays the fallback.
+//
+// Data layout (HBM):
+//   activations   NHWC bf16, C = 16 (network input: log1p radiance, albedo,
+//                 normal, depth, 6 zero channels) or 32 (hidden layers)
+//   logits        NHWC fp32, 32 channels (25 used)
+//   radiance      float4 per pixel (rgb, unused w)
+//   parameters    one fp32 vector (RC_KPCNN_PARAMS floats): per layer
+//                 W[tap][co][ci] (tap = 3*dy + dx) then bias[co]
+//   packed        bf16 copies of each W in the tensor cores' K-major
+//                 operand layout [tap][ci/8][co][8], plus for layers 2, 3
+//                 and the head the flipped/transposed copy used by the
+//                 backward-data convolution
+//
+// Kernels:
+//   conv3x3_kernel<CIN>  implicit GEMM, one CTA per 128 pixels of an image
+//                        row: D[128 px][32 co] = sum over 9 taps and CIN/16
+//                        k-steps of A[px][16 ci] x B[16 ci][32 co].  The
+//                        three input rows (130 px with the halo) sit in
+//                        shared memory channel-group-major, pixel-contiguous
+//                        ([row][ci/8][px][8 ci], 16 B per pixel and group), so
+//                        the A operand of horizontal tap dx is the same
+//                        K-major matrix shifted by dx * 16 bytes.  Epilogue:
+//                        bias, ReLU or ReLU-mask (backward), bf16 or fp32.
+//   wgrad_kernel<CIN>    dW[tap][co][ci] = sum_px dY[px][co] X[px+tap][ci]:
+//                        M = (tap, ci) in tiles of 128, N = 32 co, K = pixels,
+//                        both operands MN-major tiles of 128 pixels, FP32
+//                        partial sums atomically added per CTA; bias grads
+//                        from the same staged dY.
+//   head_kernel          softmax over 25 logits, the 5x5 filter (edge
+//                        clamped), and for training the relative-MSE loss
+//                        (x-r)^2/(r^2+0.01) with its gradient w.r.t. logits.
+//   features / crop / pack / adam   small SIMT kernels.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "retrocam.h"
+#include "tc_sm100.cuh"
+
+namespace rc {
+namespace kp {
+
+constexpr int kTile = 128;          // pixels per CTA (one row segment)
+constexpr int kHalo = kTile + 2;    // staged pixels per row
+constexpr int kPStride = 136;       // staged row pitch in 16-byte units
+constexpr int kCo = 32;             // output channels of every convolution
+constexpr uint32_t kWaitTries = 1u << 20;   // bounded mbarrier polls
+
+constexpr int kParamW1 = 0, kParamB1 = kParamW1 + 9 * 32 * 16;
+constexpr int kParamW2 = kParamB1 + 32, kParamB2 = kParamW2 + 9 * 32 * 32;
+constexpr int kParamW3 = kParamB2 + 32, kParamB3 = kParamW3 + 9 * 32 * 32;
+constexpr int kParamWH = kParamB3 + 32, kParamBH = kParamWH + 9 * 32 * 32;
+constexpr int kParams = kParamBH + 32;
+static_assert(kParams == RC_KPCNN_PARAMS, "parameter layout");
+
+struct ConvArgs {
+    const __nv_bfloat16* in;    // NHWC, CIN channels
+    const __nv_bfloat16* wpk;   // packed [9][CIN/8][32][8]
+    const float* bias;          // 32 or null
+    void* out;                  // NHWC 32 channels, bf16 or fp32
+    const __nv_bfloat16* mask;  // NHWC 32 channels: out *= (mask > 0), or null
+    int n, h, w;
+    int relu;
+    int out_f32;
+    unsigned int* err;
+};
+
+template <int CIN>
+struct ConvSmem {
+    alignas(128) uint4 rows[3 * (CIN / 8) * kPStride];
+    alignas(128) uint4 wts[9 * (CIN / 8) * kCo];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+template <int CIN>
+__global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
+    constexpr int G = CIN / 8;
+    __shared__ ConvSmem<CIN> S;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * kTile, y = blockIdx.y, n = blockIdx.z;
+    if (warp == 0) tc::tmem_alloc(&S.tmem, 32);
+    if (tid == 0) tc::mbar_init(&S.mbar, 1);
+    // stage rows y-1..y+1, pixels x0-1 .. x0+128 (zero outside the image)
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    for (int i = tid; i < 3 * kHalo * G; i += 128) {
+        const int r = i / (kHalo * G), rem = i - r * kHalo * G;
+        const int p = rem / G, g = rem - p * G;
+        const int yy = y + r - 1, xx = x0 + p - 1;
+        uint4 v = zero;
+        if (yy >= 0 && yy < A.h && xx >= 0 && xx < A.w)
+            v = __ldg(reinterpret_cast<const uint4*>(A.in + (((size_t)n * A.h + yy) * A.w + xx) * CIN) + g);
+        S.rows[(r * G + g) * kPStride + p] = v;
+    }
+    for (int i = tid; i < 9 * G * kCo; i += 128) S.wts[i] = __ldg(reinterpret_cast<const uint4*>(A.wpk) + i);
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = S.tmem;
+    if (tid == 0) {
+        constexpr uint32_t idesc = tc::idesc_bf16(128, kCo, false, false);
+        const uint32_t rows = tc::smem_u32(S.rows), wts = tc::smem_u32(S.wts);
+#pragma unroll 1
+        for (int tap = 0; tap < 9; ++tap) {
+            const int dy = tap / 3, dx = tap - 3 * dy;
+#pragma unroll
+            for (int ks = 0; ks < CIN / 16; ++ks) {
+                const uint64_t a =
+                    tc::smem_desc(rows + ((dy * G + 2 * ks) * kPStride + dx) * 16, kPStride * 16, 128);
+                const uint64_t b = tc::smem_desc(wts + (tap * G + 2 * ks) * kCo * 16, kCo * 16, 128);
+                tc::mma_bf16(tmem, a, b, idesc, (tap | ks) != 0);
+            }
+        }
+        tc::mma_commit(&S.mbar);
+    }
+    const bool ok = __syncthreads_and(tc::mbar_wait(&S.mbar, 0, kWaitTries));
+    tc::fence_after_sync();
+    if (!ok) {
+        if (tid == 0) atomicOr(A.err, RC_GUARD_MMA_WAIT);
+    } else {
+        float v[32];
+        tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16), v);
+        const int x = x0 + warp * 32 + lane;
+        if (x < A.w) {
+            const size_t pix = ((size_t)n * A.h + y) * A.w + x;
+            if (A.bias) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] += __ldg(A.bias + c);
+            }
+            if (A.relu) {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] = fmaxf(v[c], 0.0f);
+            }
+            if (A.mask) {
+                const uint4* m = reinterpret_cast<const uint4*>(A.mask + pix * 32);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const uint4 mv = __ldg(m + q);
+                    const uint32_t w4[4] = {mv.x, mv.y, mv.z, mv.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&w4[j]);
+                        if (!(__bfloat162float(h2.x) > 0.0f)) v[q * 8 + 2 * j] = 0.0f;
+                        if (!(__bfloat162float(h2.y) > 0.0f)) v[q * 8 + 2 * j + 1] = 0.0f;
+                    }
+                }
+            }
+            if (A.out_f32) {
+                float4* o = reinterpret_cast<float4*>(static_cast<float*>(A.out) + pix * 32);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+                uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(A.out) + pix * 32);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    uint32_t w4[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
+                        w4[j] = *reinterpret_cast<const uint32_t*>(&h2);
+                    }
+                    o[q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+                }
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, 32);
+}
+
+// ---------------------------------------------------------------------------
+// weight gradients
+// ---------------------------------------------------------------------------
+struct WgradArgs {
+    const __nv_bfloat16* x;    // NHWC CIN: the layer's input
+    const __nv_bfloat16* dy;   // NHWC 32: gradient at the layer's pre-activation
+    float* dw;                 // [9][32][CIN] (+=)
+    float* db;                 // [32] (+=)
+    int n, h, w;
+    unsigned int* err;
+};
+
+struct WgradSmem {
+    alignas(128) uint4 a[16 * kTile];   // [m/8][px][8]: im2col of X for one M tile
+    alignas(128) uint4 b[4 * kTile];    // [co/8][px][8]: dY
+    uint64_t mbar;
+    uint32_t tmem;
+};
+
+template <int CIN>
+__global__ void __launch_bounds__(128) wgrad_kernel(WgradArgs A) {
+    constexpr int G = CIN / 8;
+    constexpr int T = 128 / CIN;             // taps per M tile
+    constexpr int MT = (9 + T - 1) / T;      // M tiles
+    constexpr int NCOL = MT * 32 <= 32 ? 32 : (MT * 32 <= 64 ? 64 : 128);
+    __shared__ WgradSmem S;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (warp == 0) tc::tmem_alloc(&S.tmem, NCOL);
+    if (tid == 0) tc::mbar_init(&S.mbar, 1);
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    const uint32_t tmem = S.tmem;
+    const int tiles_x = (A.w + kTile - 1) / kTile;
+    const int ntiles = tiles_x * A.h * A.n;
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+    constexpr uint32_t idesc = tc::idesc_bf16(128, kCo, true, true);
+    float bsum[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t phase = 0;
+    bool ok = true;
+    int issued = 0;
+    for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int xt = t % tiles_x, rest = t / tiles_x;
+        const int y = rest % A.h, n = rest / A.h;
+        const int x0 = xt * kTile;
+        // dY tile, channel-group-major; bias sums per thread (fixed group)
+        for (int i = tid; i < 4 * kTile; i += 128) {
+            const int p = i >> 2, g = i & 3;
+            const int xx = x0 + p;
+            uint4 v = zero;
+            if (xx < A.w) v = __ldg(reinterpret_cast<const uint4*>(A.dy + (((size_t)n * A.h + y) * A.w + xx) * 32) + g);
+            S.b[g * kTile + p] = v;
+            const uint32_t w4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&w4[j]);
+                bsum[2 * j] += __bfloat162float(h2.x);
+                bsum[2 * j + 1] += __bfloat162float(h2.y);
+            }
+        }
+        for (int mt = 0; mt < MT && ok; ++mt) {
+            if (issued > 0) {   // the previous MMAs still read S.a / S.b
+                ok = __syncthreads_and(tc::mbar_wait(&S.mbar, phase, kWaitTries));
+                phase ^= 1u;
+                tc::fence_after_sync();
+                if (!ok) break;
+            }
+            for (int i = tid; i < 16 * kTile; i += 128) {
+                const int p = i / 16, mg = i - 16 * p;   // group fastest: 16 B pieces of one pixel
+                const int tl = mg / G, g = mg - tl * G;
+                const int tap = mt * T + tl;
+                uint4 v = zero;
+                if (tap < 9) {
+                    const int dy = tap / 3, dx = tap - 3 * dy;
+                    const int yy = y + dy - 1, xx = x0 + p + dx - 1;
+                    if (yy >= 0 && yy < A.h && xx >= 0 && xx < A.w && x0 + p < A.w)
+                        v = __ldg(reinterpret_cast<const uint4*>(A.x + (((size_t)n * A.h + yy) * A.w + xx) * CIN) + g);
+                }
+                S.a[mg * kTile + p] = v;
+            }
+            tc::fence_async_smem();
+            tc::fence_before_sync();
+            __syncthreads();
+            tc::fence_after_sync();
+            if (tid == 0) {
+                const uint32_t sa = tc::smem_u32(S.a), sb = tc::smem_u32(S.b);
+#pragma unroll
+                for (int ks = 0; ks < kTile / 16; ++ks) {
+                    const uint64_t a = tc::smem_desc(sa + ks * 256, 128, kTile * 16);
+                    const uint64_t b = tc::smem_desc(sb + ks * 256, 128, kTile * 16);
+                    tc::mma_bf16(tmem + mt * 32, a, b, idesc, (t != (int)blockIdx.x || ks > 0) ? 1u : 0u);
+                }
+                tc::mma_commit(&S.mbar);
+            }
+            ++issued;
+        }
+        if (!ok) break;
+        // the next tile overwrites S.b: wait for this tile's last MMAs
+        ok = __syncthreads_and(tc::mbar_wait(&S.mbar, phase, kWaitTries));
+        phase ^= 1u;
+        issued = 0;
+        tc::fence_after_sync();
+        __syncthreads();
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(A.err, RC_GUARD_MMA_WAIT);
+    } else if ((int)blockIdx.x < ntiles) {
+        // bias: reduce the 8 sums of threads sharing a channel group (lane % 4)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            float s = bsum[j];
+            s += __shfl_xor_sync(0xffffffffu, s, 4);
+            s += __shfl_xor_sync(0xffffffffu, s, 8);
+            s += __shfl_xor_sync(0xffffffffu, s, 16);
+            if (lane < 4) atomicAdd(A.db + lane * 8 + j, s);
+        }
+        for (int mt = 0; mt < MT; ++mt) {
+            float v[32];
+            tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + mt * 32, v);
+            const int m = warp * 32 + lane;
+            const int tl = m / CIN, ci = m - tl * CIN;
+            const int tap = mt * T + tl;
+            if (tap < 9) {
+#pragma unroll
+                for (int co = 0; co < 32; ++co) atomicAdd(A.dw + (tap * 32 + co) * CIN + ci, v[co]);
+            }
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) tc::tmem_dealloc(tmem, NCOL);
+}
+
+// ---------------------------------------------------------------------------
+// head: softmax 5x5 filter, loss and its gradient
+// ---------------------------------------------------------------------------
+struct HeadArgs {
+    const float* logits;        // NHWC 32 (25 used)
+    const float4* color;        // noisy radiance
+    const float4* target;       // reference radiance, or null (inference)
+    float4* out;                // filtered radiance (w = 1)
+    __nv_bfloat16* dlogits;     // NHWC 32, or null
+    double* loss;               // sum of per-channel relative squared errors, or null
+    float grad_scale;           // d(total loss)/d(per-channel term)
+    int n, h, w;
+};
+
+__global__ void __launch_bounds__(128) head_kernel(HeadArgs A) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, n = blockIdx.z;
+    float lsum = 0.0f;
+    if (x < A.w) {
+        const size_t pix = ((size_t)n * A.h + y) * A.w + x;
+        float l[25];
+        const float4* lg = reinterpret_cast<const float4*>(A.logits + pix * 32);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const float4 v = lg[q];
+            l[4 * q] = v.x;
+            l[4 * q + 1] = v.y;
+            l[4 * q + 2] = v.z;
+            l[4 * q + 3] = v.w;
+        }
+        l[24] = lg[6].x;
+        float m = l[0];
+#pragma unroll
+        for (int t = 1; t < 25; ++t) m = fmaxf(m, l[t]);
+        float s = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 25; ++t) {
+            l[t] = __expf(l[t] - m);
+            s += l[t];
+        }
+        const float inv = 1.0f / s;
+        float3 o = make_float3(0.0f, 0.0f, 0.0f);
+        const size_t img = (size_t)n * A.h * A.w;
+#pragma unroll
+        for (int t = 0; t < 25; ++t) {
+            l[t] *= inv;
+            const int yy = min(max(y + t / 5 - 2, 0), A.h - 1), xx = min(max(x + t % 5 - 2, 0), A.w - 1);
+            const float4 c = __ldg(A.color + img + (size_t)yy * A.w + xx);
+            o.x += l[t] * c.x;
+            o.y += l[t] * c.y;
+            o.z += l[t] * c.z;
+        }
+        A.out[pix] = make_float4(o.x, o.y, o.z, 1.0f);
+        if (A.target) {
+            const float4 r = __ldg(A.target + pix);
+            const float dr = o.x - r.x, dg = o.y - r.y, db = o.z - r.z;
+            const float qr = 1.0f / (r.x * r.x + 0.01f), qg = 1.0f / (r.y * r.y + 0.01f),
+                        qb = 1.0f / (r.z * r.z + 0.01f);
+            lsum = dr * dr * qr + dg * dg * qg + db * db * qb;
+            if (A.dlogits) {
+                const float gx = 2.0f * dr * qr * A.grad_scale, gy = 2.0f * dg * qg * A.grad_scale,
+                            gz = 2.0f * db * qb * A.grad_scale;
+                float dw[25], wsum = 0.0f;
+#pragma unroll
+                for (int t = 0; t < 25; ++t) {
+                    const int yy = min(max(y + t / 5 - 2, 0), A.h - 1), xx = min(max(x + t % 5 - 2, 0), A.w - 1);
+                    const float4 c = __ldg(A.color + img + (size_t)yy * A.w + xx);
+                    dw[t] = gx * c.x + gy * c.y + gz * c.z;
+                    wsum += l[t] * dw[t];
+                }
+                uint32_t packed[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const float a = 2 * j < 25 ? l[2 * j] * (dw[2 * j] - wsum) : 0.0f;
+                    const float b = 2 * j + 1 < 25 ? l[2 * j + 1] * (dw[2 * j + 1] - wsum) : 0.0f;
+                    const __nv_bfloat162 h2 = __floats2bfloat162_rn(a, b);
+                    packed[j] = *reinterpret_cast<const uint32_t*>(&h2);
+                }
+                uint4* d = reinterpret_cast<uint4*>(A.dlogits + pix * 32);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    d[q] = make_uint4(packed[4 * q], packed[4 * q + 1], packed[4 * q + 2], packed[4 * q + 3]);
+            }
+        }
+    }
+    if (A.loss) {
+        __shared__ float red[4];
+        float v = lsum;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(A.loss, (double)(red[0] + red[1] + red[2] + red[3]));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// features, crops, packing, optimizer
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float h2f(unsigned short u) { return __half2float(__ushort_as_half(u)); }
+
+// Network input from a context's images: log1p radiance, albedo, normal,
+// depth mapped to t/(1+t); plus the radiance itself for the filter.
+__global__ void features_kernel(const float4* __restrict__ accum, const ushort4* __restrict__ gbuf,
+                                const ushort4* __restrict__ galb, __nv_bfloat16* __restrict__ feat,
+                                float4* __restrict__ color, int count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float4 a = accum[i];
+    const float inv = 1.0f / fmaxf(a.w, 1.0f);
+    const float r = a.x * inv, g = a.y * inv, b = a.z * inv;
+    color[i] = make_float4(r, g, b, 1.0f);
+    const ushort4 gb = gbuf[i], ga = galb[i];
+    const float t = h2f(gb.w);
+    float f[16] = {log1pf(fmaxf(r, 0.0f)), log1pf(fmaxf(g, 0.0f)), log1pf(fmaxf(b, 0.0f)), h2f(ga.x), h2f(ga.y),
+                   h2f(ga.z), h2f(gb.x), h2f(gb.y), h2f(gb.z), t / (1.0f + fabsf(t)), 0, 0, 0, 0, 0, 0};
+    uint32_t p[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(f[2 * j], f[2 * j + 1]);
+        p[j] = *reinterpret_cast<const uint32_t*>(&h2);
+    }
+    uint4* o = reinterpret_cast<uint4*>(feat + (size_t)i * 16);
+    o[0] = make_uint4(p[0], p[1], p[2], p[3]);
+    o[1] = make_uint4(p[4], p[5], p[6], p[7]);
+}
+
+// Training crops: crop b copies the size x size window at (oy, ox) of input
+// image src[b] (features + radiance) and of target image tgt[b].
+__global__ void crop_kernel(const __nv_bfloat16* __restrict__ feat_all, const float4* __restrict__ color_all,
+                            const float4* __restrict__ target_all, const int* __restrict__ src,
+                            const int* __restrict__ tgt, const int* __restrict__ oy, const int* __restrict__ ox,
+                            int H, int W, int size, __nv_bfloat16* __restrict__ feat, float4* __restrict__ color,
+                            float4* __restrict__ target) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, b = blockIdx.z;
+    if (x >= size) return;
+    const size_t s = ((size_t)src[b] * H + oy[b] + y) * W + ox[b] + x;
+    const size_t r = ((size_t)tgt[b] * H + oy[b] + y) * W + ox[b] + x;
+    const size_t d = ((size_t)b * size + y) * size + x;
+    const uint4* fi = reinterpret_cast<const uint4*>(feat_all + s * 16);
+    uint4* fo = reinterpret_cast<uint4*>(feat + d * 16);
+    fo[0] = fi[0];
+    fo[1] = fi[1];
+    color[d] = color_all[s];
+    target[d] = target_all[r];
+}
+
+// fp32 parameters -> bf16 operand copies.  Forward layout [tap][ci/8][co][8];
+// backward-data layout [tap][co/8][ci][8] with tap flipped (8 - tap).
+__global__ void pack_kernel(const float* __restrict__ params, __nv_bfloat16* __restrict__ w1,
+                            __nv_bfloat16* __restrict__ w2, __nv_bfloat16* __restrict__ w3,
+                            __nv_bfloat16* __restrict__ wh, __nv_bfloat16* __restrict__ w2b,
+                            __nv_bfloat16* __restrict__ w3b, __nv_bfloat16* __restrict__ whb) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < 9 * 32 * 16) {
+        const int tap = e / 512, rem = e % 512, g = rem / 256, co = (rem % 256) / 8, j = rem % 8;
+        w1[e] = __float2bfloat16_rn(params[kParamW1 + (tap * 32 + co) * 16 + g * 8 + j]);
+    }
+    if (e < 9 * 32 * 32) {
+        const int tap = e / 1024, rem = e % 1024, g = rem / 256, r = (rem % 256) / 8, j = rem % 8;
+        // forward: r = co, channel g*8+j = ci
+        w2[e] = __float2bfloat16_rn(params[kParamW2 + (tap * 32 + r) * 32 + g * 8 + j]);
+        w3[e] = __float2bfloat16_rn(params[kParamW3 + (tap * 32 + r) * 32 + g * 8 + j]);
+        wh[e] = __float2bfloat16_rn(params[kParamWH + (tap * 32 + r) * 32 + g * 8 + j]);
+        // backward: r = ci (output of the transposed conv), g*8+j = co
+        const int src = ((8 - tap) * 32 + g * 8 + j) * 32 + r;
+        w2b[e] = __float2bfloat16_rn(params[kParamW2 + src]);
+        w3b[e] = __float2bfloat16_rn(params[kParamW3 + src]);
+        whb[e] = __float2bfloat16_rn(params[kParamWH + src]);
+    }
+}
+
+__global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, int count, float lr, float b1, float b2, float eps, float c1,
+                            float c2) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+    g[i] = 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+cudaError_t launch_conv(const ConvArgs& A, int cin, cudaStream_t s) {
+    const dim3 grid((A.w + kTile - 1) / kTile, A.h, A.n);
+    if (cin == 16)
+        conv3x3_kernel<16><<<grid, 128, 0, s>>>(A);
+    else
+        conv3x3_kernel<32><<<grid, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wgrad(const WgradArgs& A, int cin, cudaStream_t s) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tiles = ((A.w + kTile - 1) / kTile) * A.h * A.n;
+    const int grid = tiles < sms * 4 ? tiles : sms * 4;
+    if (grid <= 0) return cudaSuccess;
+    if (cin == 16)
+        wgrad_kernel<16><<<grid, 128, 0, s>>>(A);
+    else
+        wgrad_kernel<32><<<grid, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_head(const HeadArgs& A, cudaStream_t s) {
+    const dim3 grid((A.w + 127) / 128, A.h, A.n);
+    head_kernel<<<grid, 128, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_features(const float4* accum, const ushort4* gbuf, const ushort4* galb, __nv_bfloat16* feat,
+                            float4* color, int count, cudaStream_t s) {
+    features_kernel<<<(count + 255) / 256, 256, 0, s>>>(accum, gbuf, galb, feat, color, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pack(const float* params, __nv_bfloat16* const* w, cudaStream_t s) {
+    pack_kernel<<<(9 * 32 * 32 + 255) / 256, 256, 0, s>>>(params, w[0], w[1], w[2], w[3], w[4], w[5], w[6]);
+    return cudaGetLastError();
+}
+
+// bf16 elements of the seven packed weight copies, in rc_kp_pack order
+constexpr size_t kPackedElems[7] = {9 * 32 * 16, 9 * 32 * 32, 9 * 32 * 32, 9 * 32 * 32,
+                                    9 * 32 * 32, 9 * 32 * 32, 9 * 32 * 32};
+
+size_t packed_bytes() {
+    size_t b = 0;
+    for (size_t e : kPackedElems) b += e * 2;
+    return b;
+}
+
+// Inference over one W x H frame: pack, features, three hidden
+// convolutions, the head convolution and the filter (7 launches).
+cudaError_t run_inference(const float* params, void* packed, const float4* accum, const ushort4* gbuf,
+                          const ushort4* galb, void* feat, void* act0, void* act1, float* logits, float4* color,
+                          float4* out, int W, int H, unsigned int* err, cudaStream_t s) {
+    __nv_bfloat16* w[7];
+    __nv_bfloat16* p = static_cast<__nv_bfloat16*>(packed);
+    for (int i = 0; i < 7; ++i) {
+        w[i] = p;
+        p += kPackedElems[i];
+    }
+    cudaError_t e = launch_pack(params, w, s);
+    if (e == cudaSuccess) e = launch_features(accum, gbuf, galb, static_cast<__nv_bfloat16*>(feat), color, W * H, s);
+    const __nv_bfloat16* f = static_cast<const __nv_bfloat16*>(feat);
+    __nv_bfloat16* a0 = static_cast<__nv_bfloat16*>(act0);
+    __nv_bfloat16* a1 = static_cast<__nv_bfloat16*>(act1);
+    if (e == cudaSuccess) e = launch_conv({f, w[0], params + kParamB1, a0, nullptr, 1, H, W, 1, 0, err}, 16, s);
+    if (e == cudaSuccess) e = launch_conv({a0, w[1], params + kParamB2, a1, nullptr, 1, H, W, 1, 0, err}, 32, s);
+    if (e == cudaSuccess) e = launch_conv({a1, w[2], params + kParamB3, a0, nullptr, 1, H, W, 1, 0, err}, 32, s);
+    if (e == cudaSuccess) e = launch_conv({a0, w[3], params + kParamBH, logits, nullptr, 1, H, W, 0, 1, err}, 32, s);
+    if (e == cudaSuccess) e = launch_head({logits, color, nullptr, out, nullptr, nullptr, 0.0f, 1, H, W}, s);
+    return e;
+}
+
+}  // namespace kp
+}  // namespace rc
+
+// ---------------------------------------------------------------------------
+// C ABI of the building blocks (device pointers; the training driver and the
+// tests call these on their own buffers and stream)
+// ---------------------------------------------------------------------------
+using namespace rc::kp;
+
+extern "C" {
+
+int rc_kp_conv3x3(const void* in, int cin, const void* wpk, const float* bias, void* out, int out_f32, int relu,
+                  const void* mask, int n, int h, int w, unsigned int* err, void* stream) {
+    if (!in || !wpk || !out || !err || (cin != 16 && cin != 32) || n <= 0 || h <= 0 || w <= 0)
+        return RC_ERR_INVALID_ARG;
+    ConvArgs A{static_cast<const __nv_bfloat16*>(in), static_cast<const __nv_bfloat16*>(wpk), bias, out,
+               static_cast<const __nv_bfloat16*>(mask), n, h, w, relu, out_f32, err};
+    return launch_conv(A, cin, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
+}
+
+int rc_kp_wgrad(const void* x, int cin, const void* dy, float* dw, float* db, int n, int h, int w,
+                unsigned int* err, void* stream) {
+    if (!x || !dy || !dw || !db || !err || (cin != 16 && cin != 32) || n <= 0 || h <= 0 || w <= 0)
+        return RC_ERR_INVALID_ARG;
+    WgradArgs A{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, db, n, h, w, err};
+    return launch_wgrad(A, cin, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
+}
+
+int rc_kp_head(const float* logits, const void* color, const void* target, void* out, void* dlogits,
+               double* loss, float grad_scale, int n, int h, int w, void* stream) {
+    if (!logits || !color || !out || n <= 0 || h <= 0 || w <= 0 || (dlogits && !target)) return RC_ERR_INVALID_ARG;
+    HeadArgs A{logits,
+               static_cast<const float4*>(color),
+               static_cast<const float4*>(target),
+               static_cast<float4*>(out),
+               static_cast<__nv_bfloat16*>(dlogits),
+               loss,
+               grad_scale,
+               n,
+               h,
+               w};
+    return launch_head(A, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
+}
+
+int rc_kp_pack(const float* params, void* const* packed7, void* stream) {
+    if (!params || !packed7) return RC_ERR_INVALID_ARG;
+    __nv_bfloat16* w[7];
+    for (int i = 0; i < 7; ++i) {
+        if (!packed7[i]) return RC_ERR_INVALID_ARG;
+        w[i] = static_cast<__nv_bfloat16*>(packed7[i]);
+    }
+    return launch_pack(params, w, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
+}
+
+int rc_kp_adam(float* params, float* grads, float* m, float* v, int count, float lr, float beta1, float beta2,
+               float eps, int step, void* stream) {
+    if (!params || !grads || !m || !v || count <= 0 || step < 1) return RC_ERR_INVALID_ARG;
+    const float c1 = 1.0f / (1.0f - powf(beta1, (float)step)), c2 = 1.0f / (1.0f - powf(beta2, (float)step));
+    adam_kernel<<<(count + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(params, grads, m, v, count, lr,
+                                                                                     beta1, beta2, eps, c1, c2);
+    return cudaGetLastError() == cudaSuccess ? RC_OK : RC_ERR_CUDA;
+}
+
+int rc_kp_crop(const void* feat_all, const void* color_all, const void* target_all, const int* src, const int* tgt,
+               const int* oy, const int* ox, int batch, int H, int W, int size, void* feat, void* color,
+               void* target, void* stream) {
+    if (!feat_all || !color_all || !target_all || !src || !tgt || !oy || !ox || !feat || !color || !target ||
+        batch <= 0 || size <= 0 || size > H || size > W)
+        return RC_ERR_INVALID_ARG;
+    const dim3 grid((size + 127) / 128, size, batch);
+    crop_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<const __nv_bfloat16*>(feat_all), static_cast<const float4*>(color_all),
+        static_cast<const float4*>(target_all), src, tgt, oy, ox, H, W, size, static_cast<__nv_bfloat16*>(feat),
+        static_cast<float4*>(color), static_cast<float4*>(target));
+    return cudaGetLastError() == cudaSuccess ? RC_OK : RC_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -197,6 +197,28 @@ def cornell_small() -> Workload:
                     LensDesc(focal_length_mm=35.0, f_stop=16.0, focus_dist_m=2.5))
 
 
+def cornell_variant(seed: int, width: int = 854, height: int = 480, spp: int = 16) -> Workload:
+    """A randomised Cornell box for the learned denoiser's data: wall
+    colours, box poses, light size and lens drawn from a seeded generator.
+    Same geometry as the small box (walls, ceiling light, two boxes)."""
+    rng = np.random.default_rng(seed)
+    u = lambda lo, hi, n=None: rng.uniform(lo, hi, n)  # noqa: E731
+    grey = float(u(0.45, 0.85))
+    half = float(u(0.06, 0.2))
+    # the emitted power of the reference light (17 x 0.25^2) for any size
+    mats = [diffuse(grey, grey, grey), diffuse(*u(0.05, 0.85, 3)), diffuse(*u(0.05, 0.85, 3)),
+            emissive(1.0, 12.0 / 17.0, 4.0 / 17.0, 17.0 * (0.125 / half) ** 2)]
+    th, ts = u(0.18, 0.34), u(0.12, 0.2)
+    tall = Box(center=(float(u(0.5, 0.8)), float(th), float(u(0.45, 0.8))), half=(0.15, float(th), 0.15), mat=0,
+               rot=(0.0, float(u(-45.0, 45.0)), 0.0))
+    short = Box(center=(float(u(0.2, 0.45)), float(ts), float(u(0.2, 0.45))), half=(float(ts), float(ts), float(ts)),
+                mat=0, rot=(0.0, float(u(-45.0, 45.0)), 0.0))
+    sc = SceneDesc(mats, cornell_walls_and_light(light_half=half) + [tall, short])
+    lens = LensDesc(focal_length_mm=float(u(24.0, 50.0)), f_stop=float(u(2.8, 16.0)),
+                    focus_dist_m=float(u(1.5, 2.5)))
+    return Workload(f"cornell_variant_{seed}", width, height, spp, sc, CORNELL_ORBIT, lens)
+
+
 def export_frame_scene() -> SceneDesc:
     mats = cornell_materials() + [glass(1.5), metal(0.95, 0.85, 0.55, 0.2)]
     objs = cornell_walls_and_light() + [TALL_BOX, SHORT_BOX,
