@@ -90,6 +90,8 @@ def parse_args(argv=None):
     ap.add_argument("--retune", action="store_true", help="with --engine auto: tune again, ignore the cache")
     ap.add_argument("--chunk-paths", type=int, default=0, help="wavefront paths in flight (0: default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-quality", action="store_true", help="skip the time-to-relMSE comparison")
+    ap.add_argument("--quality-variants", type=int, default=8, help="held-out Cornell variants for time-to-relMSE")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--spp", type=int, default=0, help="override spp (profiling of a small case)")
     ap.add_argument("--sppm-iterations", type=int, default=-1, help="override SPPM iterations")
@@ -349,6 +351,22 @@ def run_reference(args):
     return 0
 
 
+def time_to_relmse(args) -> dict:
+    """The metric's second half: wall time (render + denoise, one frame at
+    854x480) to reach mean relMSE <= 1e-2 against a 4096-spp render, path
+    tracer + à-trous vs path tracer + the shipped learned denoiser, on
+    held-out seeded Cornell variants (no dataset exists for this scene)."""
+    from retrocam_b200 import kpcnn
+    seeds = list(range(5000, 5000 + args.quality_variants))
+    rep = kpcnn.evaluate(kpcnn.load(), seeds, spps=(1, 2, 4, 8, 16, 32, 64), ref_spp=4096, log=None)
+    t = rep["time_to_threshold"]
+    return {"threshold": rep["threshold"], "ref_spp": rep["ref_spp"], "variants": seeds,
+            "plain_atrous": t["atrous"], "learned": t["learned"], "plain_no_denoiser": t["noisy"],
+            "learned_speedup": rep["speedup_learned_vs_atrous"],
+            "relmse_at_spp": {"spp": rep["spp"], "atrous": rep["relmse"]["atrous"],
+                              "learned": rep["relmse"]["learned"]}}
+
+
 def workload_config(w, args):
     cfg = {"workload": w.name, "width": w.width, "height": w.height, "spp": w.spp,
            "paths_per_sample": 3 if any(w.lens.lca_delta) else 1, "max_bounces": 6,
@@ -493,6 +511,8 @@ def run_b200(args):
                               ("camera_paths", "closest_rays", "shadow_rays", "photon_rays", "gather_rays",
                                "node_tests", "tri_tests", "surface_hits", "light_samples")},
     }
+    if rank == 0 and not args.no_quality:
+        line["time_to_relmse"] = time_to_relmse(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         t_frame, info = cpu_reference_sample(w, args.cpu_seconds)
         line["cpu_baseline"] = {"value": samples_per_step / t_frame / 1e6, "unit": UNIT, "cores": info["cores"],

@@ -107,6 +107,7 @@ struct rc_ctx {
     DevBuf frames;
     // learned denoiser scratch
     DevBuf kp_feat, kp_act0, kp_act1, kp_logits, kp_color, kp_params, kp_packed;
+    std::vector<float> kp_host;   // parameters last uploaded to kp_params
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_key = 0;
     unsigned long long graph_launches = 0;
@@ -969,7 +970,13 @@ int rc_denoise_learned(rc_ctx* ctx, const rc_kpcnn* weights, float* out_rgba) {
     CK(ensure(ctx->kp_color, px * 16));
     CK(ensure(ctx->kp_params, RC_KPCNN_PARAMS * sizeof(float)));
     CK(ensure(ctx->kp_packed, kp::packed_bytes()));
-    CK(copy_h2d(ctx, ctx->kp_params.ptr, weights->params, RC_KPCNN_PARAMS * sizeof(float)));
+    // upload (and repack) only when the parameters changed since the last call
+    const bool same = ctx->kp_host.size() == (size_t)RC_KPCNN_PARAMS &&
+                      memcmp(ctx->kp_host.data(), weights->params, RC_KPCNN_PARAMS * sizeof(float)) == 0;
+    if (!same) {
+        ctx->kp_host.assign(weights->params, weights->params + RC_KPCNN_PARAMS);
+        CK(copy_h2d(ctx, ctx->kp_params.ptr, ctx->kp_host.data(), RC_KPCNN_PARAMS * sizeof(float)));
+    }
     const cudaError_t e = timed_launch(
         ctx, RC_KERNEL_KPCNN,
         [&] {

@@ -248,3 +248,114 @@ def render_dataset(seeds, input_spps=(1, 4, 16), target_spp=1024, width=854, hei
             if log and (vi + 1) % 32 == 0:
                 log(f"rendered {vi + 1}/{len(seeds)} variants ({time.perf_counter() - t0:.1f} s)")
     return data
+
+
+def _timed(ctx, fn) -> float:
+    """Milliseconds of fn() on the context's stream (synchronize on both sides)."""
+    ctx.synchronize()
+    t0 = time.perf_counter()
+    fn()
+    ctx.synchronize()
+    return (time.perf_counter() - t0) * 1e3
+
+
+def evaluate(params: np.ndarray, seeds, spps=(1, 2, 4, 8, 16, 32, 64, 128, 256), ref_spp=4096, width=854,
+             height=480, threshold=1e-2, log=print) -> dict:
+    """relMSE against an independent `ref_spp` render, for the path tracer
+    plus à-trous (5 passes, sigma_n 128, sigma_d 1, sigma_c 1) and plus the
+    learned denoiser at equal spp; wall time of render + denoise per frame.
+    `time_to_threshold` is, per method, the time at the smallest spp whose
+    mean relMSE over the variants is <= threshold (None if none is)."""
+    atrous = api.atrous_params(scenes.AtrousDesc(max_spp=0))
+    res = {"spp": list(spps), "ref_spp": ref_spp, "variants": list(seeds), "width": width, "height": height,
+           "relmse": {"noisy": [], "atrous": [], "learned": []},
+           "ms": {"render": [], "atrous": [], "learned": []}}
+    per = {k: np.zeros((len(seeds), len(spps))) for k in ("noisy", "atrous", "learned", "render", "t_atrous",
+                                                           "t_learned")}
+    with api.Context(width, height, 0, api.RC_MATH_FAST) as ctx:
+        for vi, seed in enumerate(seeds):
+            w = scenes.cornell_variant(seed, width, height)
+            ctx.upload(api.build_scene(w.scene))
+            cam = api.workload_camera(w)
+            st = (w.nee_enabled, w.nee_firefly_clamp)
+            ctx.reset()
+            ctx.render(cam, st, 1 << 21, ref_spp)
+            acc = ctx.read_buffers()[0]
+            ref = acc[..., :3] / np.maximum(acc[..., 3:4], 1)
+            # first calls allocate their scratch: keep that out of the timings
+            ctx.denoise(atrous, read=False)
+            ctx.denoise_learned(params, read=False)
+            for si, k in enumerate(spps):
+                ctx.reset()
+                per["render"][vi, si] = _timed(ctx, lambda: ctx.render(cam, st, 0, k))
+                acc = ctx.read_buffers()[0]
+                per["noisy"][vi, si] = relmse(acc[..., :3] / np.maximum(acc[..., 3:4], 1), ref)
+                per["t_atrous"][vi, si] = _timed(ctx, lambda: ctx.denoise(atrous, read=False))
+                per["atrous"][vi, si] = relmse(ctx.read_output(), ref)
+                per["t_learned"][vi, si] = _timed(ctx, lambda: ctx.denoise_learned(params, read=False))
+                per["learned"][vi, si] = relmse(ctx.read_output(), ref)
+                if ctx.counters()["error_word"]:
+                    raise api.RetroCamError(api.RC_ERR_DEVICE_GUARD, "kernel guard during evaluation")
+            if log:
+                log(f"variant {seed}: atrous {np.round(per['atrous'][vi], 4).tolist()} "
+                    f"learned {np.round(per['learned'][vi], 4).tolist()}")
+    for k in ("noisy", "atrous", "learned"):
+        res["relmse"][k] = per[k].mean(axis=0).tolist()
+    res["ms"]["render"] = per["render"].mean(axis=0).tolist()
+    res["ms"]["atrous"] = per["t_atrous"].mean(axis=0).tolist()
+    res["ms"]["learned"] = per["t_learned"].mean(axis=0).tolist()
+    ttt = {}
+    for k, tk in (("noisy", None), ("atrous", "atrous"), ("learned", "learned")):
+        hit = [i for i, v in enumerate(res["relmse"][k]) if v <= threshold]
+        if hit:
+            i = hit[0]
+            t = res["ms"]["render"][i] + (res["ms"][tk][i] if tk else 0.0)
+            ttt[k] = {"spp": spps[i], "ms": t}
+        else:
+            ttt[k] = None
+    res["threshold"] = threshold
+    res["time_to_threshold"] = ttt
+    a, l_ = ttt.get("atrous"), ttt.get("learned")
+    res["speedup_learned_vs_atrous"] = (a["ms"] / l_["ms"]) if (a and l_) else None
+    return res
+
+
+def _main(argv=None) -> int:
+    """Renders the training set, trains, saves the weights, evaluates."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--variants", type=int, default=192)
+    ap.add_argument("--target-spp", type=int, default=1024)
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=2e-3)
+    ap.add_argument("--eval-variants", type=int, default=8)
+    ap.add_argument("--ref-spp", type=int, default=4096)
+    ap.add_argument("--out", default=WEIGHTS)
+    ap.add_argument("--report", default="")
+    ap.add_argument("--eval-only", action="store_true")
+    args = ap.parse_args(argv)
+    if args.eval_only:
+        params = load(args.out)
+    else:
+        data = render_dataset(range(1000, 1000 + args.variants), target_spp=args.target_spp)
+        tr = Trainer(init_params(0), batch=args.batch, lr=args.lr)
+        t0 = time.perf_counter()
+        hist = tr.train(data, args.steps)
+        train_s = time.perf_counter() - t0
+        params = tr.params()
+        del data
+        save(args.out, params, steps=args.steps, variants=args.variants, target_spp=args.target_spp,
+             batch=args.batch, train_seconds=train_s, final_train_relmse=hist[-1][1])
+        print(f"trained {args.steps} steps in {train_s:.1f} s; saved {args.out}")
+    rep = evaluate(params, range(5000, 5000 + args.eval_variants), ref_spp=args.ref_spp)
+    print(json.dumps({k: rep[k] for k in ("relmse", "time_to_threshold", "speedup_learned_vs_atrous")}))
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(rep, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(_main())

@@ -251,3 +251,23 @@ def test_features_layout(product, T):
     t = gb.view(np.float16)[..., 3].astype(np.float32)
     np.testing.assert_allclose(f[..., 9], t / (1 + np.abs(t)), rtol=1e-2, atol=1e-3)
     assert not f[..., 10:].any()
+
+
+def test_shipped_weights_beat_atrous_on_held_out_variant(product, T):
+    """The shipped network, on a Cornell variant outside its training seeds
+    at 4 spp, lands under relMSE 1e-2 and well under the à-trous filter."""
+    from retrocam_b200 import kpcnn, scenes
+    params = kpcnn.load()
+    W, H = 320, 180
+    w = scenes.cornell_variant(6001, W, H)
+    cam = product.workload_camera(w)
+    with product.Context(W, H, 0, product.RC_MATH_FAST) as ctx:
+        ctx.upload(product.build_scene(w.scene))
+        ctx.render(cam, (1, 1.0), 1 << 21, 1024)
+        acc = ctx.read_buffers()[0]
+        ref = acc[..., :3] / acc[..., 3:4]
+        ctx.reset()
+        ctx.render(cam, (1, 1.0), 0, 4)
+        a = kpcnn.relmse(ctx.denoise(product.atrous_params(scenes.AtrousDesc())), ref)
+        l_ = kpcnn.relmse(ctx.denoise_learned(params), ref)
+    assert l_ < 1e-2 and l_ < 0.5 * a, (l_, a)
