@@ -77,6 +77,32 @@ def algorithmic_bytes(kernel: str, ctr: dict, samples: int) -> float:
     return 0.0
 
 
+FLOP_NODE_TEST = 22       # 6 sub + 6 mul + 10 min/max
+FLOP_TRI_TEST = 40        # Moller-Trumbore
+
+
+def fp32_roofline(kernel: str, ctr: dict, launches: int, avg_launch_s: float, device: int):
+    """FP32 fraction of a traversal kernel: its box and triangle tests as
+    FLOPs per launch over its average launch time, against the FMA
+    throughput measured on this GPU (rc_measure_fp32_peak).  The scene of
+    the export frame is cache-resident, so the traversal is bound by issue
+    rate rather than HBM."""
+    if kernel == "wf_trace" or kernel == "render":
+        flops = FLOP_NODE_TEST * ctr["node_tests"] + FLOP_TRI_TEST * ctr["tri_tests"]
+    elif kernel in ("photon_trace", "photon_gather"):
+        flops = FLOP_NODE_TEST * ctr["photon_node_tests"] + FLOP_TRI_TEST * ctr["photon_tri_tests"]
+    else:
+        return None
+    import ctypes
+    from retrocam_b200 import api
+    peak = ctypes.c_double(0.0)
+    if api.lib().rc_measure_fp32_peak(device, ctypes.byref(peak)) != 0 or peak.value <= 0 or avg_launch_s <= 0:
+        return None
+    achieved = flops / max(1, launches) / avg_launch_s / 1e12
+    return {"achieved": achieved, "peak": peak.value, "unit": "TFLOP/s", "frac": achieved / peak.value,
+            "flops_per_launch": flops / max(1, launches), "peak_source": "measured FMA microbenchmark"}
+
+
 def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -490,6 +516,7 @@ def run_b200(args):
     peak, peak_kind = hbm_peak()
     achieved = per_launch_bytes / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
     traffic = read_traffic(KERNEL_SYMBOL.get(kernel, kernel), w.name)
+    fp32 = fp32_roofline(kernel, ctr, k_launches, avg_launch_s, local_rank)
     rays = ctr["closest_rays"] + ctr["shadow_rays"] + ctr["photon_rays"] + ctr["gather_rays"]
     kernels_total_ms = sum(v[0] for v in ktimes.values())
     line = {
@@ -501,7 +528,7 @@ def run_b200(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                      "kernel": KERNEL_SYMBOL.get(kernel, kernel), "algorithmic_bytes_per_launch": per_launch_bytes,
-                     "avg_launch_ms": avg_launch_s * 1e3, "launches": k_launches},
+                     "avg_launch_ms": avg_launch_s * 1e3, "launches": k_launches, "fp32": fp32},
         "mrays_per_s": rays / (t_ms / 1e3) / 1e6,
         "kernel_ms": {k: v[0] / args.steps for k, v in ktimes.items()},
         "kernel_share": {k: (v[0] / kernels_total_ms if kernels_total_ms else 0.0) for k, v in ktimes.items()},

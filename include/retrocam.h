@@ -231,6 +231,11 @@ int rc_ctx_set_stream(rc_ctx* ctx, void* cuda_stream);
  * launching stream; rc_get_kernel_times synchronises and returns, per kernel
  * kind, the summed milliseconds and the launch count since the last call. */
 int rc_set_kernel_timing(rc_ctx* ctx, int enable);
+/* Measures the device's FP32 FMA throughput in TFLOP/s (16 independent FMA
+ * chains per thread on every SM; best of 5, CUDA events).  No counterpart
+ * in the reference; the denominator of the traversal kernels' FP32
+ * roofline fraction. */
+int rc_measure_fp32_peak(int device, double* tflops_out);
 /* Selects the path-tracer engine; both give identical results in exact math.
  * chunk_paths bounds the wavefront's in-flight paths (path state is about
  * 200 bytes each); 0 picks the default. */

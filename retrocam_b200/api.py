@@ -141,6 +141,7 @@ _SIGNATURES = {
     "rc_read_photon_map": (_I, [_VP, _VP, _I, _VP, _I, _VP, _VP]),
     "rc_get_counters": (_I, [_VP, _VP]),
     "rc_reset_counters": (_I, [_VP]),
+    "rc_measure_fp32_peak": (_I, [_I, C.POINTER(C.c_double)]),
     "rc_denoise_learned": (_I, [_VP, _VP, _VP]),
     "rc_kp_features": (_I, [_VP, _VP, _VP]),
     "rc_kp_conv3x3": (_I, [_VP, _I, _VP, _VP, _VP, _I, _I, _VP, _I, _I, _I, _VP, _VP]),

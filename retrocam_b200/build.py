@@ -69,7 +69,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 o = os.path.join(BUILD, f"{src}_{name.split('_')[1]}.o")
                 _run(common + flags + ["-c", os.path.join(CSRC, src + ".cu"), "-o", o], log)
                 objs.append(o)
-        for name in ("api", "noalloc", "kpcnn"):
+        for name in ("api", "noalloc", "kpcnn", "peak"):
             o = os.path.join(BUILD, name + ".o")
             _run(common + ["-c", os.path.join(CSRC, name + ".cu"), "-o", o], log)
             objs.append(o)
