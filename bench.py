@@ -552,10 +552,94 @@ def run_b200(args):
     return 0
 
 
+def run_keyframes(args):
+    """The batched keyframe export: 64 frames of the export frame's scene on a
+    keyframed orbit (spp U{8..128}, SPPM iterations U{4..16}), one
+    rc_render_frames call per step under a CUDA graph.  value = samples of
+    all frames / device time of the batch; e2e adds the read-back of every
+    finished frame to host memory."""
+    import torch
+    from retrocam_b200 import api, autotune, build, scenes
+    rank, local_rank, world = dist_env()
+    build.build()
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    dist = init_dist(world, "nccl")
+    w = scenes.export_frame()
+    sc = api.build_scene(w.scene)
+    frames = scenes.keyframe_batch(api.HOST, 64, 1)
+    sppm = api.rc_sppm_params(w.sppm.photons, w.sppm.hash_size, w.sppm.alpha)
+    atrous = api.atrous_params(w.atrous)
+    settings = (w.nee_enabled, w.nee_firefly_clamp)
+    ctx = api.Context(w.width, w.height, local_rank, api.RC_MATH_FAST)
+    stream = torch.cuda.Stream(device=device)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.upload(sc)
+    key = autotune.cache_key(torch.cuda.get_device_name(device), w.width, w.height, api.RC_MATH_FAST,
+                             autotune.scene_signature(sc))
+    t = autotune.TuningCache().get(key)
+    if t:
+        ctx.set_tuning(**t)
+    samples = sum(s for _, s, _ in frames) * w.width * w.height
+
+    def step(read=False):
+        return ctx.render_frames(frames, settings, sppm, w.sppm.r0, atrous, use_graph=True, read=read)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    ctx.reset_counters()
+    barrier(dist, device)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    clock_info = clocks.stop()
+    t_ms = max_over_ranks(ev0.elapsed_time(ev1), dist, device) / args.steps
+    ctr = ctx.counters()
+    if ctr["error_word"]:
+        raise RuntimeError(f"kernel guard raised: {ctr['error_word']:#x}")
+    launches = int(ctr["kernel_launches"]) // args.steps
+    ctx.reset_counters()
+    barrier(dist, device)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(read=True)
+    e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dist, device) / args.steps
+    ectr = ctx.counters()
+    line = {"metric": METRIC, "value": samples * world / (t_ms / 1e3) / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded procedural scene and keyframes, no dataset)",
+            "config": {"workload": "keyframes", "frames": len(frames), "width": w.width, "height": w.height,
+                       "spp_total": sum(s for _, s, _ in frames),
+                       "sppm_iterations_total": sum(i for _, _, i in frames),
+                       "photon_maps_traced_per_batch": max(i for _, _, i in frames),
+                       "graph": True, "tuning": ctx.tuning(), "parallelism": f"replicas x{world}"},
+            "e2e": {"value": samples * world / (e_ms / 1e3) / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": ectr["h2d_bytes"] // args.steps,
+                    "d2h_bytes_per_step": ectr["d2h_bytes"] // args.steps,
+                    "includes": "rc_render_frames with all 64 finished frames read back to host memory"},
+            "gpu_launches": launches, "clocks": clock_info}
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "keyframes":
+        return run_keyframes(args)
     return run_b200(args)
 
 

@@ -403,14 +403,26 @@ typedef struct rc_frame_desc {
     int32_t sppm_iterations;
 } rc_frame_desc;
 
-/* Renders n_frames frames of uneven cost back to back, each exactly as
- * rc_render_frame would, and writes the finished (denoised) frames to
+/* Renders n_frames frames of uneven cost, each with the samples, gathers and
+ * denoise rc_render_frame would give it (per frame: SPPM iteration k traces
+ * a photon map, renders sample slice [k*spp/it, (k+1)*spp/it), gathers with
+ * that slice's weight, shrinks the radius), and writes the finished frames to
  * out_frames (n_frames*W*H*4 floats, host; NULL keeps them on the device).
- * Every buffer the sequence needs is sized before the first frame.  With
- * use_graph != 0 the whole sequence is captured once into a CUDA graph and
- * replayed on later calls with the same frames and settings, so the host
- * issues one launch per batch.  Several contexts on their own streams may
- * render disjoint batches concurrently. */
+ *
+ * With the wavefront engines the frames run together: iteration k traces
+ * ONE photon map for all frames (it depends only on the scene, k and r_k),
+ * then slice k of every frame is packed into shared wavefront chunks (each
+ * chunk a list of (frame, sample range) segments, so frames of few samples
+ * fill chunks with others) and gathered into each frame.  Per frame the
+ * additions happen in rc_render_frame's order, so exact math gives its
+ * bits up to the photon-hash insertion order that the gather sums in.
+ * The megakernel engine renders the frames one after the other.
+ *
+ * Every buffer is sized before the first launch.  With use_graph != 0 the
+ * whole batch is captured once into a CUDA graph and replayed on later
+ * calls with the same frames, settings and launch shape, so the host issues
+ * one launch per batch.  Several contexts on their own streams may render
+ * disjoint batches concurrently. */
 int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames,
                      const rc_settings* settings, const rc_sppm_params* sppm,
                      float sppm_initial_radius, const rc_atrous_params* atrous,

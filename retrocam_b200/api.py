@@ -65,6 +65,10 @@ class rc_settings(C.Structure):
     _fields_ = [("nee_enabled", C.c_int32), ("nee_firefly_clamp", C.c_float)]
 
 
+class rc_frame_desc(C.Structure):
+    _fields_ = [("camera", rc_camera), ("spp", C.c_int32), ("sppm_iterations", C.c_int32)]
+
+
 class rc_sppm_params(C.Structure):
     _fields_ = [("photon_count", C.c_int32), ("hash_size", C.c_int32), ("alpha", C.c_float)]
 
@@ -246,6 +250,13 @@ class HostScene:
         _check(lib().rc_orbit_basis(theta, phi, radius, *map(float, target), _p(out)))
         return out
 
+    def keyframe(self, times, values, interp, t, default=0.0):
+        """KeyframeTrack.evaluate: interp 0 STEP, 1 LINEAR, 2 BEZIER."""
+        tt = np.ascontiguousarray(times, np.float32)
+        vv = np.ascontiguousarray(values, np.float32)
+        ii = np.ascontiguousarray(interp, np.int32)
+        return float(lib().rc_keyframe_evaluate(_p(tt), _p(vv), _p(ii), len(tt), float(t), float(default)))
+
 
 HOST = HostScene()
 
@@ -341,6 +352,20 @@ class Context:
     def denoise(self, params: rc_atrous_params, read=True):
         out = np.zeros((self.height, self.width, 4), np.float32) if read else None
         self.check(lib().rc_denoise_atrous(self.h, C.byref(params), _p(out)))
+        return out
+
+    def render_frames(self, frames, settings, sppm: rc_sppm_params | None, r0, atrous: rc_atrous_params,
+                      use_graph=True, read=True):
+        """rc_render_frames over [(camera dict, spp, sppm_iterations), ...];
+        returns the (n, H, W, 4) finished frames when `read`."""
+        n = len(frames)
+        arr = (rc_frame_desc * n)()
+        for i, (cam, spp, iters) in enumerate(frames):
+            arr[i] = rc_frame_desc(camera_struct(cam), int(spp), int(iters))
+        out = np.zeros((n, self.height, self.width, 4), np.float32) if read else None
+        self.check(lib().rc_render_frames(self.h, arr, n, C.byref(rc_settings(*settings)),
+                                          C.byref(sppm) if sppm is not None else None, r0, C.byref(atrous),
+                                          _p(out), 1 if use_graph else 0))
         return out
 
     def denoise_learned(self, params: np.ndarray, read=True):

@@ -105,6 +105,7 @@ struct rc_ctx {
     int wf_capacity = 0;
     // batched frames (rc_render_frames) and their captured graph
     DevBuf frames;
+    DevBuf batch_img, batch_segs;   // per-frame images and chunk segments of a batch
     // learned denoiser scratch
     DevBuf kp_feat, kp_act0, kp_act1, kp_logits, kp_color, kp_params, kp_packed;
     std::vector<float> kp_host;   // parameters last uploaded to kp_params
@@ -284,7 +285,7 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
                       &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->frames,
                       &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
-                      &ctx->kp_params, &ctx->kp_packed})
+                      &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs})
         release(*b);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -651,21 +652,16 @@ static int wavefront_reserve(rc_ctx* ctx, long cap) {
     return RC_OK;
 }
 
-static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
+// Path state of the wavefront engine and the chunk-invariant launch fields.
+static WaveArgs wave_args(rc_ctx* ctx, const DeviceScene& scene, int nee_enabled, float firefly_clamp) {
     const int W = ctx->width, H = ctx->height;
     const int tiles_x = (W + 7) / 8, tiles_y = (H + 3) / 4;
-    const int npix = tiles_x * tiles_y * 32;
-    const bool lca = lca_active(R.cam);
-    const int C = lca ? 3 : 1;
-    const long per_sample = (long)npix * C;
-    int ns = 1;
-    const long cap = wavefront_capacity(ctx, R.n_spp, lca, &ns);
-    const int rr = wavefront_reserve(ctx, cap);
-    if (rr != RC_OK) return rr;
     WaveArgs A;
-    A.scene = R.scene;
-    A.img = R.img;
-    A.cam = R.cam;
+    A.scene = scene;
+    A.segs = nullptr;
+    A.nsegs = 1;
+    A.width = W;
+    A.height = H;
     WaveBuffers& B = A.wb;
     B.o = (float4*)ctx->wf_o.ptr;
     B.d = (float4*)ctx->wf_d.ptr;
@@ -682,41 +678,63 @@ static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
     B.srec[1] = (float4*)ctx->wf_srec1.ptr;
     B.qlen = (unsigned int*)ctx->wf_qlen.ptr;
     B.capacity = ctx->wf_capacity;
-    A.nee_enabled = R.nee_enabled;
-    A.firefly_clamp = R.firefly_clamp;
-    A.channels = C;
+    A.nee_enabled = nee_enabled;
+    A.firefly_clamp = firefly_clamp;
     A.tiles_x = tiles_x;
-    A.npix = npix;
-    A.counters = R.counters;
+    A.npix = tiles_x * tiles_y * 32;
+    A.counters = ctx->counters;
     A.dynamic_fetch = ctx->engine == RC_ENGINE_WAVEFRONT ? 1 : 0;
+    A.bounce = 0;
+    return A;
+}
+
+// One chunk: generate, 7 traces and 6 shades interleaved, accumulate.
+static int wavefront_chunk(rc_ctx* ctx, WaveArgs& A) {
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    A.bounce = 0;
+    cudaError_t e = timed_launch(ctx, RC_KERNEL_WF_GENERATE, [&] {
+        return ex ? exact::launch_wf_generate(A, ctx->stream) : fast::launch_wf_generate(A, ctx->stream);
+    });
+    if (e != cudaSuccess) return launch_err(ctx, e, "wavefront generate");
+    for (int b = 0; b <= 6; ++b) {
+        A.bounce = b;
+        e = timed_launch(ctx, RC_KERNEL_WF_TRACE, [&] {
+            return ex ? exact::launch_wf_trace(A, ctx->stream, ctx->trace_block)
+                      : fast::launch_wf_trace(A, ctx->stream, ctx->trace_block);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront trace");
+        if (b == 6) break;
+        e = timed_launch(ctx, RC_KERNEL_WF_SHADE, [&] {
+            return ex ? exact::launch_wf_shade(A, ctx->stream, ctx->shade_block)
+                      : fast::launch_wf_shade(A, ctx->stream, ctx->shade_block);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront shade");
+    }
+    e = timed_launch(ctx, RC_KERNEL_WF_ACCUMULATE, [&] {
+        return ex ? exact::launch_wf_accumulate(A, ctx->stream) : fast::launch_wf_accumulate(A, ctx->stream);
+    });
+    if (e != cudaSuccess) return launch_err(ctx, e, "wavefront accumulate");
+    return RC_OK;
+}
+
+static int wavefront_render(rc_ctx* ctx, const RenderArgs& R) {
+    const bool lca = lca_active(R.cam);
+    const int C = lca ? 3 : 1;
+    int ns = 1;
+    const long cap = wavefront_capacity(ctx, R.n_spp, lca, &ns);
+    const int rr = wavefront_reserve(ctx, cap);
+    if (rr != RC_OK) return rr;
+    WaveArgs A = wave_args(ctx, R.scene, R.nee_enabled, R.firefly_clamp);
+    A.one.img = R.img;
+    A.one.cam = R.cam;
+    A.one.channels = C;
+    A.one.path_base = 0;
     for (int s0 = 0; s0 < R.n_spp; s0 += ns) {
-        A.first_frame = R.first_frame + s0;
-        A.n_samples = std::min(ns, R.n_spp - s0);
-        A.paths = (int)(per_sample * A.n_samples);
-        A.bounce = 0;
-        cudaError_t e = timed_launch(ctx, RC_KERNEL_WF_GENERATE, [&] {
-            return ex ? exact::launch_wf_generate(A, ctx->stream) : fast::launch_wf_generate(A, ctx->stream);
-        });
-        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront generate");
-        for (int b = 0; b <= 6; ++b) {
-            A.bounce = b;
-            e = timed_launch(ctx, RC_KERNEL_WF_TRACE, [&] {
-                return ex ? exact::launch_wf_trace(A, ctx->stream, ctx->trace_block)
-                          : fast::launch_wf_trace(A, ctx->stream, ctx->trace_block);
-            });
-            if (e != cudaSuccess) return launch_err(ctx, e, "wavefront trace");
-            if (b == 6) break;
-            e = timed_launch(ctx, RC_KERNEL_WF_SHADE, [&] {
-                return ex ? exact::launch_wf_shade(A, ctx->stream, ctx->shade_block)
-                          : fast::launch_wf_shade(A, ctx->stream, ctx->shade_block);
-            });
-            if (e != cudaSuccess) return launch_err(ctx, e, "wavefront shade");
-        }
-        e = timed_launch(ctx, RC_KERNEL_WF_ACCUMULATE, [&] {
-            return ex ? exact::launch_wf_accumulate(A, ctx->stream) : fast::launch_wf_accumulate(A, ctx->stream);
-        });
-        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront accumulate");
+        A.one.first_frame = R.first_frame + s0;
+        A.one.n_samples = std::min(ns, R.n_spp - s0);
+        A.paths = (int)((long)A.npix * C * A.one.n_samples);
+        const int r = wavefront_chunk(ctx, A);
+        if (r != RC_OK) return r;
     }
     return RC_OK;
 }
@@ -1099,6 +1117,149 @@ int rc_reset_counters(rc_ctx* ctx) {
 // ---------------------------------------------------------------------------
 // Batched export frames (keyframed animations)
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Batched frames: every frame's SPPM iteration k uses the same photon map
+// (the map depends on the scene, the iteration seed k*7919+6271 and the
+// radius r_k only), so iteration k traces it once and then renders slice k
+// of EVERY frame -- packed into shared wavefront chunks as segments -- and
+// gathers it into each frame.  Per frame, the samples and gathers are added
+// in the order rc_render_frame adds them.
+// ---------------------------------------------------------------------------
+struct BatchChunk {
+    int iteration;
+    int seg_begin, seg_count;
+    long paths;
+};
+
+struct BatchPlan {
+    std::vector<FrameSeg> segs;
+    std::vector<BatchChunk> chunks;
+    int iterations = 0;
+    long capacity = 0;
+};
+
+static int slices_of(const rc_frame_desc& d) { return d.sppm_iterations > 0 ? d.sppm_iterations : 1; }
+
+static void slice_range(const rc_frame_desc& d, int k, int& s0, int& s1) {
+    const int it = slices_of(d);
+    s0 = (int)((long)k * d.spp / it);
+    s1 = (int)((long)(k + 1) * d.spp / it);
+}
+
+static Images frame_images(rc_ctx* ctx, int f) {
+    const size_t px = (size_t)ctx->width * ctx->height;
+    char* base = (char*)ctx->batch_img.ptr;
+    Images im;
+    im.width = ctx->width;
+    im.height = ctx->height;
+    im.accum = (float4*)base + (size_t)f * px;
+    char* after_accum = base + ctx->batch_img.bytes / 36 * 16;
+    im.gbuf = (ushort4*)after_accum + (size_t)f * px;
+    char* after_gbuf = after_accum + ctx->batch_img.bytes / 36 * 8;
+    im.galb = (ushort4*)after_gbuf + (size_t)f * px;
+    char* after_galb = after_gbuf + ctx->batch_img.bytes / 36 * 8;
+    im.var = (float*)after_galb + (size_t)f * px;
+    return im;
+}
+
+// Plans the chunks: per iteration, slices of all frames in frame order,
+// split at sample boundaries so no chunk exceeds the wavefront capacity.
+static BatchPlan plan_batch(rc_ctx* ctx, const rc_frame_desc* frames, int n) {
+    BatchPlan P;
+    const int tiles_x = (ctx->width + 7) / 8, tiles_y = (ctx->height + 3) / 4;
+    const long npix = (long)tiles_x * tiles_y * 32;
+    const long cap = ctx->chunk_paths > 0 ? ctx->chunk_paths : kDefaultChunkPaths;
+    for (int f = 0; f < n; ++f) P.iterations = std::max(P.iterations, slices_of(frames[f]));
+    for (int k = 0; k < P.iterations; ++k) {
+        BatchChunk cur{k, (int)P.segs.size(), 0, 0};
+        for (int f = 0; f < n; ++f) {
+            const rc_frame_desc& d = frames[f];
+            if (k >= slices_of(d)) continue;
+            int s0, s1;
+            slice_range(d, k, s0, s1);
+            const CamParams cam = cam_params(&d.camera);
+            const int C = lca_active(cam) ? 3 : 1;
+            const long per_sample = npix * C;
+            while (s0 < s1) {
+                long room = (cap - cur.paths) / per_sample;
+                if (room < 1 && cur.seg_count > 0) {   // close the chunk
+                    P.chunks.push_back(cur);
+                    P.capacity = std::max(P.capacity, cur.paths);
+                    cur = BatchChunk{k, (int)P.segs.size(), 0, 0};
+                    room = cap / per_sample;
+                }
+                const int take = (int)std::max<long>(1, std::min<long>(room, s1 - s0));
+                FrameSeg sg;
+                sg.cam = cam;
+                sg.img = frame_images(ctx, f);
+                sg.first_frame = s0;
+                sg.n_samples = take;
+                sg.channels = C;
+                sg.path_base = (int)cur.paths;
+                P.segs.push_back(sg);
+                cur.seg_count++;
+                cur.paths += per_sample * take;
+                s0 += take;
+            }
+        }
+        if (cur.seg_count > 0) {
+            P.chunks.push_back(cur);
+            P.capacity = std::max(P.capacity, cur.paths);
+        }
+    }
+    return P;
+}
+
+static int batched_sequence(rc_ctx* ctx, const rc_frame_desc* frames, int n, const rc_settings* settings,
+                            const rc_sppm_params* sppm, float r0, const rc_atrous_params* atrous,
+                            const BatchPlan& P) {
+    const size_t px = (size_t)ctx->width * ctx->height;
+    const Images saved_img = ctx->img;
+    float4* const saved_out = ctx->out;
+    const bool sppm_on = sppm && ctx->scene.light_count > 0;
+    int r = RC_OK;
+    if (sppm_on && (r = rc_sppm_reset(ctx, r0)) != RC_OK) return r;
+    const FrameSeg* segs_dev = (const FrameSeg*)ctx->batch_segs.ptr;
+    size_t ci = 0;
+    for (int k = 0; k < P.iterations && r == RC_OK; ++k) {
+        bool gather_k = false;
+        for (int f = 0; f < n; ++f) gather_k = gather_k || (frames[f].sppm_iterations > k);
+        gather_k = gather_k && sppm_on;
+        if (gather_k && (r = rc_sppm_trace(ctx, sppm)) != RC_OK) break;
+        for (; ci < P.chunks.size() && P.chunks[ci].iteration == k; ++ci) {
+            const BatchChunk& c = P.chunks[ci];
+            WaveArgs A = wave_args(ctx, scene_for(ctx, RC_WIDE_PATHS), settings->nee_enabled,
+                                   settings->nee_firefly_clamp);
+            A.segs = segs_dev + c.seg_begin;
+            A.nsegs = c.seg_count;
+            A.one = P.segs[c.seg_begin];
+            A.paths = (int)c.paths;
+            if ((r = wavefront_chunk(ctx, A)) != RC_OK) break;
+        }
+        if (r != RC_OK) break;
+        if (gather_k) {
+            for (int f = 0; f < n && r == RC_OK; ++f) {
+                if (frames[f].sppm_iterations <= k) continue;
+                int s0, s1;
+                slice_range(frames[f], k, s0, s1);
+                ctx->img = frame_images(ctx, f);
+                r = rc_sppm_gather(ctx, &frames[f].camera, sppm, (float)(s1 - s0));
+            }
+            if (r == RC_OK) r = rc_sppm_update_radius(ctx, sppm->alpha);
+        }
+    }
+    for (int f = 0; f < n && r == RC_OK; ++f) {
+        ctx->img = frame_images(ctx, f);
+        ctx->total_samples = frames[f].spp;
+        ctx->out = (float4*)ctx->frames.ptr + (size_t)f * px;
+        r = rc_denoise_atrous(ctx, atrous, nullptr);
+    }
+    ctx->img = saved_img;
+    ctx->out = saved_out;
+    ctx->result = (float4*)ctx->frames.ptr + (size_t)(n - 1) * px;
+    return r;
+}
+
 static uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
     const unsigned char* c = (const unsigned char*)p;
     for (size_t i = 0; i < n; ++i) {
@@ -1124,6 +1285,7 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
     const size_t px = (size_t)ctx->width * ctx->height;
     // ---- reserve every buffer the sequence touches (no allocation may
     //      happen while the stream is being captured) ----
+    const bool batched = ctx->engine != RC_ENGINE_MEGAKERNEL;
     long cap = 0;
     bool any_sppm = false;
     for (int f = 0; f < n_frames; ++f) {
@@ -1132,6 +1294,18 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
         const int block = it > 0 ? (d.spp + it - 1) / it : d.spp;
         cap = std::max(cap, wavefront_capacity(ctx, block, lca_active(cam_params(&d.camera)), nullptr));
         any_sppm = any_sppm || (it > 0);
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    BatchPlan plan;
+    if (batched) {
+        // per-frame images: accum | gbuf | galb | var regions of n_frames x px
+        CK(ensure(ctx->batch_img, (size_t)n_frames * px * 36));
+        plan = plan_batch(ctx, frames, n_frames);
+        cap = std::max(cap, plan.capacity);
+        CK(ensure(ctx->batch_segs, plan.segs.size() * sizeof(FrameSeg)));
+        CK(cudaMemcpy(ctx->batch_segs.ptr, plan.segs.data(), plan.segs.size() * sizeof(FrameSeg),
+                      cudaMemcpyHostToDevice));
+        ctx->h2d += plan.segs.size() * sizeof(FrameSeg);
     }
     if (ctx->engine != RC_ENGINE_MEGAKERNEL) {
         const int r = wavefront_reserve(ctx, cap);
@@ -1146,6 +1320,8 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
     CK(cudaStreamSynchronize(ctx->stream));
     // ---- the sequence ----
     auto sequence = [&]() -> int {
+        if (batched)
+            return batched_sequence(ctx, frames, n_frames, settings, sppm, sppm_initial_radius, atrous, plan);
         for (int f = 0; f < n_frames; ++f) {
             const rc_frame_desc& d = frames[f];
             int r = rc_render_frame(ctx, &d.camera, settings, d.spp, sppm, sppm_initial_radius, d.sppm_iterations,
@@ -1171,6 +1347,16 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
         key = fnv1a(key, &ctx->math_mode, sizeof(int));
         key = fnv1a(key, &ctx->stream, sizeof(void*));
         key = fnv1a(key, &ctx->frames.ptr, sizeof(void*));
+        key = fnv1a(key, &ctx->batch_img.ptr, sizeof(void*));
+        key = fnv1a(key, &ctx->batch_segs.ptr, sizeof(void*));
+        key = fnv1a(key, &ctx->wf_o.ptr, sizeof(void*));
+        for (const DevBuf* b : {&ctx->photons, &ctx->heads, &ctx->next, &ctx->cell_of, &ctx->cell_count,
+                                &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw,
+                                &ctx->seg_powyz})
+            key = fnv1a(key, &b->ptr, sizeof(void*));
+        const int shape[6] = {ctx->chunk_paths, ctx->wide_bvh, ctx->trace_block, ctx->shade_block,
+                              ctx->photon_block, ctx->width};
+        key = fnv1a(key, shape, sizeof(shape));
         if (!ctx->graph_exec || ctx->graph_key != key) {
             if (ctx->graph_exec) {
                 cudaGraphExecDestroy(ctx->graph_exec);

@@ -191,19 +191,33 @@ struct WaveBuffers {
     int capacity;     // paths per chunk
 };
 
+// One frame's share of a wavefront chunk: samples [first_frame,
+// first_frame + n_samples) of the frame with camera `cam` and images `img`,
+// occupying paths [path_base, path_base + npix * channels * n_samples) of
+// the chunk (path = path_base + tiled pixel + npix * (channel + channels *
+// sample)).  A chunk of a single render call has one segment; a batch of
+// frames packs slices of many frames into one chunk.
+struct FrameSeg {
+    CamParams cam;
+    Images img;
+    int first_frame;
+    int n_samples;
+    int channels;      // 3 with per-channel lens offsets, else 1
+    int path_base;
+};
+
 struct WaveArgs {
     DeviceScene scene;
-    Images img;
-    CamParams cam;
     WaveBuffers wb;
+    FrameSeg one;            // the segment when segs == nullptr
+    const FrameSeg* segs;    // nsegs segments sorted by path_base, or null
+    int nsegs;
+    int width, height;       // image size of every segment
     int nee_enabled;
     float firefly_clamp;
-    int first_frame;   // frame index of the chunk's first sample
-    int n_samples;     // samples in this chunk
-    int channels;      // 3 with per-channel lens offsets, else 1
     int tiles_x;       // 8x4-pixel tiles across
     int npix;          // tiles * 32
-    int paths;         // npix * channels * n_samples
+    int paths;         // paths of the chunk (all segments)
     int bounce;
     int dynamic_fetch; // fast build: persistent trace kernel with ray refill
     DevCounters* counters;

@@ -43,16 +43,33 @@ struct PathId {
     bool valid;
 };
 
-DI PathId decode(const WaveArgs& A, int p) {
+// The segment holding chunk path p (binary search over path_base).
+DI int seg_index(const WaveArgs& A, int p) {
+    if (!A.segs) return 0;
+    int lo = 0, hi = A.nsegs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&A.segs[mid].path_base) <= p)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+DI const FrameSeg& seg_at(const WaveArgs& A, int i) { return A.segs ? A.segs[i] : A.one; }
+
+DI PathId decode(const WaveArgs& A, const FrameSeg& sg, int p) {
     PathId id;
-    const int j = p % A.npix;
-    const int k = p / A.npix;
-    id.channel = k % A.channels;
-    id.sample = k / A.channels;
+    const int local = p - sg.path_base;
+    const int j = local % A.npix;
+    const int k = local / A.npix;
+    id.channel = k % sg.channels;
+    id.sample = k / sg.channels;
     const int tile = j >> 5, lane = j & 31;
     id.px = (tile % A.tiles_x) * 8 + (lane & 7);
     id.py = (tile / A.tiles_x) * 4 + (lane >> 3);
-    id.valid = id.px < A.img.width && id.py < A.img.height;
+    id.valid = id.px < A.width && id.py < A.height;
     return id;
 }
 
@@ -60,16 +77,17 @@ DI bool lca_on(const CamParams& c) { return (fabs_(c.lca[0]) + fabs_(c.lca[2])) 
 
 __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
     const WaveBuffers& B = A.wb;
-    const bool lca = A.channels == 3;
     uint32_t paths = 0;
     for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.paths; p += gridDim.x * blockDim.x) {
-        const PathId id = decode(A, p);
+        const FrameSeg& sg = seg_at(A, seg_index(A, p));
+        const PathId id = decode(A, sg, p);
+        const bool lca = sg.channels == 3;
         bool want = false;
         if (id.valid) {
-            const int f = A.first_frame + id.sample;
+            const int f = sg.first_frame + id.sample;
             uint32_t s = init_seed(id.px, id.py, lca ? f * 3 + id.channel : f);
-            const Ray r = generate_ray(A.cam, A.img.width, A.img.height, id.px, id.py, s,
-                                       lca ? A.cam.lca[id.channel] : 0.0f);
+            const Ray r = generate_ray(sg.cam, A.width, A.height, id.px, id.py, s,
+                                       lca ? sg.cam.lca[id.channel] : 0.0f);
             B.o[p] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
             B.d[p] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
             B.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -156,13 +174,17 @@ __global__ void __launch_bounds__(256) wf_shade(WaveArgs A) {
         bool cont = false, shadow_rec = false;
         float4 rec0, rec1, rec2, rec3;
         // frame-0 albedo image: first hit of the G channel (or the only one)
-        const bool alb_path = b == 0 && A.first_frame + (p / A.npix) / A.channels == 0 &&
-                              ((p / A.npix) % A.channels) == (A.channels == 3 ? 1 : 0);
+        bool alb_path = false;
+        PathId id;
+        ushort4* galb = nullptr;
+        if (b == 0) {
+            const FrameSeg& sg = seg_at(A, seg_index(A, p));
+            id = decode(A, sg, p);
+            alb_path = sg.first_frame + id.sample == 0 && id.channel == (sg.channels == 3 ? 1 : 0);
+            galb = sg.img.galb;
+        }
         if (prim < 0) {
-            if (alb_path) {
-                const PathId id = decode(A, p);
-                A.img.galb[(long)id.py * A.img.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
-            }
+            if (alb_path) galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
             B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
         } else {
             ++hits;
@@ -181,8 +203,7 @@ __global__ void __launch_bounds__(256) wf_shade(WaveArgs A) {
             const bool last_diffuse = B.thr[p].w != 0.0f;
             if (alb_path) {
                 const float3 a = (m.transmission > 0.5f) ? f3(1.0f, 1.0f, 1.0f) : m.albedo;
-                const PathId id = decode(A, p);
-                A.img.galb[(long)id.py * A.img.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
+                galb[(long)id.py * A.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
             }
             if (!last_diffuse) rad = rad + (thr * m.emission) * m.strength;
             bool alive = true;
@@ -344,25 +365,31 @@ __global__ void __launch_bounds__(256) wf_shade(WaveArgs A) {
 // pathtrace.comp:633-654 per pixel for the chunk's samples, in frame order;
 // on frame 0 also the G-buffer ray (seed 99991, no lens offset).
 __global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
-    const int W = A.img.width, H = A.img.height;
+    const int W = A.width, H = A.height;
     Guard g = {0u, 0u, 0u};
     uint32_t closest = 0, ghits = 0;
-    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < A.npix; j += gridDim.x * blockDim.x) {
+    const int nsegs = A.segs ? A.nsegs : 1;
+    const int items = nsegs * A.npix;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < items; t += gridDim.x * blockDim.x) {
+        const int j = t % A.npix;
+        const FrameSeg& sg = seg_at(A, t / A.npix);
         const int tile = j >> 5, lane = j & 31;
         const int px = (tile % A.tiles_x) * 8 + (lane & 7);
         const int py = (tile / A.tiles_x) * 4 + (lane >> 3);
         if (px >= W || py >= H) continue;
         const long i = (long)py * W + px;
+        const Images& img = sg.img;
+        const int C = sg.channels;
         float4 acc = make_float4(0, 0, 0, 0);
         float var = 0.0f;
-        if (A.first_frame > 0) {
-            acc = A.img.accum[i];
-            var = A.img.var[i];
+        if (sg.first_frame > 0) {
+            acc = img.accum[i];
+            var = img.var[i];
         }
-        for (int s = 0; s < A.n_samples; ++s) {
-            const int base = j + A.npix * (A.channels * s);
+        for (int s = 0; s < sg.n_samples; ++s) {
+            const int base = sg.path_base + j + A.npix * (C * s);
             float3 rad;
-            if (A.channels == 3) {
+            if (C == 3) {
                 rad = f3(A.wb.res[base].x, A.wb.res[base + A.npix].y, A.wb.res[base + 2 * A.npix].z);
             } else {
                 rad = xyz(A.wb.res[base]);
@@ -370,11 +397,11 @@ __global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
             if (bad(rad.x) || bad(rad.y) || bad(rad.z)) rad = f3(0, 0, 0);
             const float l = luma709(rad);
             const float l2 = l * l;
-            if (A.first_frame + s == 0) {
+            if (sg.first_frame + s == 0) {
                 acc = make_float4(rad.x, rad.y, rad.z, 1.0f);
                 var = l2;
                 uint32_t gs = init_seed(px, py, 99991);
-                const Ray gr = generate_ray(A.cam, W, H, px, py, gs, 0.0f);
+                const Ray gr = generate_ray(sg.cam, W, H, px, py, gs, 0.0f);
                 ++closest;
                 const Hit h = closest_hit(A.scene, gr, g);
                 float4 gv = make_float4(0.0f, 1.0f, 0.0f, 1e4f);
@@ -384,7 +411,7 @@ __global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
                     const float3 nn = dot(gr.d, sf.normal) < 0.0f ? sf.normal : -sf.normal;
                     gv = make_float4(nn.x, nn.y, nn.z, h.t);
                 }
-                A.img.gbuf[i] = to_half4(gv.x, gv.y, gv.z, gv.w);
+                img.gbuf[i] = to_half4(gv.x, gv.y, gv.z, gv.w);
             } else {
                 acc.x = acc.x + rad.x;
                 acc.y = acc.y + rad.y;
@@ -393,8 +420,8 @@ __global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
                 var = var + l2;
             }
         }
-        A.img.accum[i] = acc;
-        A.img.var[i] = var;
+        img.accum[i] = acc;
+        img.var[i] = var;
     }
     const unsigned int active = __activemask();
     const unsigned int c = __reduce_add_sync(active, closest);

@@ -235,6 +235,48 @@ def export_frame() -> Workload:
                     sppm=SppmDesc(), atrous=AtrousDesc())
 
 
+@dataclass
+class KeyTrack:
+    """A keyframe track (keyframe/KeyframeTrack.java): times in [0, 1],
+    values, and per-key interpolation (0 STEP, 1 LINEAR, 2 BEZIER)."""
+    times: tuple
+    values: tuple
+    interp: tuple = (2, 2, 2, 2)
+
+
+# The keyframed orbit of the batched export: azimuth sweep of 90 degrees
+# centred on the front view, lens zoom, aperture and focus pulls.
+KEYFRAME_TRACKS = {
+    "azimuth_deg": KeyTrack((0.0, 1 / 3, 2 / 3, 1.0), (0.0, 30.0, 60.0, 90.0)),
+    "focal_mm": KeyTrack((0.0, 1 / 3, 2 / 3, 1.0), (20.0, 35.0, 50.0, 80.0)),
+    "f_stop": KeyTrack((0.0, 1 / 3, 2 / 3, 1.0), (1.8, 4.0, 8.0, 16.0)),
+    "focus_m": KeyTrack((0.0, 1 / 3, 2 / 3, 1.0), (1.0, 2.5, 1.5, 4.0)),
+}
+
+
+def keyframe_batch(backend, n_frames: int = 64, seed: int = 1):
+    """Frames of the batched keyframe export: (camera dict, spp, SPPM
+    iterations) per frame.  Cameras from the Catmull-Rom tracks above at
+    t = f / (n - 1) (orbit theta = front view - 45 deg + azimuth); spp drawn
+    from U{8..128} and SPPM iterations from U{4..16} (capped at spp) with an
+    MT19937 generator seeded `seed`; LCA offsets +-0.5% of the focus
+    distance, 6 blades, as in the export frame."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    spp = rng.integers(8, 129, n_frames)
+    iters = rng.integers(4, 17, n_frames)
+    frames = []
+    for f in range(n_frames):
+        t = f / max(1, n_frames - 1)
+        ev = {k: backend.keyframe(tr.times, tr.values, tr.interp, t) for k, tr in KEYFRAME_TRACKS.items()}
+        orbit = OrbitDesc(theta=CORNELL_ORBIT.theta + math.radians(ev["azimuth_deg"] - 45.0), phi=CORNELL_ORBIT.phi,
+                          radius=CORNELL_ORBIT.radius, target=CORNELL_ORBIT.target)
+        focus = ev["focus_m"]
+        lens = LensDesc(focal_length_mm=ev["focal_mm"], f_stop=ev["f_stop"], focus_dist_m=focus, blades=6,
+                        lca_delta=(-0.005 * focus, 0.0, 0.005 * focus))
+        frames.append((camera(orbit, lens, backend), int(spp[f]), int(min(iters[f], spp[f]))))
+    return frames
+
+
 def bvh_stress(n_tris: int = 1_000_000, seed: int = 1) -> Workload:
     """Seeded random triangles (numpy PCG64): centres U[0,1]^3, two edge
     lengths log-uniform in [1e-3, 5e-2] along random unit directions;

@@ -380,6 +380,55 @@ def test_render_frame_matches_reference_sequence(product, orc, c1):
     np.testing.assert_allclose(out, ref_out, rtol=1e-3, atol=1e-5)
 
 
+def _batch_frames(product, n, spps, iters):
+    from retrocam_b200 import scenes
+    frames = scenes.keyframe_batch(product.HOST, n_frames=n)
+    return [(cam, s, it) for (cam, _, _), s, it in zip(frames, spps, iters)]
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_batch_without_sppm_bit_identical_to_frames(product, c1, use_graph):
+    """A batch packs slices of several frames into shared chunks (here split
+    across many small chunks); without SPPM every frame is bit-identical to
+    its own rc_render_frame, with and without the CUDA graph."""
+    w, sc, cam = c1
+    W, H = 96, 64
+    frames = _batch_frames(product, 4, (3, 5, 2, 4), (0, 0, 0, 0))
+    p = product.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.set_tuning(chunk_paths=30_000)
+        ctx.upload(sc)
+        single = [ctx.render_frame(c, (1, 1.0), s, None, 0.02, 0, p) for c, s, _ in frames]
+        batch = ctx.render_frames(frames, (1, 1.0), None, 0.02, p, use_graph=use_graph)
+        again = ctx.render_frames(frames, (1, 1.0), None, 0.02, p, use_graph=use_graph)
+        assert ctx.counters()["error_word"] == 0
+    for f in range(len(frames)):
+        assert np.array_equal(bits(batch[f]), bits(single[f])), f
+    assert np.array_equal(bits(again), bits(batch))
+
+
+def test_batch_with_sppm_matches_frames(product, c1):
+    """With SPPM, iteration k's photon map is traced once for all frames;
+    each frame's slices, gathers and radius schedule follow rc_render_frame.
+    Only the hash-chain order of the gather sums differs (GPU atomics)."""
+    w, sc, cam = c1
+    W, H, N, hs = 96, 64, 100_000, 1 << 18
+    frames = _batch_frames(product, 3, (6, 4, 5), (3, 4, 0))
+    p = product.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)
+    sp = product.rc_sppm_params(N, hs, 0.7)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        single = [ctx.render_frame(c, (1, 1.0), s, sp, 0.02, it, p) for c, s, it in frames]
+        batch = ctx.render_frames(frames, (1, 1.0), sp, 0.02, p, use_graph=True)
+        assert ctx.counters()["error_word"] == 0
+    for f in range(len(frames)):
+        close = np.abs(batch[f] - single[f]) <= 1e-3 * np.abs(single[f]) + 1e-5
+        assert np.mean(close) > 0.999, (f, np.mean(close))
+        np.testing.assert_allclose(batch[f].mean(axis=(0, 1)), single[f].mean(axis=(0, 1)), rtol=1e-4)
+    # frame 2 has no SPPM: bit-identical
+    assert np.array_equal(bits(batch[2]), bits(single[2]))
+
+
 def test_errors_are_codes_not_crashes(product, c0):
     w, sc, cam = c0
     with _ctx(product, 32, 32, product.RC_MATH_FAST) as ctx:
