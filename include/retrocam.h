@@ -194,6 +194,10 @@ typedef struct rc_tuning {
     int32_t trace_block;   /* threads per block of the wavefront trace: 64, 128, 256 (0 = 128) */
     int32_t shade_block;   /* threads per block of the wavefront shade: 64, 128, 256 (0 = 128) */
     int32_t photon_block;  /* threads per block of the photon trace: 64, 128, 256 (0 = 128) */
+    int32_t photon_full_first; /* fast math: 0 traces a photon's first segment against the
+                                  specular triangles, then tests the others up to that hit
+                                  (a diffuse first hit ends the photon unstored, so only
+                                  the specular hit matters); 1 traces the whole scene */
 } rc_tuning;
 
 /* error_word bits. */

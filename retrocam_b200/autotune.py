@@ -36,6 +36,7 @@ KNOBS: dict[str, tuple[int, ...]] = {
     "trace_block": (64, 128, 256),
     "shade_block": (64, 128, 256),
     "photon_block": (64, 128, 256),
+    "photon_full_first": (0, 1),
 }
 
 

@@ -100,12 +100,17 @@ struct rc_ctx {
     int chunk_paths = 0;   // 0: default
     int wide_bvh = 0;
     int trace_block = 128, shade_block = 128, photon_block = 128;
+    int photon_full_first = 0;
     DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
         wf_qlen;
     int wf_capacity = 0;
     // batched frames (rc_render_frames) and their captured graph
     DevBuf frames;
     DevBuf batch_img, batch_segs;   // per-frame images and chunk segments of a batch
+    // photon first-segment split: specular / other triangles with own BVHs
+    DevBuf sp_nodes, sp_isect, sp_orig, df_nodes, df_isect, ph_queue, ph_queue_len;
+    DeviceScene spec_view, diff_view;
+    bool photon_split = false;
     // learned denoiser scratch
     DevBuf kp_feat, kp_act0, kp_act1, kp_logits, kp_color, kp_params, kp_packed;
     std::vector<float> kp_host;   // parameters last uploaded to kp_params
@@ -285,7 +290,9 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
                       &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->frames,
                       &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
-                      &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs})
+                      &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs, &ctx->sp_nodes,
+                      &ctx->sp_isect, &ctx->sp_orig, &ctx->df_nodes, &ctx->df_isect, &ctx->ph_queue,
+                      &ctx->ph_queue_len})
         release(*b);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -326,6 +333,74 @@ int rc_synchronize(rc_ctx* ctx) {
 }
 
 }  // extern "C"
+
+// The kernels' record of interior node n: both children's boxes and refs.
+static void node_record(const rc_bvh_node* nodes, const rc_bvh_node& n, NodeRec& r) {
+    const rc_bvh_node& L = nodes[n.left_child];
+    const rc_bvh_node& R = nodes[n.right_child];
+    r.a = make_float4(L.aabb_min[0], L.aabb_min[1], L.aabb_min[2], L.aabb_max[0]);
+    r.b = make_float4(L.aabb_max[1], L.aabb_max[2], R.aabb_min[0], R.aabb_min[1]);
+    r.c = make_float4(R.aabb_min[2], R.aabb_max[0], R.aabb_max[1], R.aabb_max[2]);
+    r.d = make_int4(L.prim_count > 0 ? L.prim_start : n.left_child, L.prim_count,
+                    R.prim_count > 0 ? R.prim_start : n.right_child, R.prim_count);
+}
+
+static void isect_record(const rc_triangle& t, float4* out3) {
+    // e1, e2 with the same float subtraction the reference does per test
+    out3[0] = make_float4(t.v0[0], t.v0[1], t.v0[2], 0.0f);
+    out3[1] = make_float4(t.v1[0] - t.v0[0], t.v1[1] - t.v0[1], t.v1[2] - t.v0[2], 0.0f);
+    out3[2] = make_float4(t.v2[0] - t.v0[0], t.v2[1] - t.v0[1], t.v2[2] - t.v0[2], 0.0f);
+}
+
+// A BVH (the reference's SAH builder) over a subset of the scene's
+// triangles, in the kernels' layout, with each subset triangle's index in
+// the full scene.
+struct SubsetBvh {
+    std::vector<NodeRec> recs;
+    std::vector<float4> isect;
+    std::vector<int> orig;
+    rc_bvh_node root;
+    int node_count = 0;
+};
+
+static bool build_subset(const std::vector<rc_triangle>& in, int scene_tris, SubsetBvh& out) {
+    const int n = (int)in.size();
+    std::vector<rc_triangle> tris(n);
+    std::vector<rc_bvh_node> nodes(2 * (size_t)n + 1);
+    int nn = 0;
+    if (n == 0 || rc_build_bvh(in.data(), n, tris.data(), nodes.data(), (int)nodes.size(), &nn) != RC_OK || nn < 1)
+        return false;
+    out.recs.assign(nn, NodeRec{});
+    for (int i = 0; i < nn; ++i)
+        if (nodes[i].prim_count <= 0) node_record(nodes.data(), nodes[i], out.recs[i]);
+    out.isect.resize(3 * (size_t)n);
+    out.orig.resize(n);
+    for (int i = 0; i < n; ++i) {
+        isect_record(tris[i], &out.isect[3 * (size_t)i]);
+        int o;
+        memcpy(&o, &tris[i].pad6, sizeof(int));   // the full-scene index rides in a pad field
+        if (o < 0 || o >= scene_tris) return false;
+        out.orig[i] = o;
+    }
+    out.root = nodes[0];
+    out.node_count = nn;
+    return true;
+}
+
+static DeviceScene subset_view(const SubsetBvh& b, const DevBuf& nodes, const DevBuf& isect) {
+    DeviceScene S;
+    S.nodes = (const NodeRec*)nodes.ptr;
+    S.tri_isect = (const float4*)isect.ptr;
+    S.node_count = b.node_count;
+    S.tri_count = (int)b.orig.size();
+    for (int a = 0; a < 3; ++a) {
+        S.root_min[a] = b.root.aabb_min[a];
+        S.root_max[a] = b.root.aabb_max[a];
+    }
+    S.root_ref = b.root.prim_count > 0 ? b.root.prim_start : 0;
+    S.root_count = b.root.prim_count;
+    return S;
+}
 
 // Collapses the binary BVH below interior node `bin` into 4-wide nodes,
 // pre-order, returning the index of the node made for `bin`.  A node takes
@@ -432,6 +507,10 @@ int rc_get_kernel_times(rc_ctx* ctx, double* ms_out, uint64_t* launches_out) {
     return RC_OK;
 }
 
+// Scenes up to this size also get the photon first-segment split (two more
+// host SAH builds at upload).
+static const int kSplitMaxTris = 1 << 18;
+
 int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const rc_bvh_node* nodes,
                     int node_count, const rc_material* mats, int material_count, const rc_light* lights,
                     int light_count, float total_light_power) {
@@ -475,14 +554,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     for (int i = 0; i < node_count; ++i) {
         const rc_bvh_node& n = nodes[i];
         if (n.prim_count > 0 || !seen[i] || (tri_count == 0)) continue;
-        const rc_bvh_node& L = nodes[n.left_child];
-        const rc_bvh_node& R = nodes[n.right_child];
-        NodeRec& r = recs[i];
-        r.a = make_float4(L.aabb_min[0], L.aabb_min[1], L.aabb_min[2], L.aabb_max[0]);
-        r.b = make_float4(L.aabb_max[1], L.aabb_max[2], R.aabb_min[0], R.aabb_min[1]);
-        r.c = make_float4(R.aabb_min[2], R.aabb_max[0], R.aabb_max[1], R.aabb_max[2]);
-        r.d = make_int4(L.prim_count > 0 ? L.prim_start : n.left_child, L.prim_count,
-                        R.prim_count > 0 ? R.prim_start : n.right_child, R.prim_count);
+        node_record(nodes, n, recs[i]);
     }
     // 4-wide copy for the fast build's traversal; a tree deeper than any SAH
     // build makes keeps the binary traversal (the collapse recurses per level).
@@ -491,10 +563,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     std::vector<float4> isect(3 * (size_t)tri_count), shade(3 * (size_t)tri_count);
     for (int i = 0; i < tri_count; ++i) {
         const rc_triangle& t = tris[i];
-        // e1, e2 with the same float subtraction the reference does per test
-        isect[3 * i + 0] = make_float4(t.v0[0], t.v0[1], t.v0[2], 0.0f);
-        isect[3 * i + 1] = make_float4(t.v1[0] - t.v0[0], t.v1[1] - t.v0[1], t.v1[2] - t.v0[2], 0.0f);
-        isect[3 * i + 2] = make_float4(t.v2[0] - t.v0[0], t.v2[1] - t.v0[1], t.v2[2] - t.v0[2], 0.0f);
+        isect_record(t, &isect[3 * (size_t)i]);
         float mbits;
         memcpy(&mbits, &t.mat_index, 4);
         shade[3 * i + 0] = make_float4(t.n0[0], t.n0[1], t.n0[2], mbits);
@@ -552,6 +621,35 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     S.root_ref = nodes[0].prim_count > 0 ? nodes[0].prim_start : 0;
     S.root_count = nodes[0].prim_count;
     S.depth = max_depth;
+    // ---- first-segment split of the photon trace (fast build): BVHs over
+    //      the specular (metal or glass) triangles and over the others ----
+    ctx->photon_split = false;
+    if (tri_count > 0 && tri_count <= kSplitMaxTris && light_count > 0) {
+        std::vector<rc_triangle> spec, diff;
+        for (int i = 0; i < tri_count; ++i) {
+            const rc_material& m = mats[tris[i].mat_index];
+            rc_triangle t = tris[i];
+            memcpy(&t.pad6, &i, sizeof(int));
+            (m.metallic > 0.5f || m.transmission > 0.5f ? spec : diff).push_back(t);
+        }
+        SubsetBvh sb, db;
+        if (!spec.empty() && !diff.empty() && build_subset(spec, tri_count, sb) && build_subset(diff, tri_count, db)) {
+            CK(ensure(ctx->sp_nodes, sb.recs.size() * sizeof(NodeRec)));
+            CK(ensure(ctx->sp_isect, sb.isect.size() * sizeof(float4)));
+            CK(ensure(ctx->sp_orig, sb.orig.size() * sizeof(int)));
+            CK(ensure(ctx->df_nodes, db.recs.size() * sizeof(NodeRec)));
+            CK(ensure(ctx->df_isect, db.isect.size() * sizeof(float4)));
+            CK(copy_h2d(ctx, ctx->sp_nodes.ptr, sb.recs.data(), sb.recs.size() * sizeof(NodeRec)));
+            CK(copy_h2d(ctx, ctx->sp_isect.ptr, sb.isect.data(), sb.isect.size() * sizeof(float4)));
+            CK(copy_h2d(ctx, ctx->sp_orig.ptr, sb.orig.data(), sb.orig.size() * sizeof(int)));
+            CK(copy_h2d(ctx, ctx->df_nodes.ptr, db.recs.data(), db.recs.size() * sizeof(NodeRec)));
+            CK(copy_h2d(ctx, ctx->df_isect.ptr, db.isect.data(), db.isect.size() * sizeof(float4)));
+            CK(cudaStreamSynchronize(ctx->stream));
+            ctx->spec_view = subset_view(sb, ctx->sp_nodes, ctx->sp_isect);
+            ctx->diff_view = subset_view(db, ctx->df_nodes, ctx->df_isect);
+            ctx->photon_split = true;
+        }
+    }
     ctx->has_scene = true;
     return RC_OK;
 }
@@ -579,15 +677,18 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
     if ((t->engine != RC_ENGINE_MEGAKERNEL && t->engine != RC_ENGINE_WAVEFRONT &&
          t->engine != RC_ENGINE_WAVEFRONT_STATIC) ||
         t->chunk_paths < 0 || (t->wide_bvh & ~(RC_WIDE_PATHS | RC_WIDE_PHOTONS)) || !valid_block(t->trace_block) ||
-        !valid_block(t->shade_block) || !valid_block(t->photon_block))
-        return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d", t->engine,
-                    t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block);
+        !valid_block(t->shade_block) || !valid_block(t->photon_block) ||
+        (t->photon_full_first != 0 && t->photon_full_first != 1))
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d first %d",
+                    t->engine, t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block,
+                    t->photon_full_first);
     ctx->engine = t->engine;
     ctx->chunk_paths = t->chunk_paths;
     ctx->wide_bvh = t->wide_bvh;
     ctx->trace_block = t->trace_block ? t->trace_block : 128;
     ctx->shade_block = t->shade_block ? t->shade_block : 128;
     ctx->photon_block = t->photon_block ? t->photon_block : 128;
+    ctx->photon_full_first = t->photon_full_first;
     return RC_OK;
 }
 
@@ -600,6 +701,7 @@ int rc_get_tuning(rc_ctx* ctx, rc_tuning* out) {
     out->trace_block = ctx->trace_block;
     out->shade_block = ctx->shade_block;
     out->photon_block = ctx->photon_block;
+    out->photon_full_first = ctx->photon_full_first;
     return RC_OK;
 }
 
@@ -823,6 +925,7 @@ static int photon_reserve(rc_ctx* ctx, const rc_sppm_params* p) {
         CK(ensure(ctx->seg_photon, (size_t)cap * sizeof(int)));
         CK(ensure(ctx->seg_posw, (size_t)cap * sizeof(float4)));
         CK(ensure(ctx->seg_powyz, (size_t)cap * sizeof(float2)));
+        CK(ensure(ctx->ph_queue, (size_t)cap * 4 * sizeof(float4)));
         ctx->photon_cap = cap;
     }
     if (p->hash_size > ctx->hash_cap) {
@@ -833,6 +936,7 @@ static int photon_reserve(rc_ctx* ctx, const rc_sppm_params* p) {
         ctx->hash_cap = p->hash_size;
     }
     CK(ensure(ctx->counter, sizeof(unsigned int)));
+    CK(ensure(ctx->ph_queue_len, sizeof(unsigned int)));
     return RC_OK;
 }
 
@@ -868,12 +972,21 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     A.hash_size = p->hash_size;
     A.radius = ctx->sppm_radius;
     A.seed = ctx->sppm_iteration * 7919 + 6271;
+    A.split = (ctx->math_mode == RC_MATH_FAST && ctx->photon_split && !ctx->photon_full_first) ? 1 : 0;
+    A.spec = ctx->spec_view;
+    A.diff = ctx->diff_view;
+    A.spec_orig = (const int*)ctx->sp_orig.ptr;
+    A.queue = (float4*)ctx->ph_queue.ptr;
+    A.queue_len = (unsigned int*)ctx->ph_queue_len.ptr;
     A.counters = ctx->counters;
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
-    cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_TRACE, [&] {
-        return ex ? exact::launch_photon_trace(A, ctx->stream, ctx->photon_block)
-                  : fast::launch_photon_trace(A, ctx->stream, ctx->photon_block);
-    });
+    cudaError_t e = timed_launch(
+        ctx, RC_KERNEL_PHOTON_TRACE,
+        [&] {
+            return ex ? exact::launch_photon_trace(A, ctx->stream, ctx->photon_block)
+                      : fast::launch_photon_trace(A, ctx->stream, ctx->photon_block);
+        },
+        A.split ? 2 : 1);
     if (e != cudaSuccess) return launch_err(ctx, e, "photon trace");
     e = timed_launch(ctx, RC_KERNEL_PHOTON_LAYOUT, [&] {
         return ex ? exact::launch_photon_layout(A, ctx->stream) : fast::launch_photon_layout(A, ctx->stream);
@@ -1352,7 +1465,7 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
         key = fnv1a(key, &ctx->wf_o.ptr, sizeof(void*));
         for (const DevBuf* b : {&ctx->photons, &ctx->heads, &ctx->next, &ctx->cell_of, &ctx->cell_count,
                                 &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw,
-                                &ctx->seg_powyz})
+                                &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len})
             key = fnv1a(key, &b->ptr, sizeof(void*));
         const int shape[6] = {ctx->chunk_paths, ctx->wide_bvh, ctx->trace_block, ctx->shade_block,
                               ctx->photon_block, ctx->width};

@@ -213,6 +213,12 @@ DI bool tslab(Guard& g, const Ray& r, float nx, float ny, float nz, float xx, fl
     return slab(r, nx, ny, nz, xx, xy, xz, tmin);
 }
 
+// The root box test; a scene without triangles has no root to enter.
+DI bool enter_root(const DeviceScene& S, Guard& g, const Ray& r, float& tmin) {
+    return S.tri_count > 0 &&
+           tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin);
+}
+
 DI bool thit(Guard& g, const Ray& r, const float4* __restrict__ tri_isect, int i, float& t, float& u, float& v) {
     ++g.tris;
     return hit_triangle(r, tri_isect, i, t, u, v);
@@ -228,7 +234,7 @@ DI Hit trace_closest(const DeviceScene& S, const Ray& r, Guard& g) {
     h.prim = -1;
     h.u = h.v = 0.0f;
     float tmin;
-    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin))
+    if (!enter_root(S, g, r, tmin))
         return h;
     if (tmin > h.t) return h;
     int2 stk[64];
@@ -297,7 +303,7 @@ DI Hit trace_unordered(const DeviceScene& S, const Ray& r, Guard& g) {
     h.prim = -1;
     h.u = h.v = 0.0f;
     float tmin;
-    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin))
+    if (!enter_root(S, g, r, tmin))
         return h;
     if (tmin > h.t) return h;
     int2 stk[64];
@@ -367,7 +373,7 @@ DI Hit trace_unordered(const DeviceScene& S, const Ray& r, Guard& g) {
 template <bool kTestAtParent>
 DI bool trace_shadow(const DeviceScene& S, const Ray& r, float max_dist, Guard& g) {
     float tmin;
-    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin))
+    if (!enter_root(S, g, r, tmin))
         return true;
     if (tmin > max_dist) return true;
     int2 stk[32];
@@ -451,7 +457,7 @@ DI bool traverse_ww(const DeviceScene& S, const Ray& r, float max_t, Guard& g, H
     h.prim = -1;
     h.u = h.v = 0.0f;
     float tmin;
-    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin) ||
+    if (!enter_root(S, g, r, tmin) ||
         tmin > h.t)
         return false;
     int2 stk[64];
@@ -535,7 +541,7 @@ DI bool traverse4(const DeviceScene& S, const Ray& r, float max_t, Guard& g, Hit
     h.prim = -1;
     h.u = h.v = 0.0f;
     float tmin;
-    if (!tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin) ||
+    if (!enter_root(S, g, r, tmin) ||
         tmin > h.t)
         return false;
     int2 stk[kStack4];

@@ -119,6 +119,19 @@ struct RenderArgs {
 // views list the same photons in the same order.
 struct PhotonArgs {
     DeviceScene scene;
+    // First segment split (fast build): a photon's first segment leaves the
+    // light and only matters when its nearest hit is specular (a diffuse
+    // first hit ends it unstored).  `spec` holds the specular triangles,
+    // `diff` the others, each with its own BVH; spec_orig maps a `spec`
+    // triangle to its index in `scene`.  split == 0 traces the full scene.
+    DeviceScene spec;
+    DeviceScene diff;
+    const int* spec_orig;
+    int split;
+    // photons whose first hit is specular, for the second phase of the
+    // split trace (4 float4 each), and their count
+    float4* queue;
+    unsigned int* queue_len;
     float4* photons;        // 3 float4 per photon (std430 record)
     int* heads;
     int* next;

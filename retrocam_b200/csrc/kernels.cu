@@ -108,90 +108,117 @@ DI float fresnel_schlick(float cos_theta, float ior) {
     return r0 + (1.0f - r0) * pow5(gclamp(1.0f - cos_theta, 0.0f, 1.0f));
 }
 
-// photon_trace.comp:168-252: one thread per photon; stored photons are
-// appended with a warp-aggregated 32-bit atomicAdd on the counter and linked
-// into their cell with a 32-bit atomicExch on the cell head.
-template <bool kAtParent>
-__global__ void __launch_bounds__(256) photon_trace_kernel(PhotonArgs A) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const DeviceScene& S = A.scene;
-    Guard g = {0u, 0u, 0u};
-    uint32_t rays = 0, hits = 0;
-    bool store = false;
-    float3 spos = f3(0, 0, 0), spow = f3(0, 0, 0), sdir = f3(0, 0, 0);
-    if (gid < A.photon_count && S.light_count != 0) {
-        uint32_t seed = photon_seed((uint32_t)gid, A.seed);
-        const float u = rnd(seed);
-        int sel = S.light_count - 1;
-        for (int i = 0; i < S.light_count; ++i)
-            if (u < __ldg(S.light_cdf + i)) {
-                sel = i;
-                break;
-            }
-        const float4* L = S.lights + 5 * sel;
-        const float4 l0 = __ldg(L + 0), l1 = __ldg(L + 1), l2 = __ldg(L + 2), l3 = __ldg(L + 3), l4 = __ldg(L + 4);
-        float r1 = rnd(seed);
-        float r2 = rnd(seed);
-        if (r1 + r2 > 1.0f) {
-            r1 = 1.0f - r1;
-            r2 = 1.0f - r2;
-        }
-        const float3 lv0 = xyz(l0);
-        const float3 sp = lv0 + r1 * (xyz(l1) - lv0) + r2 * (xyz(l2) - lv0);
-        const float3 en = normalize(xyz(l4));
-        const float e1 = rnd(seed);
-        const float e2 = rnd(seed);
-        float3 rd = cosine_hemisphere(e1, e2, en);
-        const float3 em = xyz(l3);
-        const float lum = dot(em, f3(0.299f, 0.587f, 0.114f));
-        const float per = S.total_light_power / (float)A.photon_count;
-        float3 power = (lum > 1e-6f) ? (em / lum) * per : f3(per, per, per);
-        Ray ray = make_ray(sp + en * 1e-3f, rd);
-        bool spec = false;
-        for (int b = 0; b < 8; ++b) {
-            ++rays;
-            const Hit hit = photon_hit<kAtParent>(S, ray, g);
-            if (hit.prim < 0) break;
-            ++hits;
-            const Surf sf = surface(S, ray, hit);
-            const Mat m = load_mat(S, sf.mat);
-            rd = ray.d;
-            const float3 n = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
-            if (m.transmission > 0.5f) {
-                const bool entering = dot(rd, sf.normal) < 0.0f;
-                const float eta = entering ? (1.0f / m.ior) : m.ior;
-                const float cosI = fabs_(dot(rd, n));
-                const float F = fresnel_schlick(cosI, m.ior);
-                float3 nd;
-                if (rnd(seed) < F) {
-                    nd = reflect(rd, n);
-                } else {
-                    float3 refr = refract(rd, n, eta);
-                    if (dot(refr, refr) < 0.001f) refr = reflect(rd, n);
-                    nd = normalize(refr);
-                }
-                ray = make_ray(sf.pos + nd * 2e-3f, nd);
-                spec = true;
-                continue;
-            }
-            if (m.metallic > 0.5f) {
-                power = power * m.albedo;
-                const float3 nd = reflect(rd, n);
-                ray = make_ray(sf.pos + n * 2e-3f, nd);
-                spec = true;
-                continue;
-            }
-            if (spec) {
-                store = true;
-                spos = sf.pos;
-                spow = power;
-                sdir = rd;
-            }
+// photon_trace.comp:168-196: the emitted photon -- light picked by the CDF,
+// a uniform point on its triangle, a cosine direction about its normal, an
+// equal share of the total power.
+struct PhotonState {
+    Ray ray;
+    float3 power;
+    uint32_t seed;
+};
+
+DI PhotonState emit_photon(const PhotonArgs& A, const DeviceScene& S, int gid) {
+    PhotonState st;
+    st.seed = photon_seed((uint32_t)gid, A.seed);
+    const float u = rnd(st.seed);
+    int sel = S.light_count - 1;
+    for (int i = 0; i < S.light_count; ++i)
+        if (u < __ldg(S.light_cdf + i)) {
+            sel = i;
             break;
         }
+    const float4* L = S.lights + 5 * sel;
+    const float4 l0 = __ldg(L + 0), l1 = __ldg(L + 1), l2 = __ldg(L + 2), l3 = __ldg(L + 3), l4 = __ldg(L + 4);
+    float r1 = rnd(st.seed);
+    float r2 = rnd(st.seed);
+    if (r1 + r2 > 1.0f) {
+        r1 = 1.0f - r1;
+        r2 = 1.0f - r2;
     }
-    // warp-aggregated counter increment: one atomicAdd per warp
-    const unsigned int mask = __ballot_sync(0xffffffffu, store);
+    const float3 lv0 = xyz(l0);
+    const float3 sp = lv0 + r1 * (xyz(l1) - lv0) + r2 * (xyz(l2) - lv0);
+    const float3 en = normalize(xyz(l4));
+    const float e1 = rnd(st.seed);
+    const float e2 = rnd(st.seed);
+    const float3 rd = cosine_hemisphere(e1, e2, en);
+    const float3 em = xyz(l3);
+    const float lum = dot(em, f3(0.299f, 0.587f, 0.114f));
+    const float per = S.total_light_power / (float)A.photon_count;
+    st.power = (lum > 1e-6f) ? (em / lum) * per : f3(per, per, per);
+    st.ray = make_ray(sp + en * 1e-3f, rd);
+    return st;
+}
+
+struct PhotonStore {
+    bool store;
+    float3 pos, power, dir;
+};
+
+// photon_trace.comp:205-251: up to 8 segments; glass reflects or refracts by
+// Fresnel, metal mirrors, the first diffuse hit after a specular bounce is
+// stored.  With `have_first` the first segment's hit is given (already
+// traced and counted by the caller).
+template <bool kAtParent>
+DI PhotonStore photon_walk(const PhotonArgs& A, const DeviceScene& S, PhotonState st, bool have_first,
+                           const Hit& first, Guard& g, uint32_t& rays) {
+    PhotonStore out;
+    out.store = false;
+    bool spec = false;
+    for (int b = 0; b < 8; ++b) {
+        Hit hit;
+        if (b == 0 && have_first) {
+            hit = first;
+        } else {
+            ++rays;
+            hit = photon_hit<kAtParent>(S, st.ray, g);
+        }
+        if (hit.prim < 0) break;
+        const Surf sf = surface(S, st.ray, hit);
+        const Mat m = load_mat(S, sf.mat);
+        const float3 rd = st.ray.d;
+        const float3 n = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
+        if (m.transmission > 0.5f) {
+            const bool entering = dot(rd, sf.normal) < 0.0f;
+            const float eta = entering ? (1.0f / m.ior) : m.ior;
+            const float cosI = fabs_(dot(rd, n));
+            const float F = fresnel_schlick(cosI, m.ior);
+            float3 nd;
+            if (rnd(st.seed) < F) {
+                nd = reflect(rd, n);
+            } else {
+                float3 refr = refract(rd, n, eta);
+                if (dot(refr, refr) < 0.001f) refr = reflect(rd, n);
+                nd = normalize(refr);
+            }
+            st.ray = make_ray(sf.pos + nd * 2e-3f, nd);
+            spec = true;
+            continue;
+        }
+        if (m.metallic > 0.5f) {
+            st.power = st.power * m.albedo;
+            const float3 nd = reflect(rd, n);
+            st.ray = make_ray(sf.pos + n * 2e-3f, nd);
+            spec = true;
+            continue;
+        }
+        if (spec) {
+            out.store = true;
+            out.pos = sf.pos;
+            out.power = st.power;
+            out.dir = rd;
+        }
+        break;
+    }
+    return out;
+}
+
+// Appends the warp's stored photons: one atomicAdd on the counter per warp;
+// each photon's hash cell is recorded and counted for the cell-sorted
+// layout (the reference links the photon into its cell here with an
+// atomicExchange on the head; the scan/scatter kernels below build that
+// layout and heads/next from it).  Every lane of the warp calls this.
+DI void store_photons(const PhotonArgs& A, const PhotonStore& s, uint32_t rays, Guard& g) {
+    const unsigned int mask = __ballot_sync(0xffffffffu, s.store);
     const int lane = threadIdx.x & 31;
     unsigned int base = 0;
     if (mask != 0u) {
@@ -199,27 +226,129 @@ __global__ void __launch_bounds__(256) photon_trace_kernel(PhotonArgs A) {
         if (lane == leader) base = atomicAdd(A.counter, (unsigned int)__popc(mask));
         base = __shfl_sync(0xffffffffu, base, leader);
     }
-    if (store) {
+    if (s.store) {
         const unsigned int idx = base + __popc(mask & ((1u << lane) - 1u));
         if (idx < (unsigned int)A.photon_count) {
-            const int cx = (int)floorf(spos.x / A.radius);
-            const int cy = (int)floorf(spos.y / A.radius);
-            const int cz = (int)floorf(spos.z / A.radius);
+            const int cx = (int)floorf(s.pos.x / A.radius);
+            const int cy = (int)floorf(s.pos.y / A.radius);
+            const int cz = (int)floorf(s.pos.z / A.radius);
             const int h = cell_hash(cx, cy, cz, A.hash_size);
-            // the reference links the photon into its cell here with an
-            // atomicExchange on the head; the cell-sorted layout is built by
-            // the scan/scatter kernels below, and heads/next from it
             A.cell_of[idx] = h;
             atomicAdd(A.cell_count + h, 1u);
-            A.photons[3 * idx + 0] = make_float4(spos.x, spos.y, spos.z, 0.0f);
-            A.photons[3 * idx + 1] = make_float4(spow.x, spow.y, spow.z, 0.0f);
-            A.photons[3 * idx + 2] = make_float4(sdir.x, sdir.y, sdir.z, 0.0f);
+            A.photons[3 * idx + 0] = make_float4(s.pos.x, s.pos.y, s.pos.z, 0.0f);
+            A.photons[3 * idx + 1] = make_float4(s.power.x, s.power.y, s.power.z, 0.0f);
+            A.photons[3 * idx + 2] = make_float4(s.dir.x, s.dir.y, s.dir.z, 0.0f);
         }
     }
     const unsigned int rsum = __reduce_add_sync(0xffffffffu, rays);
     if (lane == 0 && rsum) atomicAdd(&A.counters->photon_rays, (unsigned long long)rsum);
     flush_work(g, 0u, 0u, A.counters, true);
 }
+
+#if !RC_EXACT
+// First segment against the split scene: the nearest specular triangle,
+// then whether any other triangle lies before it.  True (with the hit in
+// the full scene's numbering) when the photon's first hit is specular.
+DI bool first_specular(const PhotonArgs& A, const Ray& ray, Guard& g, Hit& hit) {
+    Hit hs, hd;
+    traverse_ww<false>(A.spec, ray, 1e30f, g, hs);
+    if (hs.prim < 0 || traverse_ww<true>(A.diff, ray, hs.t, g, hd)) return false;
+    hit = hs;
+    hit.prim = __ldg(A.spec_orig + hs.prim);
+    return true;
+}
+#endif
+
+// photon_trace.comp:168-252: one thread per photon, all its segments.
+template <bool kAtParent>
+__global__ void __launch_bounds__(256) photon_trace_kernel(PhotonArgs A) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const DeviceScene& S = A.scene;
+    Guard g = {0u, 0u, 0u};
+    uint32_t rays = 0;
+    PhotonStore out;
+    out.store = false;
+    if (gid < A.photon_count && S.light_count != 0) {
+        const PhotonState st = emit_photon(A, S, gid);
+        Hit none;
+        none.prim = -1;
+#if !RC_EXACT
+        if (A.split) {
+            ++rays;
+            Hit h;
+            if (first_specular(A, st.ray, g, h)) out = photon_walk<kAtParent>(A, S, st, true, h, g, rays);
+        } else
+#endif
+            out = photon_walk<kAtParent>(A, S, st, false, none, g, rays);
+    }
+    store_photons(A, out, rays, g);
+}
+
+#if !RC_EXACT
+// Two-phase trace (fast build with the split): every photon's emission and
+// first segment, and only the photons whose first hit is specular -- the
+// only ones that can be stored -- go on, compacted into a queue, so the
+// multi-bounce walks run in full warps instead of holding every warp that
+// has one of them.  Queue entry: (origin, seed), (direction, power.x),
+// (power.y, power.z, t, u), (v, triangle).
+__global__ void __launch_bounds__(256) photon_emit_kernel(PhotonArgs A) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const DeviceScene& S = A.scene;
+    Guard g = {0u, 0u, 0u};
+    uint32_t rays = 0;
+    bool want = false;
+    PhotonState st;
+    Hit h;
+    if (gid < A.photon_count && S.light_count != 0) {
+        st = emit_photon(A, S, gid);
+        ++rays;
+        want = first_specular(A, st.ray, g, h);
+    }
+    const unsigned int mask = __ballot_sync(0xffffffffu, want);
+    const int lane = threadIdx.x & 31;
+    if (mask != 0u) {
+        const int leader = __ffs(mask) - 1;
+        unsigned int base = 0;
+        if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (want) {
+            float4* q = A.queue + 4 * (size_t)(base + __popc(mask & ((1u << lane) - 1u)));
+            q[0] = make_float4(st.ray.o.x, st.ray.o.y, st.ray.o.z, __uint_as_float(st.seed));
+            q[1] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, st.power.x);
+            q[2] = make_float4(st.power.y, st.power.z, h.t, h.u);
+            q[3] = make_float4(h.v, __int_as_float(h.prim), 0.0f, 0.0f);
+        }
+    }
+    PhotonStore none;
+    none.store = false;
+    store_photons(A, none, rays, g);
+}
+
+template <bool kAtParent>
+__global__ void __launch_bounds__(256) photon_bounce_kernel(PhotonArgs A) {
+    const unsigned int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned int n = *A.queue_len;
+    Guard g = {0u, 0u, 0u};
+    uint32_t rays = 0;
+    PhotonStore out;
+    out.store = false;
+    if (i < n && i < (unsigned int)A.photon_count) {
+        const float4* q = A.queue + 4 * (size_t)i;
+        const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+        PhotonState st;
+        st.ray = make_ray(xyz(q0), xyz(q1));
+        st.seed = __float_as_uint(q0.w);
+        st.power = f3(q1.w, q2.x, q2.y);
+        Hit h;
+        h.t = q2.z;
+        h.u = q2.w;
+        h.v = q3.x;
+        h.prim = __float_as_int(q3.y);
+        out = photon_walk<kAtParent>(A, A.scene, st, true, h, g, rays);
+    }
+    store_photons(A, out, rays, g);
+}
+#endif
 
 // photon_gather.comp:128-222: pinhole ray to the first diffuse surface,
 // 3x3x3 hash-cell query, Epanechnikov kernel, added into the accumulation.
@@ -546,6 +675,18 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) 
     const int b = block <= 64 ? 64 : (block <= 128 ? 128 : 256);
     const int blocks = (A.photon_count + b - 1) / b;
     if (blocks == 0) return cudaSuccess;
+#if !RC_EXACT
+    if (A.split && A.queue) {
+        cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
+        if (e != cudaSuccess) return e;
+        photon_emit_kernel<<<blocks, b, 0, s>>>(A);
+        if (A.scene.depth <= 60)
+            photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
+        else
+            photon_bounce_kernel<false><<<blocks, b, 0, s>>>(A);
+        return cudaGetLastError();
+    }
+#endif
     if (A.scene.depth <= 60)
         photon_trace_kernel<true><<<blocks, b, 0, s>>>(A);
     else

@@ -526,8 +526,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
                     L.node.ref = S.root_ref;
                     L.node.cnt = S.root_count;
                     float tmin;
-                    L.have_node = tslab(g, L.r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0],
-                                        S.root_max[1], S.root_max[2], tmin) && !(tmin > L.h.t);
+                    L.have_node = enter_root(S, g, L.r, tmin) && !(tmin > L.h.t);
                     steps = 0;
                 }
             }

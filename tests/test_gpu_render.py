@@ -60,12 +60,12 @@ def test_tuning_roundtrip_and_validation(product):
     with product.Context(64, 64, 0, product.RC_MATH_FAST) as ctx:
         t = ctx.tuning()
         assert t == {"engine": product.RC_ENGINE_WAVEFRONT, "chunk_paths": 0, "wide_bvh": 0,
-                     "trace_block": 128, "shade_block": 128, "photon_block": 128}
+                     "trace_block": 128, "shade_block": 128, "photon_block": 128, "photon_full_first": 0}
         ctx.set_tuning(engine=product.RC_ENGINE_WAVEFRONT_STATIC, wide_bvh=3, trace_block=256, shade_block=64)
         t = ctx.tuning()
         assert (t["engine"], t["wide_bvh"], t["trace_block"], t["shade_block"]) == (2, 3, 256, 64)
         for bad in ({"engine": 7}, {"chunk_paths": -1}, {"wide_bvh": 4}, {"trace_block": 96},
-                    {"photon_block": 512}):
+                    {"photon_block": 512}, {"photon_full_first": 2}):
             with pytest.raises(product.RetroCamError) as e:
                 ctx.set_tuning(**bad)
             assert e.value.code == product.RC_ERR_INVALID_ARG
@@ -125,6 +125,51 @@ def test_fast_wide_bvh_photon_map(product, c1):
     assert abs(len(a) - len(b)) <= max(2, len(a) // 1000)
     k = min(len(a), len(b))
     assert np.mean(np.all(bits(a[:k]) == bits(b[:k]), axis=-1)) > 0.99
+
+
+def test_fast_photon_first_segment_split(product, c1):
+    """Tracing a photon's first segment against the specular triangles and
+    then testing the others up to that hit stores the same photons as
+    tracing the whole scene (ties between triangles at one distance aside)."""
+    w, sc, cam = c1
+    maps, rays = [], []
+    for full in (1, 0):
+        with product.Context(64, 64, 0, product.RC_MATH_FAST) as ctx:
+            ctx.set_tuning(photon_full_first=full)
+            ctx.upload(sc)
+            ctx.sppm_reset(0.02)
+            ctx.sppm_trace(300_000, 1 << 18)
+            ph, heads, nxt, n = ctx.read_photon_map(300_000, 1 << 18)
+            maps.append(_photon_records(ph, n))
+            c = ctx.counters()
+            rays.append((c["photon_rays"], c["photon_node_tests"]))
+            assert c["error_word"] == 0
+    a, b = maps
+    assert len(a) > 1000 and abs(len(a) - len(b)) <= max(2, len(a) // 1000)
+    k = min(len(a), len(b))
+    assert np.mean(np.all(bits(a[:k]) == bits(b[:k]), axis=-1)) > 0.99
+    assert rays[0][0] == rays[1][0]          # one traversal per segment either way
+    assert rays[1][1] < 0.5 * rays[0][1]     # far fewer box tests with the split
+
+
+def test_empty_scene_renders_black(product):
+    """A scene without triangles: every ray misses, no guard is raised."""
+    from retrocam_b200 import scenes
+    w = scenes.cornell_small()
+    sc = product.build_scene(w.scene)
+    sc = dict(sc)
+    sc["tris"] = sc["tris"][:0]
+    sc["nodes"] = sc["nodes"][:1].copy()
+    sc["nodes"]["prim_count"] = 0
+    sc["nodes"]["left_child"] = 0
+    sc["nodes"]["right_child"] = 0
+    sc["light_count"] = 0
+    with product.Context(32, 32, 0, product.RC_MATH_FAST) as ctx:
+        ctx.upload(sc)
+        ctx.render(product.workload_camera(w), (1, 1.0), 0, 2)
+        acc = ctx.read_buffers()[0]
+        assert ctx.counters()["error_word"] == 0
+    assert not acc[..., :3].any() and (acc[..., 3] == 2).all()
 
 
 @pytest.fixture(scope="module")
