@@ -109,6 +109,13 @@ struct rc_ctx {
     DevBuf batch_img, batch_segs;   // per-frame images and chunk segments of a batch
     // photon first-segment split: specular / other triangles with own BVHs
     DevBuf sp_nodes, sp_isect, sp_orig, df_nodes, df_isect, ph_queue, ph_queue_len;
+    // gather hits per pixel (see GatherArgs::hit_cache)
+    DevBuf gcache, batch_gcache;
+    uint64_t gcache_key = 0;
+    bool gcache_valid = false;
+    unsigned int scene_gen = 0;
+    float4* gcache_force = nullptr;   // a batch frame's slice, and its mode
+    int gcache_force_mode = 0;
     DeviceScene spec_view, diff_view;
     bool photon_split = false;
     // learned denoiser scratch
@@ -292,7 +299,7 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
                       &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs, &ctx->sp_nodes,
                       &ctx->sp_isect, &ctx->sp_orig, &ctx->df_nodes, &ctx->df_isect, &ctx->ph_queue,
-                      &ctx->ph_queue_len})
+                      &ctx->ph_queue_len, &ctx->gcache, &ctx->batch_gcache})
         release(*b);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -650,6 +657,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
             ctx->photon_split = true;
         }
     }
+    ctx->scene_gen++;
     ctx->has_scene = true;
     return RC_OK;
 }
@@ -994,6 +1002,8 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     return launch_err(ctx, e, "photon trace");
 }
 
+static uint64_t fnv1a(uint64_t h, const void* p, size_t n);
+
 int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, float weight) {
     if (!ctx) return RC_ERR_INVALID_ARG;
     int r = check_sppm(ctx, p);
@@ -1014,6 +1024,21 @@ int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, f
     A.radius = ctx->sppm_radius;
     A.weight = weight;
     A.counters = ctx->counters;
+    // per-pixel gather hits: reused while the camera, scene, math mode and
+    // traversal stay the same (a batch passes each frame's own slice)
+    if (ctx->gcache_force) {
+        A.hit_cache = ctx->gcache_force;
+        A.cache_mode = ctx->gcache_force_mode;
+    } else {
+        uint64_t key = fnv1a(1469598103934665603ull, &A.cam, sizeof(A.cam));
+        const int salt[4] = {(int)ctx->scene_gen, ctx->math_mode, ctx->wide_bvh, ctx->width * 65536 + ctx->height};
+        key = fnv1a(key, salt, sizeof(salt));
+        CK(ensure(ctx->gcache, (size_t)ctx->width * ctx->height * sizeof(float4)));
+        A.hit_cache = (float4*)ctx->gcache.ptr;
+        A.cache_mode = (ctx->gcache_valid && ctx->gcache_key == key) ? 2 : 1;
+        ctx->gcache_key = key;
+        ctx->gcache_valid = true;
+    }
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
     const cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_GATHER, [&] {
         return ex ? exact::launch_photon_gather(A, ctx->stream) : fast::launch_photon_gather(A, ctx->stream);
@@ -1356,7 +1381,10 @@ static int batched_sequence(rc_ctx* ctx, const rc_frame_desc* frames, int n, con
                 int s0, s1;
                 slice_range(frames[f], k, s0, s1);
                 ctx->img = frame_images(ctx, f);
+                ctx->gcache_force = (float4*)ctx->batch_gcache.ptr + (size_t)f * px;
+                ctx->gcache_force_mode = k == 0 ? 1 : 2;
                 r = rc_sppm_gather(ctx, &frames[f].camera, sppm, (float)(s1 - s0));
+                ctx->gcache_force = nullptr;
             }
             if (r == RC_OK) r = rc_sppm_update_radius(ctx, sppm->alpha);
         }
@@ -1413,6 +1441,7 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
     if (batched) {
         // per-frame images: accum | gbuf | galb | var regions of n_frames x px
         CK(ensure(ctx->batch_img, (size_t)n_frames * px * 36));
+        if (any_sppm) CK(ensure(ctx->batch_gcache, (size_t)n_frames * px * sizeof(float4)));
         plan = plan_batch(ctx, frames, n_frames);
         cap = std::max(cap, plan.capacity);
         CK(ensure(ctx->batch_segs, plan.segs.size() * sizeof(FrameSeg)));
@@ -1432,7 +1461,9 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
     CK(ensure(ctx->frames, (size_t)n_frames * px * sizeof(float4)));
     CK(cudaStreamSynchronize(ctx->stream));
     // ---- the sequence ----
+    if (any_sppm) CK(ensure(ctx->gcache, px * sizeof(float4)));
     auto sequence = [&]() -> int {
+        ctx->gcache_valid = false;   // each replay traces its frames' gather hits afresh
         if (batched)
             return batched_sequence(ctx, frames, n_frames, settings, sppm, sppm_initial_radius, atrous, plan);
         for (int f = 0; f < n_frames; ++f) {
@@ -1465,7 +1496,8 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
         key = fnv1a(key, &ctx->wf_o.ptr, sizeof(void*));
         for (const DevBuf* b : {&ctx->photons, &ctx->heads, &ctx->next, &ctx->cell_of, &ctx->cell_count,
                                 &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw,
-                                &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len})
+                                &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len, &ctx->gcache,
+                                &ctx->batch_gcache})
             key = fnv1a(key, &b->ptr, sizeof(void*));
         const int shape[6] = {ctx->chunk_paths, ctx->wide_bvh, ctx->trace_block, ctx->shade_block,
                               ctx->photon_block, ctx->width};

@@ -161,6 +161,12 @@ struct GatherArgs {
     float radius;
     float weight;
     DevCounters* counters;
+    // The gather ray of a pixel (pixel centre, no lens) and its specular walk
+    // are the same in every SPPM iteration of one camera: cache_mode 1 traces
+    // them and stores the first diffuse hit (position, material; -1 = none)
+    // per pixel in hit_cache, 2 reads it back, 0 traces without the cache.
+    float4* hit_cache;
+    int cache_mode;
 };
 
 struct AtrousArgs {

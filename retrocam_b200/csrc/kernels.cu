@@ -374,7 +374,14 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
         bool found = false;
         float3 hp = f3(0, 0, 0);
         int hm = 0;
-        for (int s = 0; s <= 6; ++s) {
+        const long pix = (long)py * W + px;
+        if (A.cache_mode == 2) {
+            const float4 c = A.hit_cache[pix];
+            hm = __float_as_int(c.w);
+            found = hm >= 0;
+            hp = xyz(c);
+        }
+        for (int s = 0; s <= 6 && A.cache_mode != 2; ++s) {
             ++rays;
             const Hit hit = photon_hit<kAtParent>(S, ray, g);
             if (hit.prim < 0) break;
@@ -401,6 +408,7 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
             }
             ray = make_ray(sf.pos + nd * 2e-3f, nd);
         }
+        if (A.cache_mode == 1) A.hit_cache[pix] = make_float4(hp.x, hp.y, hp.z, __int_as_float(found ? hm : -1));
         if (found) {
             const float r = A.radius, r2 = r * r;
             const int ccx = (int)floorf(hp.x / r), ccy = (int)floorf(hp.y / r), ccz = (int)floorf(hp.z / r);

@@ -352,6 +352,39 @@ def test_gather_matches_oracle(product, orc, c1):
     np.testing.assert_array_equal(after[..., 3], before[..., 3])
 
 
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+def test_gather_hits_reused_across_iterations(product, c1, mode):
+    """The pixel-centre gather rays and their specular walks are traced once
+    per camera: a second gather with the same camera and photon map adds the
+    same amounts (bit for bit) without tracing, and a new camera traces
+    again."""
+    w, sc, cam = c1
+    W, H, N, hs = 96, 64, 100_000, 1 << 18
+    m = product.RC_MATH_EXACT if mode == "exact" else product.RC_MATH_FAST
+    with product.Context(W, H, 0, m) as ctx:
+        ctx.upload(sc)
+        ctx.sppm_reset(0.02)
+        ctx.sppm_trace(N, hs)
+        ctx.reset_counters()
+        a0 = ctx.read_buffers()[0]
+        ctx.sppm_gather(cam, N, hs)
+        a1 = ctx.read_buffers()[0]
+        traced = ctx.counters()["gather_rays"]
+        ctx.reset_counters()
+        ctx.sppm_gather(cam, N, hs)
+        a2 = ctx.read_buffers()[0]
+        assert ctx.counters()["gather_rays"] == 0 and traced >= W * H
+        cam2 = dict(cam)
+        cam2["cam_pos"] = np.asarray(cam["cam_pos"], np.float32) + np.float32(0.01)
+        ctx.reset_counters()
+        ctx.sppm_gather(cam2, N, hs)
+        assert ctx.counters()["gather_rays"] >= W * H
+    d1, d2 = a1 - a0, a2 - a1
+    assert np.abs(d1).max() > 0
+    # the same per-pixel amounts, added onto a different running sum
+    np.testing.assert_allclose(d2, d1, rtol=1e-5, atol=1e-7)
+
+
 def test_gather_with_capped_chains(product, orc, c1):
     """Chains longer than 512 are cut by the reference's `safety < 512` walk
     cap (photon_gather.comp:193), so which photons count depends on insertion
