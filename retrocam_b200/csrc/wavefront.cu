@@ -535,12 +535,21 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
         // ---- advance the rays ----
         while (true) {
             bool busy = L.item >= 0;
+            // A lane is blocked when it has a leaf parked and cannot step
+            // on (no node left, or its next node is a leaf too).  Leaves are
+            // tested warp-wide -- every lane with one parked tests it in the
+            // same iteration -- once all busy lanes have one parked or half
+            // of them are blocked; otherwise the unblocked lanes take an
+            // interior step and the blocked ones wait.  Leaf tests and
+            // interior steps never share an iteration.
+            const bool blocked = busy && L.leaf.cnt > 0 && (!L.have_node || L.node.cnt > 0);
             const unsigned int act = __ballot_sync(FULL, busy);
             const unsigned int parked = __ballot_sync(FULL, busy && L.leaf.cnt > 0);
-            if (busy) {
+            const unsigned int blk = __ballot_sync(FULL, blocked);
+            const bool leaf_phase = parked == act || 2 * __popc(blk) >= __popc(act);
+            if (busy && (leaf_phase ? L.leaf.cnt > 0 : !blocked)) {
                 bool done = false;
-                const bool do_leaf = L.leaf.cnt > 0 && (parked == act || !L.have_node || L.node.cnt > 0);
-                if (do_leaf) {
+                if (leaf_phase) {
                     for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
                         float t, u, v;
                         if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
