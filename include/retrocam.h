@@ -198,6 +198,11 @@ typedef struct rc_tuning {
                                   specular triangles, then tests the others up to that hit
                                   (a diffuse first hit ends the photon unstored, so only
                                   the specular hit matters); 1 traces the whole scene */
+    int32_t refill_lanes;  /* RC_ENGINE_WAVEFRONT trace: a warp fetches new rays when fewer
+                              than this many lanes are busy, 1..32 (0 = 16) */
+    int32_t leaf_quarters; /* RC_ENGINE_WAVEFRONT trace: a warp tests its parked leaves
+                              once this many quarters of its busy lanes cannot step on
+                              (or all have a leaf parked), 1..4 (0 = 2) */
 } rc_tuning;
 
 /* error_word bits. */

@@ -37,6 +37,8 @@ KNOBS: dict[str, tuple[int, ...]] = {
     "shade_block": (64, 128, 256),
     "photon_block": (64, 128, 256),
     "photon_full_first": (0, 1),
+    "refill_lanes": (12, 16, 20, 24, 28),
+    "leaf_quarters": (1, 2, 3, 4),
 }
 
 

@@ -101,6 +101,7 @@ struct rc_ctx {
     int wide_bvh = 0;
     int trace_block = 128, shade_block = 128, photon_block = 128;
     int photon_full_first = 0;
+    int refill_lanes = 16, leaf_quarters = 2;
     DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
         wf_qlen;
     int wf_capacity = 0;
@@ -686,10 +687,12 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
          t->engine != RC_ENGINE_WAVEFRONT_STATIC) ||
         t->chunk_paths < 0 || (t->wide_bvh & ~(RC_WIDE_PATHS | RC_WIDE_PHOTONS)) || !valid_block(t->trace_block) ||
         !valid_block(t->shade_block) || !valid_block(t->photon_block) ||
-        (t->photon_full_first != 0 && t->photon_full_first != 1))
-        return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d first %d",
-                    t->engine, t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block,
-                    t->photon_full_first);
+        (t->photon_full_first != 0 && t->photon_full_first != 1) || t->refill_lanes < 0 || t->refill_lanes > 32 ||
+        t->leaf_quarters < 0 || t->leaf_quarters > 4)
+        return fail(ctx, RC_ERR_INVALID_ARG,
+                    "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d first %d refill %d leaf %d", t->engine,
+                    t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block,
+                    t->photon_full_first, t->refill_lanes, t->leaf_quarters);
     ctx->engine = t->engine;
     ctx->chunk_paths = t->chunk_paths;
     ctx->wide_bvh = t->wide_bvh;
@@ -697,6 +700,8 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
     ctx->shade_block = t->shade_block ? t->shade_block : 128;
     ctx->photon_block = t->photon_block ? t->photon_block : 128;
     ctx->photon_full_first = t->photon_full_first;
+    ctx->refill_lanes = t->refill_lanes ? t->refill_lanes : 16;
+    ctx->leaf_quarters = t->leaf_quarters ? t->leaf_quarters : 2;
     return RC_OK;
 }
 
@@ -710,6 +715,8 @@ int rc_get_tuning(rc_ctx* ctx, rc_tuning* out) {
     out->shade_block = ctx->shade_block;
     out->photon_block = ctx->photon_block;
     out->photon_full_first = ctx->photon_full_first;
+    out->refill_lanes = ctx->refill_lanes;
+    out->leaf_quarters = ctx->leaf_quarters;
     return RC_OK;
 }
 
@@ -794,6 +801,8 @@ static WaveArgs wave_args(rc_ctx* ctx, const DeviceScene& scene, int nee_enabled
     A.npix = tiles_x * tiles_y * 32;
     A.counters = ctx->counters;
     A.dynamic_fetch = ctx->engine == RC_ENGINE_WAVEFRONT ? 1 : 0;
+    A.refill_lanes = ctx->refill_lanes;
+    A.leaf_quarters = ctx->leaf_quarters;
     A.bounce = 0;
     return A;
 }
@@ -1499,8 +1508,9 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
                                 &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len, &ctx->gcache,
                                 &ctx->batch_gcache})
             key = fnv1a(key, &b->ptr, sizeof(void*));
-        const int shape[6] = {ctx->chunk_paths, ctx->wide_bvh, ctx->trace_block, ctx->shade_block,
-                              ctx->photon_block, ctx->width};
+        const int shape[9] = {ctx->chunk_paths,  ctx->wide_bvh,       ctx->trace_block,
+                              ctx->shade_block,  ctx->photon_block,   ctx->width,
+                              ctx->photon_full_first, ctx->refill_lanes, ctx->leaf_quarters};
         key = fnv1a(key, shape, sizeof(shape));
         if (!ctx->graph_exec || ctx->graph_key != key) {
             if (ctx->graph_exec) {

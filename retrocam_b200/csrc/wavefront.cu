@@ -450,12 +450,10 @@ static int grid_for(const void* fn, int block) {
 // Persistent trace with dynamic ray fetch (fast build).  Each lane owns one
 // ray at a time and advances it one traversal step per loop iteration: an
 // interior node, parking a reached leaf, or the triangles of a parked leaf
-// (taken together once every busy lane of the warp has parked one).  When
-// fewer than kRefill lanes are still busy, the idle lanes take the next rays
-// from the work counter (one atomicAdd per warp), so a warp is not held by
-// its slowest ray.  Same rays and results as wf_trace; only the schedule
-// differs.
-constexpr int kRefill = 20;
+// (see the leaf phase below).  When fewer than A.refill_lanes lanes are
+// still busy, the idle lanes take the next rays from the work counter (one
+// atomicAdd per warp), so a warp is not held by its slowest ray.  Same rays
+// and results as wf_trace; only the schedule differs.
 
 struct LaneRay {
     Ray r;
@@ -546,7 +544,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
             const unsigned int act = __ballot_sync(FULL, busy);
             const unsigned int parked = __ballot_sync(FULL, busy && L.leaf.cnt > 0);
             const unsigned int blk = __ballot_sync(FULL, blocked);
-            const bool leaf_phase = parked == act || 2 * __popc(blk) >= __popc(act);
+            const bool leaf_phase = parked == act || 4 * __popc(blk) >= A.leaf_quarters * __popc(act);
             if (busy && (leaf_phase ? L.leaf.cnt > 0 : !blocked)) {
                 bool done = false;
                 if (leaf_phase) {
@@ -619,7 +617,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
                 }
             }
             const unsigned int still = __ballot_sync(FULL, busy);
-            if (__popc(still) < kRefill) break;
+            if (__popc(still) < A.refill_lanes) break;
         }
     }
     const unsigned int c = __reduce_add_sync(FULL, closest);

@@ -60,12 +60,14 @@ def test_tuning_roundtrip_and_validation(product):
     with product.Context(64, 64, 0, product.RC_MATH_FAST) as ctx:
         t = ctx.tuning()
         assert t == {"engine": product.RC_ENGINE_WAVEFRONT, "chunk_paths": 0, "wide_bvh": 0,
-                     "trace_block": 128, "shade_block": 128, "photon_block": 128, "photon_full_first": 0}
+                     "trace_block": 128, "shade_block": 128, "photon_block": 128, "photon_full_first": 0,
+                     "refill_lanes": 16, "leaf_quarters": 2}
         ctx.set_tuning(engine=product.RC_ENGINE_WAVEFRONT_STATIC, wide_bvh=3, trace_block=256, shade_block=64)
         t = ctx.tuning()
         assert (t["engine"], t["wide_bvh"], t["trace_block"], t["shade_block"]) == (2, 3, 256, 64)
         for bad in ({"engine": 7}, {"chunk_paths": -1}, {"wide_bvh": 4}, {"trace_block": 96},
-                    {"photon_block": 512}, {"photon_full_first": 2}):
+                    {"photon_block": 512}, {"photon_full_first": 2},
+                    {"refill_lanes": 33}, {"leaf_quarters": 5}):
             with pytest.raises(product.RetroCamError) as e:
                 ctx.set_tuning(**bad)
             assert e.value.code == product.RC_ERR_INVALID_ARG
