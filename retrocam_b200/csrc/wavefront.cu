@@ -156,7 +156,10 @@ __global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
 
 // One bounce of pathtrace.comp's traceRadiance for every path in ray queue
 // rq[bounce&1] whose closest hit wf_trace has stored.
-__global__ void __launch_bounds__(256) wf_shade(WaveArgs A) {
+// Registers capped for 3 blocks of 256 threads per SM (85): the kernel
+// streams path state and waits on memory, so resident warps matter more
+// than the registers the compiler would otherwise use (105).
+__global__ void __launch_bounds__(256, 3) wf_shade(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
     const int cur = A.bounce & 1;
