@@ -531,7 +531,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     std::vector<int> todo;
     todo.push_back(0);
     seen[0] = 1;
-    int max_depth = 0;
+    int max_depth = 0, max_leaf = 0;
     while (!todo.empty()) {
         const int i = todo.back();
         todo.pop_back();
@@ -541,6 +541,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
                 return fail(ctx, RC_ERR_BAD_SCENE, "node %d: primitives [%d,+%d) outside %d triangles", i,
                             n.prim_start, n.prim_count, tri_count);
             if (depth[i] > max_depth) max_depth = depth[i];
+            if (n.prim_count > max_leaf) max_leaf = n.prim_count;
             continue;
         }
         if (tri_count == 0 && i == 0) break;
@@ -629,6 +630,7 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     S.root_ref = nodes[0].prim_count > 0 ? nodes[0].prim_start : 0;
     S.root_count = nodes[0].prim_count;
     S.depth = max_depth;
+    S.max_leaf = max_leaf;
     // ---- first-segment split of the photon trace (fast build): BVHs over
     //      the specular (metal or glass) triangles and over the others ----
     ctx->photon_split = false;

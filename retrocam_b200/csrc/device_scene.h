@@ -64,6 +64,7 @@ struct DeviceScene {
     int root_ref = 0;     // prim_start when the root is a leaf, else 0
     int root_count = 0;   // > 0 when the root is a leaf
     int depth = 0;        // max leaf depth (root = 0)
+    int max_leaf = 0;     // most triangles in one leaf
 };
 
 // Per-context images (core/Renderer.java:152-193).

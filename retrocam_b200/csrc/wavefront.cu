@@ -458,6 +458,18 @@ static int grid_for(const void* fn, int block) {
 // atomicAdd per warp), so a warp is not held by its slowest ray.  Same rays
 // and results as wf_trace; only the schedule differs.
 
+// Pops the next stack entry not culled by the current hit distance.
+DI bool pop_packed(const int2* stk, int& top, float cull, TravNode& n) {
+    while (top > 0) {
+        const int2 e = stk[--top];
+        if (__int_as_float(e.y & (int)0xffff0000) > cull) continue;
+        n.ref = e.x;
+        n.cnt = e.y & 0xffff;
+        return true;
+    }
+    return false;
+}
+
 struct LaneRay {
     Ray r;
     Hit h;
@@ -484,8 +496,10 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
     const int lane = threadIdx.x & 31;
     Guard g = {0u, 0u, 0u};
     uint32_t closest = 0, shadow = 0;
+    // traversal stack, 8 bytes an entry: (ref, count | entry distance
+    // truncated to its top 16 bits); truncation rounds a positive distance
+    // down, so the pop-time cull `t > hit` never drops a needed entry
     int2 stk[64];
-    float stt[64];
     LaneRay L;
     L.item = -1;
     L.top = 0;
@@ -568,7 +582,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
                 } else if (L.have_node) {
                     if (L.node.cnt > 0) {
                         L.leaf = L.node;
-                        L.have_node = pop_entry(stk, stt, L.top, L.h.t, L.node);
+                        L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
                     } else {
                         const NodeRec* nrec = S.nodes + L.node.ref;
                         const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
@@ -579,8 +593,10 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
                         if (hl && hr) {
                             const bool left_first = tl < tr;
                             if (L.top < 62) {
-                                stk[L.top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
-                                stt[L.top++] = left_first ? tr : tl;
+                                const float tf = left_first ? tr : tl;
+                                const int cf = left_first ? d.w : d.y;
+                                stk[L.top++] = make_int2(left_first ? d.z : d.x,
+                                                         (cf & 0xffff) | (__float_as_int(tf) & (int)0xffff0000));
                             }
                             L.node.ref = left_first ? d.x : d.z;
                             L.node.cnt = left_first ? d.y : d.w;
@@ -591,7 +607,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
                             L.node.ref = d.z;
                             L.node.cnt = d.w;
                         } else {
-                            L.have_node = pop_entry(stk, stt, L.top, L.h.t, L.node);
+                            L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
                         }
                     }
                 }
@@ -675,7 +691,8 @@ cudaError_t launch_wf_generate(const WaveArgs& A, cudaStream_t s) {
 cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
     const int c = block_class(block), b = 64 << c;
 #if !RC_EXACT
-    if (A.dynamic_fetch) {
+    // the refill trace packs leaf counts into 16 bits of a stack entry
+    if (A.dynamic_fetch && A.scene.max_leaf < 0x10000) {
         wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
         return cudaGetLastError();
     }
