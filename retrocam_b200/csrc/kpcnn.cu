@@ -72,109 +72,198 @@ struct ConvArgs {
     unsigned int* err;
 };
 
+// Shared memory of the persistent convolution: three row buffers (the tile
+// being multiplied, the tile whose rows are in flight, and the one the
+// previous MMAs just released), the weights, and one mbarrier per TMEM
+// accumulator.
+constexpr int kRowBufs = 3;
+
 template <int CIN>
 struct ConvSmem {
-    alignas(128) uint4 rows[3 * (CIN / 8) * kPStride];
+    alignas(128) uint4 rows[kRowBufs][3 * (CIN / 8) * kPStride];
     alignas(128) uint4 wts[9 * (CIN / 8) * kCo];
-    uint64_t mbar;
+    uint64_t mbar[2];
     uint32_t tmem;
 };
 
+// 16-byte asynchronous global -> shared copy; src_bytes 0 writes zeros.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Rows y-1..y+1, pixels x0-1 .. x0+128 of tile t into `rows` (zeros outside
+// the image), as asynchronous copies; the caller commits the group.
 template <int CIN>
-__global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
+__device__ __forceinline__ void stage_rows(const ConvArgs& A, uint4* rows, int t, int tiles_x) {
     constexpr int G = CIN / 8;
-    __shared__ ConvSmem<CIN> S;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int x0 = blockIdx.x * kTile, y = blockIdx.y, n = blockIdx.z;
-    if (warp == 0) tc::tmem_alloc(&S.tmem, 32);
-    if (tid == 0) tc::mbar_init(&S.mbar, 1);
-    // stage rows y-1..y+1, pixels x0-1 .. x0+128 (zero outside the image)
-    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
-    for (int i = tid; i < 3 * kHalo * G; i += 128) {
+    const int xt = t % tiles_x, rest = t / tiles_x;
+    const int y = rest % A.h, n = rest / A.h;
+    const int x0 = xt * kTile;
+    const uint32_t base = tc::smem_u32(rows);
+    for (int i = threadIdx.x; i < 3 * kHalo * G; i += 128) {
         const int r = i / (kHalo * G), rem = i - r * kHalo * G;
         const int p = rem / G, g = rem - p * G;
         const int yy = y + r - 1, xx = x0 + p - 1;
-        uint4 v = zero;
-        if (yy >= 0 && yy < A.h && xx >= 0 && xx < A.w)
-            v = __ldg(reinterpret_cast<const uint4*>(A.in + (((size_t)n * A.h + yy) * A.w + xx) * CIN) + g);
-        S.rows[(r * G + g) * kPStride + p] = v;
+        const bool in = yy >= 0 && yy < A.h && xx >= 0 && xx < A.w;
+        const uint4* src = in ? reinterpret_cast<const uint4*>(A.in + (((size_t)n * A.h + yy) * A.w + xx) * CIN) + g
+                              : reinterpret_cast<const uint4*>(A.in);
+        cp_async16(base + ((r * G + g) * kPStride + p) * 16, src, in ? 16u : 0u);
+    }
+}
+
+template <int CIN>
+__device__ __forceinline__ void issue_tile(uint32_t rows, uint32_t wts, uint32_t tmem_d, uint64_t* mbar) {
+    constexpr int G = CIN / 8;
+    constexpr uint32_t idesc = tc::idesc_bf16(128, kCo, false, false);
+#pragma unroll 1
+    for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap - 3 * dy;
+#pragma unroll
+        for (int ks = 0; ks < CIN / 16; ++ks) {
+            const uint64_t a = tc::smem_desc(rows + ((dy * G + 2 * ks) * kPStride + dx) * 16, kPStride * 16, 128);
+            const uint64_t b = tc::smem_desc(wts + (tap * G + 2 * ks) * kCo * 16, kCo * 16, 128);
+            tc::mma_bf16(tmem_d, a, b, idesc, (tap | ks) != 0);
+        }
+    }
+    tc::mma_commit(mbar);
+}
+
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&vin)[32], int t, int tiles_x) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int xt = t % tiles_x, rest = t / tiles_x;
+    const int y = rest % A.h, n = rest / A.h;
+    const int x = xt * kTile + warp * 32 + lane;
+    if (x >= A.w) return;
+    float v[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) v[c] = vin[c];
+    const size_t pix = ((size_t)n * A.h + y) * A.w + x;
+    if (A.bias) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] += __ldg(A.bias + c);
+    }
+    if (A.relu) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] = fmaxf(v[c], 0.0f);
+    }
+    if (A.mask) {
+        const uint4* m = reinterpret_cast<const uint4*>(A.mask + pix * 32);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint4 mv = __ldg(m + q);
+            const uint32_t w4[4] = {mv.x, mv.y, mv.z, mv.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&w4[j]);
+                if (!(__bfloat162float(h2.x) > 0.0f)) v[q * 8 + 2 * j] = 0.0f;
+                if (!(__bfloat162float(h2.y) > 0.0f)) v[q * 8 + 2 * j + 1] = 0.0f;
+            }
+        }
+    }
+    if (A.out_f32) {
+        float4* o = reinterpret_cast<float4*>(static_cast<float*>(A.out) + pix * 32);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else {
+        uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(A.out) + pix * 32);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t w4[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
+                w4[j] = *reinterpret_cast<const uint32_t*>(&h2);
+            }
+            o[q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        }
+    }
+}
+
+// Persistent implicit-GEMM convolution: each CTA keeps the weights in shared
+// memory and walks tiles t_k = blockIdx.x + k * gridDim.x.  Step k copies
+// the rows of t_{k+1} asynchronously into a free buffer, issues the MMAs of
+// t_k (rows landed in step k-1) into one TMEM accumulator, and meanwhile runs
+// the epilogue of t_{k-1} from the other, so row copies, tensor-core work and
+// epilogues of three consecutive tiles overlap.
+template <int CIN>
+__global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
+    extern __shared__ __align__(128) unsigned char conv_smem_raw[];
+    ConvSmem<CIN>& S = *reinterpret_cast<ConvSmem<CIN>*>(conv_smem_raw);
+    constexpr int G = CIN / 8;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int tiles_x = (A.w + kTile - 1) / kTile;
+    const int ntiles = tiles_x * A.h * A.n;
+    const int stride = gridDim.x;
+    if (warp == 0) tc::tmem_alloc(&S.tmem, 64);
+    if (tid == 0) {
+        tc::mbar_init(&S.mbar[0], 1);
+        tc::mbar_init(&S.mbar[1], 1);
     }
     for (int i = tid; i < 9 * G * kCo; i += 128) S.wts[i] = __ldg(reinterpret_cast<const uint4*>(A.wpk) + i);
-    tc::fence_async_smem();
+    const int t0 = blockIdx.x;
+    if (t0 < ntiles) stage_rows<CIN>(A, S.rows[0], t0, tiles_x);
+    cp_async_commit();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = S.tmem;
-    if (tid == 0) {
-        constexpr uint32_t idesc = tc::idesc_bf16(128, kCo, false, false);
-        const uint32_t rows = tc::smem_u32(S.rows), wts = tc::smem_u32(S.wts);
-#pragma unroll 1
-        for (int tap = 0; tap < 9; ++tap) {
-            const int dy = tap / 3, dx = tap - 3 * dy;
-#pragma unroll
-            for (int ks = 0; ks < CIN / 16; ++ks) {
-                const uint64_t a =
-                    tc::smem_desc(rows + ((dy * G + 2 * ks) * kPStride + dx) * 16, kPStride * 16, 128);
-                const uint64_t b = tc::smem_desc(wts + (tap * G + 2 * ks) * kCo * 16, kCo * 16, 128);
-                tc::mma_bf16(tmem, a, b, idesc, (tap | ks) != 0);
+    const uint32_t wts = tc::smem_u32(S.wts);
+    uint32_t phase[2] = {0u, 0u};
+    bool ok = true;
+    int k = 0;
+    for (int t = t0; t < ntiles && ok; t += stride, ++k) {
+        const int acc = k & 1;
+        // rows of t_{k+1}: its buffer was last read by the MMAs of t_{k-2},
+        // whose completion the epilogue of step k-1 waited for
+        const int tn = t + stride;
+        if (tn < ntiles) stage_rows<CIN>(A, S.rows[(k + 1) % kRowBufs], tn, tiles_x);
+        cp_async_commit();
+        // rows of t_k landed (all but the group just committed)
+        cp_async_wait<1>();
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (tid == 0) issue_tile<CIN>(tc::smem_u32(S.rows[k % kRowBufs]), wts, tmem + acc * 32, &S.mbar[acc]);
+        if (k > 0) {
+            // epilogue of t_{k-1} while the tensor cores work on t_k
+            const int pa = acc ^ 1;
+            ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
+            phase[pa] ^= 1u;
+            tc::fence_after_sync();
+            if (ok) {
+                float v[32];
+                tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
+                conv_epilogue(A, v, t - stride, tiles_x);
             }
+            tc::fence_before_sync();
         }
-        tc::mma_commit(&S.mbar);
     }
-    const bool ok = __syncthreads_and(tc::mbar_wait(&S.mbar, 0, kWaitTries));
-    tc::fence_after_sync();
+    // epilogue of the last tile
+    if (ok && k > 0) {
+        const int pa = (k - 1) & 1;
+        ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
+        tc::fence_after_sync();
+        if (ok) {
+            float v[32];
+            tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
+            conv_epilogue(A, v, t0 + (k - 1) * stride, tiles_x);
+        }
+    }
+    cp_async_wait<0>();
     if (!ok) {
         if (tid == 0) atomicOr(A.err, RC_GUARD_MMA_WAIT);
-    } else {
-        float v[32];
-        tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16), v);
-        const int x = x0 + warp * 32 + lane;
-        if (x < A.w) {
-            const size_t pix = ((size_t)n * A.h + y) * A.w + x;
-            if (A.bias) {
-#pragma unroll
-                for (int c = 0; c < 32; ++c) v[c] += __ldg(A.bias + c);
-            }
-            if (A.relu) {
-#pragma unroll
-                for (int c = 0; c < 32; ++c) v[c] = fmaxf(v[c], 0.0f);
-            }
-            if (A.mask) {
-                const uint4* m = reinterpret_cast<const uint4*>(A.mask + pix * 32);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint4 mv = __ldg(m + q);
-                    const uint32_t w4[4] = {mv.x, mv.y, mv.z, mv.w};
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const __nv_bfloat162 h2 = *reinterpret_cast<const __nv_bfloat162*>(&w4[j]);
-                        if (!(__bfloat162float(h2.x) > 0.0f)) v[q * 8 + 2 * j] = 0.0f;
-                        if (!(__bfloat162float(h2.y) > 0.0f)) v[q * 8 + 2 * j + 1] = 0.0f;
-                    }
-                }
-            }
-            if (A.out_f32) {
-                float4* o = reinterpret_cast<float4*>(static_cast<float*>(A.out) + pix * 32);
-#pragma unroll
-                for (int q = 0; q < 8; ++q) o[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-            } else {
-                uint4* o = reinterpret_cast<uint4*>(static_cast<__nv_bfloat16*>(A.out) + pix * 32);
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    uint32_t w4[4];
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const __nv_bfloat162 h2 = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
-                        w4[j] = *reinterpret_cast<const uint32_t*>(&h2);
-                    }
-                    o[q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
-                }
-            }
-        }
+        // give MMAs still in flight a bounded time before the columns go
+        for (int a = 0; a < 2; ++a) (void)tc::mbar_wait(&S.mbar[a], phase[a], kWaitTries);
     }
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, 32);
+    if (warp == 0) tc::tmem_dealloc(tmem, 64);
 }
 
 // ---------------------------------------------------------------------------
@@ -498,13 +587,41 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-cudaError_t launch_conv(const ConvArgs& A, int cin, cudaStream_t s) {
-    const dim3 grid((A.w + kTile - 1) / kTile, A.h, A.n);
-    if (cin == 16)
-        conv3x3_kernel<16><<<grid, 128, 0, s>>>(A);
-    else
-        conv3x3_kernel<32><<<grid, 128, 0, s>>>(A);
+template <int CIN>
+static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
+    // resident CTAs per SM, found (and the shared-memory limit raised) once
+    // per device
+    static int per_device[64] = {};
+    const size_t smem = sizeof(ConvSmem<CIN>) + 128;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int scratch = 0;
+    int& per = dev >= 0 && dev < 64 ? per_device[dev] : scratch;
+    if (per == 0) {
+        cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(conv3x3_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        // shared memory bounds the CTAs per SM (registers allow 7 of 128
+        // threads); TMEM allows 8 of 64 columns; 4 keeps both with room
+        int smem_sm = 0;
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        per = (int)(smem_sm / (smem + 1024));   // 1 KB reserved per CTA
+        if (per < 1) per = 1;
+        if (per > 4) per = 4;
+    }
+    const int ntiles = ((A.w + kTile - 1) / kTile) * A.h * A.n;
+    const int grid = ntiles < sms * per ? ntiles : sms * per;
+    if (grid <= 0) return cudaSuccess;
+    conv3x3_kernel<CIN><<<grid, 128, smem, s>>>(A);
     return cudaGetLastError();
+}
+
+cudaError_t launch_conv(const ConvArgs& A, int cin, cudaStream_t s) {
+    return cin == 16 ? launch_conv_t<16>(A, s) : launch_conv_t<32>(A, s);
 }
 
 cudaError_t launch_wgrad(const WgradArgs& A, int cin, cudaStream_t s) {

@@ -320,6 +320,28 @@ def evaluate(params: np.ndarray, seeds, spps=(1, 2, 4, 8, 16, 32, 64, 128, 256),
     return res
 
 
+def time_inference(params: np.ndarray, width=854, height=480, calls=20) -> dict:
+    """Wall and CUDA-event milliseconds of one rc_denoise_learned call on a
+    1-spp render of a held-out Cornell variant (3 untimed calls first)."""
+    w = scenes.cornell_variant(5000, width, height)
+    with api.Context(width, height, 0, api.RC_MATH_FAST) as ctx:
+        ctx.upload(api.build_scene(w.scene))
+        ctx.render(api.workload_camera(w), (w.nee_enabled, w.nee_firefly_clamp), 0, 1)
+        for _ in range(3):
+            ctx.denoise_learned(params, read=False)
+        ctx.synchronize()
+        ctx.set_kernel_timing(True)
+        ctx.kernel_times()
+        t0 = time.perf_counter()
+        for _ in range(calls):
+            ctx.denoise_learned(params, read=False)
+        ctx.synchronize()
+        wall = (time.perf_counter() - t0) / calls * 1e3
+        kt = ctx.kernel_times()
+        ctx.set_kernel_timing(False)
+    return {"wall_ms": wall, "kernel_ms": kt["kpcnn"][0] / calls, "launches_per_call": kt["kpcnn"][1] // calls * 7}
+
+
 def _main(argv=None) -> int:
     """Renders the training set, trains, saves the weights, evaluates."""
     import argparse
@@ -335,7 +357,12 @@ def _main(argv=None) -> int:
     ap.add_argument("--out", default=WEIGHTS)
     ap.add_argument("--report", default="")
     ap.add_argument("--eval-only", action="store_true")
+    ap.add_argument("--time-inference", action="store_true",
+                    help="time rc_denoise_learned on a 1-spp 854x480 frame (3 warm-up + 20 timed calls)")
     args = ap.parse_args(argv)
+    if args.time_inference:
+        print(json.dumps(time_inference(load(args.out))))
+        return 0
     if args.eval_only:
         params = load(args.out)
     else:
