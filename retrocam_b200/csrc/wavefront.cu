@@ -458,6 +458,10 @@ static int grid_for(const void* fn, int block) {
 // atomicAdd per warp), so a warp is not held by its slowest ray.  Same rays
 // and results as wf_trace; only the schedule differs.
 
+// Stack entries of the refill trace: the binary walk pushes at most one per
+// level (guarded at 62, as the reference), the 4-wide walk up to three.
+constexpr int kDynStack = 96;
+
 // Pops the next stack entry not culled by the current hit distance.
 DI bool pop_packed(const int2* stk, int& top, float cull, TravNode& n) {
     while (top > 0) {
@@ -480,6 +484,9 @@ struct LaneRay {
     int top;
 };
 
+// kWide: interior steps over the 4-wide nodes (scene.nodes4) instead of the
+// binary records.
+template <bool kWide>
 __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
@@ -499,7 +506,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
     // traversal stack, 8 bytes an entry: (ref, count | entry distance
     // truncated to its top 16 bits); truncation rounds a positive distance
     // down, so the pop-time cull `t > hit` never drops a needed entry
-    int2 stk[64];
+    int2 stk[kDynStack];
     LaneRay L;
     L.item = -1;
     L.top = 0;
@@ -583,6 +590,51 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
                     if (L.node.cnt > 0) {
                         L.leaf = L.node;
                         L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                    } else if (kWide) {
+                        // 4-wide node: hit children ordered by entry distance,
+                        // the nearest entered, the others pushed far to near
+                        const Node4* n4 = S.nodes4 + L.node.ref;
+                        const float4 lx = __ldg(&n4->lox), hx = __ldg(&n4->hix), ly = __ldg(&n4->loy);
+                        const float4 hy = __ldg(&n4->hiy), lz = __ldg(&n4->loz), hz = __ldg(&n4->hiz);
+                        const int4 cr = __ldg(&n4->ref), cc = __ldg(&n4->cnt);
+                        const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
+                        const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
+                        const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+                        const int CR[4] = {cr.x, cr.y, cr.z, cr.w}, CC[4] = {cc.x, cc.y, cc.z, cc.w};
+                        float t4[4];
+                        unsigned int key[4];
+#pragma unroll
+                        for (int k = 0; k < 4; ++k) {
+                            const bool hit = CC[k] >= 0 &&
+                                             tslab(g, L.r, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k], t4[k]) &&
+                                             !(t4[k] > L.h.t);
+                            key[k] = hit ? ((__float_as_uint(fmaxf(t4[k], 0.0f)) & ~3u) | (unsigned int)k)
+                                         : 0xffffffffu;
+                        }
+                        cswap(key[0], key[1]);
+                        cswap(key[2], key[3]);
+                        cswap(key[0], key[2]);
+                        cswap(key[1], key[3]);
+                        cswap(key[1], key[2]);
+                        if (key[0] == 0xffffffffu) {
+                            L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                        } else {
+#pragma unroll
+                            for (int k = 3; k >= 1; --k) {
+                                if (key[k] != 0xffffffffu) {
+                                    if (L.top < kDynStack) {
+                                        const int s = key[k] & 3u;
+                                        stk[L.top++] = make_int2(CR[s], (CC[s] & 0xffff) |
+                                                                            (__float_as_int(t4[s]) & (int)0xffff0000));
+                                    } else {
+                                        g.flags |= RC_GUARD_TRAVERSAL_CAP;
+                                    }
+                                }
+                            }
+                            const int s0 = key[0] & 3u;
+                            L.node.ref = CR[s0];
+                            L.node.cnt = CC[s0];
+                        }
                     } else {
                         const NodeRec* nrec = S.nodes + L.node.ref;
                         const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
@@ -660,7 +712,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
 // kernel and block size (64, 128 or 256 threads).
 struct WfGrids {
     int gen = 0, acc = 0;
-    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, dyn[3] = {};
+    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, dyn[3] = {}, dyn4[3] = {};
 };
 static int block_class(int block) { return block <= 64 ? 0 : (block <= 128 ? 1 : 2); }
 static WfGrids& grids() {
@@ -674,7 +726,8 @@ static WfGrids& grids() {
             g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
             g.shade[c] = grid_for((const void*)wf_shade, b);
 #if !RC_EXACT
-            g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
+            g.dyn[c] = grid_for((const void*)wf_trace_dyn<false>, b);
+            g.dyn4[c] = grid_for((const void*)wf_trace_dyn<true>, b);
 #endif
         }
     }
@@ -693,7 +746,10 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
 #if !RC_EXACT
     // the refill trace packs leaf counts into 16 bits of a stack entry
     if (A.dynamic_fetch && A.scene.max_leaf < 0x10000) {
-        wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
+        if (A.scene.nodes4)
+            wf_trace_dyn<true><<<grids().dyn4[c], b, 0, s>>>(A);
+        else
+            wf_trace_dyn<false><<<grids().dyn[c], b, 0, s>>>(A);
         return cudaGetLastError();
     }
 #endif
