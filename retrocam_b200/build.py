@@ -1,7 +1,9 @@
 """Builds retrocam_b200/_lib/libretrocam.so for sm_100a.
 
-  kernels.cu  x2  -DRC_EXACT=1 -fmad=false  (bit-exact math, rc::exact)
-                  -DRC_EXACT=0              (fast math, rc::fast)
+  kernels.cu, wavefront.cu  x2
+                  -DRC_EXACT=1 -fmad=false  (bit-exact math, rc::exact)
+                  -DRC_EXACT=0 -prec-div=false  (fast math, rc::fast: FMA
+                  contraction, the approximate divide within 2 ulp)
   api.cu          C ABI, device half
   noalloc.cu      allocation-free à-trous entry point
   kpcnn.cu        learned denoiser (tcgen05 BF16 convolutions)
@@ -64,7 +66,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with open(os.path.join(BUILD, "ptxas.log"), "w") as log:
         for name, flags in (("kernels_exact", ["-DRC_EXACT=1", "-fmad=false", "-prec-div=true",
                                                "-prec-sqrt=true", "-ftz=false"]),
-                            ("kernels_fast", ["-DRC_EXACT=0", "-fmad=true"])):
+                            ("kernels_fast", ["-DRC_EXACT=0", "-fmad=true", "-prec-div=false"])):
             for src in ("kernels", "wavefront"):
                 o = os.path.join(BUILD, f"{src}_{name.split('_')[1]}.o")
                 _run(common + flags + ["-c", os.path.join(CSRC, src + ".cu"), "-o", o], log)

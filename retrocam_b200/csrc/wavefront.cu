@@ -15,7 +15,8 @@
 //   wf_accumulate  per pixel, the samples in frame order, LCA channel
 //                  assembly, NaN scrub, variance, G-buffer on frame 0
 //                  (pathtrace.comp:601-655)
-// Queues are compacted with a warp ballot + popc and one atomicAdd per warp.
+// Queues are compacted with warp ballots: one shared-memory atomic per warp
+// and one global atomicAdd per block (generate, shade) or per warp (trace).
 // Path arithmetic is the megakernel's, operation for operation, and the
 // accumulation adds samples in frame order, so exact-math results stay
 // bit-identical to the oracle.  Kernels are grid-stride loops over device-side
@@ -25,17 +26,42 @@
 namespace rc {
 namespace RC_NS {
 
-// Appends `value` to queue q when `want`, one atomic per warp.
-DI void push_queue(bool want, int value, int* q, unsigned int* len) {
-    const unsigned int active = __activemask();
-    const unsigned int m = __ballot_sync(active, want);
-    if (m == 0u) return;
+// Block-wide appends to two queues with counters la and lb (lb unused when
+// no thread wants it): one shared-memory atomic per warp and one global
+// atomicAdd per queue per block.  Appends to one global counter serialise in
+// L2 (about 1 ns each), so one per warp bounded the generate and shade
+// kernels.  Every thread of the block calls it the same number of times;
+// `sh.cnt` starts at zero.  Returns each wanting thread's queue slot; a
+// warp's slots are consecutive.
+struct BlockAppend {
+    unsigned int cnt[2];
+    unsigned int base[2];
+};
+
+DI void block_append(BlockAppend& sh, bool wa, bool wb, unsigned int* la, unsigned int* lb,
+                     unsigned int& slot_a, unsigned int& slot_b) {
+    const unsigned int FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const int leader = __ffs(m) - 1;
-    unsigned int base = 0;
-    if (lane == leader) base = atomicAdd(len, (unsigned int)__popc(m));
-    base = __shfl_sync(active, base, leader);
-    if (want) q[base + __popc(m & ((1u << lane) - 1u))] = value;
+    const unsigned int ma = __ballot_sync(FULL, wa), mb = __ballot_sync(FULL, wb);
+    unsigned int oa = 0u, ob = 0u;
+    if (lane == 0) {
+        if (ma) oa = atomicAdd(&sh.cnt[0], (unsigned int)__popc(ma));
+        if (mb) ob = atomicAdd(&sh.cnt[1], (unsigned int)__popc(mb));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int ca = sh.cnt[0], cb = sh.cnt[1];
+        sh.base[0] = ca ? atomicAdd(la, ca) : 0u;
+        sh.base[1] = cb ? atomicAdd(lb, cb) : 0u;
+        sh.cnt[0] = 0u;
+        sh.cnt[1] = 0u;
+    }
+    __syncthreads();
+    oa = __shfl_sync(FULL, oa, 0);
+    ob = __shfl_sync(FULL, ob, 0);
+    const unsigned int below = (1u << lane) - 1u;
+    slot_a = sh.base[0] + oa + (unsigned int)__popc(ma & below);
+    slot_b = sh.base[1] + ob + (unsigned int)__popc(mb & below);
 }
 
 struct PathId {
@@ -77,13 +103,17 @@ DI bool lca_on(const CamParams& c) { return (fabs_(c.lca[0]) + fabs_(c.lca[2])) 
 
 __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
     const WaveBuffers& B = A.wb;
+    __shared__ BlockAppend sh;
+    if (threadIdx.x == 0) sh.cnt[0] = sh.cnt[1] = 0u;
+    __syncthreads();
     uint32_t paths = 0;
-    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < A.paths; p += gridDim.x * blockDim.x) {
-        const FrameSeg& sg = seg_at(A, seg_index(A, p));
+    for (int p0 = blockIdx.x * blockDim.x; p0 < A.paths; p0 += gridDim.x * blockDim.x) {
+        const int p = p0 + threadIdx.x;
+        bool want = false;
+        const FrameSeg& sg = seg_at(A, seg_index(A, p < A.paths ? p : A.paths - 1));
         const PathId id = decode(A, sg, p);
         const bool lca = sg.channels == 3;
-        bool want = false;
-        if (id.valid) {
+        if (p < A.paths && id.valid) {
             const int f = sg.first_frame + id.sample;
             uint32_t s = init_seed(id.px, id.py, lca ? f * 3 + id.channel : f);
             const Ray r = generate_ray(sg.cam, A.width, A.height, id.px, id.py, s,
@@ -96,7 +126,9 @@ __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
             want = true;
             ++paths;
         }
-        push_queue(want, p, B.rq[0], B.qlen + 0);
+        unsigned int slot, unused;
+        block_append(sh, want, false, B.qlen + 0, nullptr, slot, unused);
+        if (want) B.rq[0][slot] = p;
     }
     const unsigned int n = __reduce_add_sync(__activemask(), paths);
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(&A.counters->camera_paths, (unsigned long long)n);
@@ -168,192 +200,191 @@ __global__ void __launch_bounds__(256, 3) wf_shade(WaveArgs A) {
     const bool last = b == 5;
     const unsigned int n = B.qlen[cur];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.qlen[4] = 0u;  // work counter of the next trace
+    __shared__ BlockAppend sh;
+    if (threadIdx.x == 0) sh.cnt[0] = sh.cnt[1] = 0u;
+    __syncthreads();
     uint32_t hits = 0, lights = 0;
-    for (unsigned int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int p = B.rq[cur][i];
-        const float4 hv = B.hit[p];
-        const int prim = __float_as_int(hv.w);
-        float3 rad = xyz(B.rad[p]);
+    // block-uniform trip count: the appends at the bottom synchronise the block
+    for (unsigned int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const unsigned int i = i0 + threadIdx.x;
         bool cont = false, shadow_rec = false;
         float4 rec0, rec1, rec2, rec3;
-        // frame-0 albedo image: first hit of the G channel (or the only one)
-        bool alb_path = false;
-        PathId id;
-        ushort4* galb = nullptr;
-        if (b == 0) {
-            const FrameSeg& sg = seg_at(A, seg_index(A, p));
-            id = decode(A, sg, p);
-            alb_path = sg.first_frame + id.sample == 0 && id.channel == (sg.channels == 3 ? 1 : 0);
-            galb = sg.img.galb;
-        }
-        if (prim < 0) {
-            if (alb_path) galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
-            B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
-        } else {
-            ++hits;
-            const Ray ray = make_ray(xyz(B.o[p]), xyz(B.d[p]));
-            Hit h;
-            h.t = hv.x;
-            h.u = hv.y;
-            h.v = hv.z;
-            h.prim = prim;
-            const Surf sf = surface(S, ray, h);
-            const Mat m = load_mat(S, sf.mat);
-            const float3 rd = ray.d;
-            const float3 nrm = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
-            uint32_t seed = B.seed[p];
-            float3 thr = xyz(B.thr[p]);
-            const bool last_diffuse = B.thr[p].w != 0.0f;
-            if (alb_path) {
-                const float3 a = (m.transmission > 0.5f) ? f3(1.0f, 1.0f, 1.0f) : m.albedo;
-                galb[(long)id.py * A.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
+        int p = 0;
+        if (i < n) {
+            p = B.rq[cur][i];
+            const float4 hv = B.hit[p];
+            const int prim = __float_as_int(hv.w);
+            float3 rad = xyz(B.rad[p]);
+            // frame-0 albedo image: first hit of the G channel (or the only one)
+            bool alb_path = false;
+            PathId id;
+            ushort4* galb = nullptr;
+            if (b == 0) {
+                const FrameSeg& sg = seg_at(A, seg_index(A, p));
+                id = decode(A, sg, p);
+                alb_path = sg.first_frame + id.sample == 0 && id.channel == (sg.channels == 3 ? 1 : 0);
+                galb = sg.img.galb;
             }
-            if (!last_diffuse) rad = rad + (thr * m.emission) * m.strength;
-            bool alive = true;
-            if (b >= 2) {
-                float survive = gmax(m.albedo.x, gmax(m.albedo.y, m.albedo.z));
-                if (m.metallic > 0.5f || m.transmission > 0.5f) survive = 0.95f;
-                survive = gclamp(survive, 0.01f, 0.95f);
-                if (rnd(seed) > survive) alive = false;
-                else thr = thr / survive;
-            }
-            float3 no = f3(0, 0, 0), nd = f3(0, 0, 0);
-            bool nd_diffuse = false;
-            if (alive) {
-                if (m.transmission > 0.5f) {
-                    const bool entering = dot(rd, sf.normal) < 0.0f;
-                    const float eta = entering ? (1.0f / m.ior) : m.ior;
-                    const float cosI = fabs_(dot(rd, nrm));
-                    float r0 = (1.0f - m.ior) / (1.0f + m.ior);
-                    r0 *= r0;
-                    const float F = r0 + (1.0f - r0) * pow5(gclamp(1.0f - cosI, 0.0f, 1.0f));
-                    if (rnd(seed) < F) {
-                        nd = reflect(rd, nrm);
+            if (prim < 0) {
+                if (alb_path) galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
+                B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+            } else {
+                ++hits;
+                const Ray ray = make_ray(xyz(B.o[p]), xyz(B.d[p]));
+                Hit h;
+                h.t = hv.x;
+                h.u = hv.y;
+                h.v = hv.z;
+                h.prim = prim;
+                const Surf sf = surface(S, ray, h);
+                const Mat m = load_mat(S, sf.mat);
+                const float3 rd = ray.d;
+                const float3 nrm = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
+                uint32_t seed = B.seed[p];
+                float3 thr = xyz(B.thr[p]);
+                const bool last_diffuse = B.thr[p].w != 0.0f;
+                if (alb_path) {
+                    const float3 a = (m.transmission > 0.5f) ? f3(1.0f, 1.0f, 1.0f) : m.albedo;
+                    galb[(long)id.py * A.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
+                }
+                if (!last_diffuse) rad = rad + (thr * m.emission) * m.strength;
+                bool alive = true;
+                if (b >= 2) {
+                    float survive = gmax(m.albedo.x, gmax(m.albedo.y, m.albedo.z));
+                    if (m.metallic > 0.5f || m.transmission > 0.5f) survive = 0.95f;
+                    survive = gclamp(survive, 0.01f, 0.95f);
+                    if (rnd(seed) > survive) alive = false;
+                    else thr = thr / survive;
+                }
+                float3 no = f3(0, 0, 0), nd = f3(0, 0, 0);
+                bool nd_diffuse = false;
+                if (alive) {
+                    if (m.transmission > 0.5f) {
+                        const bool entering = dot(rd, sf.normal) < 0.0f;
+                        const float eta = entering ? (1.0f / m.ior) : m.ior;
+                        const float cosI = fabs_(dot(rd, nrm));
+                        float r0 = (1.0f - m.ior) / (1.0f + m.ior);
+                        r0 *= r0;
+                        const float F = r0 + (1.0f - r0) * pow5(gclamp(1.0f - cosI, 0.0f, 1.0f));
+                        if (rnd(seed) < F) {
+                            nd = reflect(rd, nrm);
+                        } else {
+                            float3 refr = refract(rd, nrm, eta);
+                            if (dot(refr, refr) < 0.001f) refr = reflect(rd, nrm);
+                            nd = normalize(refr);
+                        }
+                        no = sf.pos + nd * 2e-3f;
+                        thr = thr * m.albedo;
+                    } else if (m.metallic > 0.5f) {
+                        const float3 wo = -rd;
+                        const float alpha = gmax(m.roughness, 1e-3f);
+                        const float3 up3 = fabs_(nrm.y) < 0.9999f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);
+                        const float3 T = normalize(cross(up3, nrm));
+                        const float3 Bv = cross(nrm, T);
+                        const float3 wol = f3(dot(wo, T), dot(wo, nrm), dot(wo, Bv));
+                        const float u1 = rnd(seed);
+                        const float u2 = rnd(seed);
+                        const float3 hl = sample_ggx_vndf(wol, alpha, u1, u2);
+                        const float3 hh = normalize(T * hl.x + nrm * hl.y + Bv * hl.z);
+                        nd = reflect(-wo, hh);
+                        if (dot(nd, nrm) <= 0.0f) nd = reflect(-wo, nrm);
+                        const float NdotL = gmax(dot(nrm, nd), 1e-4f);
+                        const float NdotV = gmax(dot(nrm, wo), 1e-4f);
+                        const float HdotV = gmax(dot(hh, wo), 1e-4f);
+                        const float p5 = pow5(1.0f - HdotV);
+                        const float3 F = m.albedo + f3(1.0f - m.albedo.x, 1.0f - m.albedo.y, 1.0f - m.albedo.z) * p5;
+                        const float G1 = smith_g1(NdotV, alpha);
+                        const float G2 = smith_g2(NdotL, NdotV, alpha);
+                        thr = thr * (F * (G2 / gmax(G1, 1e-7f)));
+                        no = sf.pos + nrm * 2e-3f;
                     } else {
-                        float3 refr = refract(rd, nrm, eta);
-                        if (dot(refr, refr) < 0.001f) refr = reflect(rd, nrm);
-                        nd = normalize(refr);
-                    }
-                    no = sf.pos + nd * 2e-3f;
-                    thr = thr * m.albedo;
-                } else if (m.metallic > 0.5f) {
-                    const float3 wo = -rd;
-                    const float alpha = gmax(m.roughness, 1e-3f);
-                    const float3 up3 = fabs_(nrm.y) < 0.9999f ? f3(0.0f, 1.0f, 0.0f) : f3(1.0f, 0.0f, 0.0f);
-                    const float3 T = normalize(cross(up3, nrm));
-                    const float3 Bv = cross(nrm, T);
-                    const float3 wol = f3(dot(wo, T), dot(wo, nrm), dot(wo, Bv));
-                    const float u1 = rnd(seed);
-                    const float u2 = rnd(seed);
-                    const float3 hl = sample_ggx_vndf(wol, alpha, u1, u2);
-                    const float3 hh = normalize(T * hl.x + nrm * hl.y + Bv * hl.z);
-                    nd = reflect(-wo, hh);
-                    if (dot(nd, nrm) <= 0.0f) nd = reflect(-wo, nrm);
-                    const float NdotL = gmax(dot(nrm, nd), 1e-4f);
-                    const float NdotV = gmax(dot(nrm, wo), 1e-4f);
-                    const float HdotV = gmax(dot(hh, wo), 1e-4f);
-                    const float p5 = pow5(1.0f - HdotV);
-                    const float3 F = m.albedo + f3(1.0f - m.albedo.x, 1.0f - m.albedo.y, 1.0f - m.albedo.z) * p5;
-                    const float G1 = smith_g1(NdotV, alpha);
-                    const float G2 = smith_g2(NdotL, NdotV, alpha);
-                    thr = thr * (F * (G2 / gmax(G1, 1e-7f)));
-                    no = sf.pos + nrm * 2e-3f;
-                } else {
-                    // NEE (pathtrace.comp:341-395) up to the visibility test;
-                    // the test and the add happen in the next wf_trace.
-                    if (A.nee_enabled != 0) {
-                        bool early = true;
-                        if (S.light_count > 0 && S.total_light_power > 0.0f) {
-                            const float u = rnd(seed);
-                            int sel = S.light_count - 1;
-                            for (int q = 0; q < S.light_count; ++q)
-                                if (u < __ldg(S.light_cdf + q)) {
-                                    sel = q;
-                                    break;
-                                }
-                            const float4* Lr = S.lights + 5 * sel;
-                            const float4 l0 = __ldg(Lr + 0), l1 = __ldg(Lr + 1), l2 = __ldg(Lr + 2);
-                            const float4 l3 = __ldg(Lr + 3), l4 = __ldg(Lr + 4);
-                            ++lights;
-                            const float pick = l3.w / S.total_light_power;
-                            if (pick > 0.0f) {
-                                float r1 = rnd(seed);
-                                float r2 = rnd(seed);
-                                if (r1 + r2 > 1.0f) {
-                                    r1 = 1.0f - r1;
-                                    r2 = 1.0f - r2;
-                                }
-                                const float3 lv0 = xyz(l0);
-                                const float3 lp = lv0 + r1 * (xyz(l1) - lv0) + r2 * (xyz(l2) - lv0);
-                                const float3 to = lp - sf.pos;
-                                const float dist2 = dot(to, to);
-                                const float dist = sqrtf(dist2);
-                                const float3 sd = to / dist;
-                                const float cos_hit = dot(nrm, sd);
-                                if (cos_hit > 0.0f) {
-                                    const float cos_light = fabs_(dot(xyz(l4), sd));
-                                    if (cos_light > 0.0f) {
-                                        const float area = l0.w;
-                                        const float dist2_safe = gmax(dist2, area);
-                                        const float pdf = pick * (dist2_safe / (area * cos_light));
-                                        float3 contrib = f3(0.0f, 0.0f, 0.0f);
-                                        if (pdf > 0.0f) {
-                                            const float3 em = xyz(l3);
-                                            contrib = (((m.albedo / 3.14159265359f) * em) * cos_hit) / pdf;
-                                            const float cap = dot(em, f3(0.299f, 0.587f, 0.114f)) * A.firefly_clamp;
-                                            contrib = vmin(contrib, f3(cap, cap, cap));
+                        // NEE (pathtrace.comp:341-395) up to the visibility test;
+                        // the test and the add happen in the next wf_trace.
+                        if (A.nee_enabled != 0) {
+                            bool early = true;
+                            if (S.light_count > 0 && S.total_light_power > 0.0f) {
+                                const float u = rnd(seed);
+                                int sel = S.light_count - 1;
+                                for (int q = 0; q < S.light_count; ++q)
+                                    if (u < __ldg(S.light_cdf + q)) {
+                                        sel = q;
+                                        break;
+                                    }
+                                const float4* Lr = S.lights + 5 * sel;
+                                const float4 l0 = __ldg(Lr + 0), l1 = __ldg(Lr + 1), l2 = __ldg(Lr + 2);
+                                const float4 l3 = __ldg(Lr + 3), l4 = __ldg(Lr + 4);
+                                ++lights;
+                                const float pick = l3.w / S.total_light_power;
+                                if (pick > 0.0f) {
+                                    float r1 = rnd(seed);
+                                    float r2 = rnd(seed);
+                                    if (r1 + r2 > 1.0f) {
+                                        r1 = 1.0f - r1;
+                                        r2 = 1.0f - r2;
+                                    }
+                                    const float3 lv0 = xyz(l0);
+                                    const float3 lp = lv0 + r1 * (xyz(l1) - lv0) + r2 * (xyz(l2) - lv0);
+                                    const float3 to = lp - sf.pos;
+                                    const float dist2 = dot(to, to);
+                                    const float dist = sqrtf(dist2);
+                                    const float3 sd = to / dist;
+                                    const float cos_hit = dot(nrm, sd);
+                                    if (cos_hit > 0.0f) {
+                                        const float cos_light = fabs_(dot(xyz(l4), sd));
+                                        if (cos_light > 0.0f) {
+                                            const float area = l0.w;
+                                            const float dist2_safe = gmax(dist2, area);
+                                            const float pdf = pick * (dist2_safe / (area * cos_light));
+                                            float3 contrib = f3(0.0f, 0.0f, 0.0f);
+                                            if (pdf > 0.0f) {
+                                                const float3 em = xyz(l3);
+                                                contrib = (((m.albedo / 3.14159265359f) * em) * cos_hit) / pdf;
+                                                const float cap = dot(em, f3(0.299f, 0.587f, 0.114f)) * A.firefly_clamp;
+                                                contrib = vmin(contrib, f3(cap, cap, cap));
+                                            }
+                                            const float3 so = sf.pos + nrm * 2e-3f;
+                                            rec0 = make_float4(so.x, so.y, so.z, dist - 4e-3f);
+                                            rec1 = make_float4(sd.x, sd.y, sd.z, __int_as_float(p));
+                                            rec2 = make_float4(thr.x, thr.y, thr.z, __int_as_float(last ? 1 : 0));
+                                            rec3 = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                                            shadow_rec = true;
+                                            early = false;
                                         }
-                                        const float3 so = sf.pos + nrm * 2e-3f;
-                                        rec0 = make_float4(so.x, so.y, so.z, dist - 4e-3f);
-                                        rec1 = make_float4(sd.x, sd.y, sd.z, __int_as_float(p));
-                                        rec2 = make_float4(thr.x, thr.y, thr.z, __int_as_float(last ? 1 : 0));
-                                        rec3 = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
-                                        shadow_rec = true;
-                                        early = false;
                                     }
                                 }
                             }
+                            if (early) rad = rad + thr * f3(0.0f, 0.0f, 0.0f);
                         }
-                        if (early) rad = rad + thr * f3(0.0f, 0.0f, 0.0f);
+                        const float u1 = rnd(seed);
+                        const float u2 = rnd(seed);
+                        nd = cosine_hemisphere(u1, u2, nrm);
+                        thr = thr * m.albedo;
+                        no = sf.pos + nrm * 1e-3f;
+                        nd_diffuse = true;
                     }
-                    const float u1 = rnd(seed);
-                    const float u2 = rnd(seed);
-                    nd = cosine_hemisphere(u1, u2, nrm);
-                    thr = thr * m.albedo;
-                    no = sf.pos + nrm * 1e-3f;
-                    nd_diffuse = true;
+                    cont = !last;
                 }
-                cont = !last;
-            }
-            B.rad[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
-            if (cont) {
-                B.o[p] = make_float4(no.x, no.y, no.z, 0.0f);
-                B.d[p] = make_float4(nd.x, nd.y, nd.z, 0.0f);
-                B.thr[p] = make_float4(thr.x, thr.y, thr.z, nd_diffuse ? 1.0f : 0.0f);
-                B.seed[p] = seed;
-            } else if (!shadow_rec) {
-                B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                B.rad[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                if (cont) {
+                    B.o[p] = make_float4(no.x, no.y, no.z, 0.0f);
+                    B.d[p] = make_float4(nd.x, nd.y, nd.z, 0.0f);
+                    B.thr[p] = make_float4(thr.x, thr.y, thr.z, nd_diffuse ? 1.0f : 0.0f);
+                    B.seed[p] = seed;
+                } else if (!shadow_rec) {
+                    B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                }
             }
         }
-        push_queue(cont, p, B.rq[nxt], B.qlen + nxt);
-        // shadow records go to the slot the ray index takes in sq[cur]
-        {
-            const unsigned int active = __activemask();
-            const unsigned int m = __ballot_sync(active, shadow_rec);
-            if (m != 0u) {
-                const int lane = threadIdx.x & 31;
-                const int leader = __ffs(m) - 1;
-                unsigned int base = 0;
-                if (lane == leader) base = atomicAdd(B.qlen + 2 + cur, (unsigned int)__popc(m));
-                base = __shfl_sync(active, base, leader);
-                if (shadow_rec) {
-                    float4* r = B.srec[cur] + 4 * (base + __popc(m & ((1u << lane) - 1u)));
-                    r[0] = rec0;
-                    r[1] = rec1;
-                    r[2] = rec2;
-                    r[3] = rec3;
-                }
-            }
+        // continuing paths -> rq[nxt]; shadow records -> srec[cur]
+        unsigned int slot_r, slot_s;
+        block_append(sh, cont, shadow_rec, B.qlen + nxt, B.qlen + 2 + cur, slot_r, slot_s);
+        if (cont) B.rq[nxt][slot_r] = p;
+        if (shadow_rec) {
+            float4* r = B.srec[cur] + 4 * slot_s;
+            r[0] = rec0;
+            r[1] = rec1;
+            r[2] = rec2;
+            r[3] = rec3;
         }
     }
     const unsigned int active = __activemask();
