@@ -120,8 +120,8 @@ __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
                                        lca ? sg.cam.lca[id.channel] : 0.0f);
             B.o[p] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
             B.d[p] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
-            B.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-            B.rad[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            // throughput (1, 1, 1) and radiance 0 are implied at bounce 0:
+            // wf_shade takes them as constants instead of reading them
             B.seed[p] = s;
             want = true;
             ++paths;
@@ -214,7 +214,7 @@ __global__ void __launch_bounds__(256, 3) wf_shade(WaveArgs A) {
             p = B.rq[cur][i];
             const float4 hv = B.hit[p];
             const int prim = __float_as_int(hv.w);
-            float3 rad = xyz(B.rad[p]);
+            float3 rad = b == 0 ? f3(0.0f, 0.0f, 0.0f) : xyz(B.rad[p]);
             // frame-0 albedo image: first hit of the G channel (or the only one)
             bool alb_path = false;
             PathId id;
@@ -241,8 +241,9 @@ __global__ void __launch_bounds__(256, 3) wf_shade(WaveArgs A) {
                 const float3 rd = ray.d;
                 const float3 nrm = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
                 uint32_t seed = B.seed[p];
-                float3 thr = xyz(B.thr[p]);
-                const bool last_diffuse = B.thr[p].w != 0.0f;
+                const float4 thr4 = b == 0 ? make_float4(1.0f, 1.0f, 1.0f, 0.0f) : B.thr[p];
+                float3 thr = xyz(thr4);
+                const bool last_diffuse = thr4.w != 0.0f;
                 if (alb_path) {
                     const float3 a = (m.transmission > 0.5f) ? f3(1.0f, 1.0f, 1.0f) : m.albedo;
                     galb[(long)id.py * A.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
@@ -518,7 +519,7 @@ struct LaneRay {
 // kWide: interior steps over the 4-wide nodes (scene.nodes4) instead of the
 // binary records.
 template <bool kWide>
-__global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
+DI void trace_dyn(const WaveArgs& A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
     const int cur = A.bounce & 1;
@@ -735,6 +736,13 @@ __global__ void __launch_bounds__(256) wf_trace_dyn(WaveArgs A) {
         if (gf) atomicOr(&A.counters->error_word, gf);
     }
 }
+
+// Binary walk: registers capped at 56 (62 uncapped, no spills either way),
+// so 9 blocks of 128 threads fit an SM instead of 8; the kernel waits on L1
+// latency and the extra warps pay (65.0 vs 67.4 ms per export frame).
+__global__ void __maxnreg__(56) wf_trace_dyn(WaveArgs A) { trace_dyn<false>(A); }
+// 4-wide walk: uncapped (77 registers; 56 spills)
+__global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<true>(A); }
 #endif
 
 // Launchers; the chunk sequence (generate, 7 x trace, 6 x shade interleaved,
@@ -757,8 +765,8 @@ static WfGrids& grids() {
             g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
             g.shade[c] = grid_for((const void*)wf_shade, b);
 #if !RC_EXACT
-            g.dyn[c] = grid_for((const void*)wf_trace_dyn<false>, b);
-            g.dyn4[c] = grid_for((const void*)wf_trace_dyn<true>, b);
+            g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
+            g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
 #endif
         }
     }
@@ -778,9 +786,9 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
     // the refill trace packs leaf counts into 16 bits of a stack entry
     if (A.dynamic_fetch && A.scene.max_leaf < 0x10000) {
         if (A.scene.nodes4)
-            wf_trace_dyn<true><<<grids().dyn4[c], b, 0, s>>>(A);
+            wf_trace_dyn4<<<grids().dyn4[c], b, 0, s>>>(A);
         else
-            wf_trace_dyn<false><<<grids().dyn[c], b, 0, s>>>(A);
+            wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
         return cudaGetLastError();
     }
 #endif
