@@ -188,10 +188,10 @@ __global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
 
 // One bounce of pathtrace.comp's traceRadiance for every path in ray queue
 // rq[bounce&1] whose closest hit wf_trace has stored.
-// Registers capped for 3 blocks of 256 threads per SM (85): the kernel
-// streams path state and waits on memory, so resident warps matter more
-// than the registers the compiler would otherwise use (105).
-__global__ void __launch_bounds__(256, 3) wf_shade(WaveArgs A) {
+// Registers capped at 72 (105 uncapped, no spills at 72; 64 spills): the
+// kernel streams path state and waits on memory, so resident warps matter
+// more than registers (7 blocks of 128 threads per SM instead of 4).
+__global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
     const int cur = A.bounce & 1;
