@@ -110,8 +110,9 @@ struct rc_ctx {
     DevBuf batch_img, batch_segs;   // per-frame images and chunk segments of a batch
     // photon first-segment split: specular / other triangles with own BVHs
     DevBuf sp_nodes, sp_isect, sp_orig, df_nodes, df_isect, ph_queue, ph_queue_len;
-    // gather hits per pixel (see GatherArgs::hit_cache)
-    DevBuf gcache, batch_gcache;
+    // gather hits per pixel (see GatherArgs::hit_cache); the heavy-pixel
+    // list of the fast gather (count, then pixel indices)
+    DevBuf gcache, batch_gcache, gheavy;
     uint64_t gcache_key = 0;
     bool gcache_valid = false;
     unsigned int scene_gen = 0;
@@ -300,7 +301,7 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
                       &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs, &ctx->sp_nodes,
                       &ctx->sp_isect, &ctx->sp_orig, &ctx->df_nodes, &ctx->df_isect, &ctx->ph_queue,
-                      &ctx->ph_queue_len, &ctx->gcache, &ctx->batch_gcache})
+                      &ctx->ph_queue_len, &ctx->gcache, &ctx->batch_gcache, &ctx->gheavy})
         release(*b);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -1051,9 +1052,17 @@ int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, f
         ctx->gcache_valid = true;
     }
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    A.heavy = nullptr;
+    A.heavy_len = nullptr;
+    if (!ex) {
+        // a batch allocated the list before its capture
+        if (!ctx->gcache_force) CK(ensure(ctx->gheavy, ((size_t)ctx->width * ctx->height + 1) * sizeof(int)));
+        A.heavy_len = (unsigned int*)ctx->gheavy.ptr;
+        A.heavy = (int*)ctx->gheavy.ptr + 1;
+    }
     const cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_GATHER, [&] {
         return ex ? exact::launch_photon_gather(A, ctx->stream) : fast::launch_photon_gather(A, ctx->stream);
-    });
+    }, ex ? 1 : 2);
     return launch_err(ctx, e, "photon gather");
 }
 
@@ -1473,6 +1482,7 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
     CK(cudaStreamSynchronize(ctx->stream));
     // ---- the sequence ----
     if (any_sppm) CK(ensure(ctx->gcache, px * sizeof(float4)));
+    if (any_sppm) CK(ensure(ctx->gheavy, (px + 1) * sizeof(int)));
     auto sequence = [&]() -> int {
         ctx->gcache_valid = false;   // each replay traces its frames' gather hits afresh
         if (batched)
@@ -1508,7 +1518,7 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
         for (const DevBuf* b : {&ctx->photons, &ctx->heads, &ctx->next, &ctx->cell_of, &ctx->cell_count,
                                 &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw,
                                 &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len, &ctx->gcache,
-                                &ctx->batch_gcache})
+                                &ctx->batch_gcache, &ctx->gheavy})
             key = fnv1a(key, &b->ptr, sizeof(void*));
         const int shape[9] = {ctx->chunk_paths,  ctx->wide_bvh,       ctx->trace_block,
                               ctx->shade_block,  ctx->photon_block,   ctx->width,

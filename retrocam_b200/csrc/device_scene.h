@@ -168,6 +168,11 @@ struct GatherArgs {
     // per pixel in hit_cache, 2 reads it back, 0 traces without the cache.
     float4* hit_cache;
     int cache_mode;
+    // Fast build with a hit cache: pixels whose 27 cells hold many photons
+    // are listed here (heavy_len of them, pixel index y * W + x) and
+    // gathered one warp per pixel by a second kernel; null: one pass.
+    int* heavy;
+    unsigned int* heavy_len;
 };
 
 struct AtrousArgs {

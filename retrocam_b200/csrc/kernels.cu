@@ -350,6 +350,31 @@ __global__ void __launch_bounds__(256) photon_bounce_kernel(PhotonArgs A) {
 }
 #endif
 
+// The gathered caustic of one pixel scaled into radiance and added into the
+// accumulation (photon_gather.comp:200-222).
+DI void add_caustic(const GatherArgs& A, long pix, int hm, float3 caustic, float r2) {
+    const float PI_G = 3.14159265358979f;
+    const float4 ma = __ldg(A.scene.materials + 4 * hm);
+    float3 L = (xyz(ma) * caustic) / (PI_G * r2);
+    if (bad(L.x) || bad(L.y) || bad(L.z)) L = f3(0, 0, 0);
+    if (A.weight != 1.0f) L = L * A.weight;
+    float4* a = A.img.accum + pix;
+    float4 v = *a;
+    v.x = v.x + L.x;
+    v.y = v.y + L.y;
+    v.z = v.z + L.z;
+    v.w = v.w + 0.0f;
+    *a = v;
+}
+
+#if !RC_EXACT
+// Fast build: a pixel whose 27 cells hold more than this many photons (as
+// walked, at most 512 a cell) is gathered by photon_gather_heavy, one warp
+// per pixel.  One thread walking 27 x 512 photons held a whole gather launch
+// (the rest of the GPU idle) for about 0.5 ms.
+constexpr unsigned int kGatherLight = 64;
+#endif
+
 // photon_gather.comp:128-222: pinhole ray to the first diffuse surface,
 // 3x3x3 hash-cell query, Epanechnikov kernel, added into the accumulation.
 template <bool kAtParent>
@@ -360,6 +385,7 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
     const int W = A.img.width, H = A.img.height;
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0, hits = 0;
+    bool heavy = false;
     if (px < W && py < H) {
         const DeviceScene& S = A.scene;
         const CamParams& cam = A.cam;
@@ -409,9 +435,23 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
             ray = make_ray(sf.pos + nd * 2e-3f, nd);
         }
         if (A.cache_mode == 1) A.hit_cache[pix] = make_float4(hp.x, hp.y, hp.z, __int_as_float(found ? hm : -1));
+        const float r = A.radius, r2 = r * r;
+        const int ccx = (int)floorf(hp.x / r), ccy = (int)floorf(hp.y / r), ccz = (int)floorf(hp.z / r);
+#if !RC_EXACT
+        if (found && A.heavy && A.cache_mode != 0) {
+            unsigned int total = 0;
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        const int h = cell_hash(ccx + dx, ccy + dy, ccz + dz, A.hash_size);
+                        const unsigned int n = __ldg(A.cell_start + h + 1) - __ldg(A.cell_start + h);
+                        total += n < 512u ? n : 512u;
+                    }
+            heavy = total > kGatherLight;
+            found = found && !heavy;
+        }
+#endif
         if (found) {
-            const float r = A.radius, r2 = r * r;
-            const int ccx = (int)floorf(hp.x / r), ccy = (int)floorf(hp.y / r), ccz = (int)floorf(hp.z / r);
             float3 caustic = f3(0, 0, 0);
             for (int dz = -1; dz <= 1; ++dz)
                 for (int dy = -1; dy <= 1; ++dy)
@@ -454,24 +494,82 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
                             }
                         }
                     }
-            const float PI_G = 3.14159265358979f;
-            const float4 ma = __ldg(S.materials + 4 * hm);
-            float3 L = (xyz(ma) * caustic) / (PI_G * r2);
-            if (bad(L.x) || bad(L.y) || bad(L.z)) L = f3(0, 0, 0);
-            if (A.weight != 1.0f) L = L * A.weight;
-            float4* a = A.img.accum + (long)py * W + px;
-            float4 v = *a;
-            v.x = v.x + L.x;
-            v.y = v.y + L.y;
-            v.z = v.z + L.z;
-            v.w = v.w + 0.0f;
-            *a = v;
+            add_caustic(A, pix, hm, caustic, r2);
         }
     }
+#if !RC_EXACT
+    if (A.heavy) {
+        const unsigned int m = __ballot_sync(0xffffffffu, heavy);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned int base = 0;
+            if (lane == leader) base = atomicAdd(A.heavy_len, (unsigned int)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (heavy) A.heavy[base + __popc(m & ((1u << lane) - 1u))] = py * W + px;
+        }
+    }
+#endif
     const unsigned int rsum = __reduce_add_sync(0xffffffffu, rays);
     if (lane == 0 && rsum) atomicAdd(&A.counters->gather_rays, (unsigned long long)rsum);
     flush_work(g, 0u, 0u, A.counters, true);
 }
+
+#if !RC_EXACT
+// The heavy pixels of photon_gather_kernel, one warp per pixel: lanes 0..26
+// look up the 27 cells, then the warp walks each cell's photons 32 (two
+// loads deep, 64) at a time and sums the caustic with a butterfly
+// reduction.  The photons summed are the reference's (the first 512 of
+// each cell's chain); only the order of the float additions differs.
+__global__ void __launch_bounds__(256) photon_gather_heavy(GatherArgs A) {
+    const unsigned int FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned int n = *A.heavy_len;
+    const unsigned int nw = (gridDim.x * blockDim.x) >> 5;
+    const float r = A.radius, r2 = r * r;
+    for (unsigned int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += nw) {
+        const int pix = A.heavy[w];
+        const float4 c = A.hit_cache[pix];
+        const float3 hp = xyz(c);
+        const int hm = __float_as_int(c.w);
+        const int ccx = (int)floorf(hp.x / r), ccy = (int)floorf(hp.y / r), ccz = (int)floorf(hp.z / r);
+        unsigned int s0 = 0u, cnt = 0u;
+        if (lane < 27) {
+            const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+            const int h = cell_hash(ccx + dx, ccy + dy, ccz + dz, A.hash_size);
+            s0 = __ldg(A.cell_start + h);
+            const unsigned int s1 = __ldg(A.cell_start + h + 1);
+            cnt = (s1 - s0) < 512u ? (s1 - s0) : 512u;
+        }
+        float3 caustic = f3(0, 0, 0);
+        for (int k = 0; k < 27; ++k) {
+            const unsigned int b = __shfl_sync(FULL, s0, k);
+            const unsigned int m = __shfl_sync(FULL, cnt, k);
+            for (unsigned int q = lane; q < m; q += 64) {
+                const bool two = q + 32 < m;
+                const float4 p0 = __ldg(A.seg_posw + b + q);
+                const float4 p1 = two ? __ldg(A.seg_posw + b + q + 32) : p0;
+                const float3 d0 = hp - xyz(p0), d1 = hp - xyz(p1);
+                const float e0 = dot(d0, d0), e1 = dot(d1, d1);
+                if (e0 <= r2) {
+                    const float2 yz = __ldg(A.seg_powyz + b + q);
+                    caustic = caustic + f3(p0.w, yz.x, yz.y) * (1.0f - e0 / r2);
+                }
+                if (two && e1 <= r2) {
+                    const float2 yz = __ldg(A.seg_powyz + b + q + 32);
+                    caustic = caustic + f3(p1.w, yz.x, yz.y) * (1.0f - e1 / r2);
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            caustic.x += __shfl_xor_sync(FULL, caustic.x, o);
+            caustic.y += __shfl_xor_sync(FULL, caustic.y, o);
+            caustic.z += __shfl_xor_sync(FULL, caustic.z, o);
+        }
+        if (lane == 0) add_caustic(A, pix, hm, caustic, r2);
+    }
+}
+#endif
 
 // ---------------------------------------------------------------------------
 // photon map: cell-sorted layout
@@ -709,8 +807,9 @@ cudaError_t launch_photon_layout(const PhotonArgs& A, cudaStream_t s) {
     cell_scan_blocks<<<nb, 1024, 0, s>>>(A.cell_count, A.cell_start, A.block_sums, n);
     cell_scan_top<<<1, 1024, 0, s>>>(A.block_sums, nb, A.cell_start, n);
     cell_scan_add<<<(n + 1023) / 1024, 1024, 0, s>>>(A.cell_start, A.block_sums, n);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     photon_scatter<<<sms * 4, 256, 0, s>>>(A, A.counter);
     photon_links<<<sms * 4, 256, 0, s>>>(A, A.counter);
     return cudaGetLastError();
@@ -718,10 +817,24 @@ cudaError_t launch_photon_layout(const PhotonArgs& A, cudaStream_t s) {
 
 cudaError_t launch_photon_gather(const GatherArgs& A, cudaStream_t s) {
     const dim3 grid((A.img.width + 15) / 16, (A.img.height + 7) / 8);
+#if !RC_EXACT
+    if (A.heavy) {
+        const cudaError_t e = cudaMemsetAsync(A.heavy_len, 0, sizeof(unsigned int), s);
+        if (e != cudaSuccess) return e;
+    }
+#endif
     if (A.scene.depth <= 60)
         photon_gather_kernel<true><<<grid, 128, 0, s>>>(A);
     else
         photon_gather_kernel<false><<<grid, 128, 0, s>>>(A);
+#if !RC_EXACT
+    if (A.heavy) {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        photon_gather_heavy<<<sms * 8, 256, 0, s>>>(A);
+    }
+#endif
     return cudaGetLastError();
 }
 

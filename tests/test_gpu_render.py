@@ -400,6 +400,43 @@ def test_gather_with_capped_chains(product, orc, c1):
     assert abs(g.sum() - c.sum()) / c.sum() < 0.02
 
 
+@pytest.mark.parametrize("photons", [100_000, 300_000])
+def test_gather_fast_matches_oracle_on_its_map(product, orc, c1, photons):
+    """Fast build: pixels whose 27 cells hold more than 64 photons are
+    gathered one warp per pixel with lanes striding the photons.  Against
+    the oracle's gather over the product's own photon map (same chains, so
+    the same first 512 photons of a long chain), only the summation order
+    and the fast-math gather hit points differ.  300k photons make chains
+    longer than the 512 cap, so those pixels take the warp-per-pixel path."""
+    w, sc, cam = c1
+    W, H, hs, r0 = 96, 64, 1 << 20, 0.02
+    with _ctx(product, W, H, product.RC_MATH_FAST) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, 1)
+        before = ctx.read_buffers()[0]
+        ctx.sppm_reset(r0)
+        ctx.sppm_trace(photons, hs)
+        ph, heads, nxt, stored = ctx.read_photon_map(photons, hs)
+        ctx.sppm_gather(cam, photons, hs, 1.0)
+        after = ctx.read_buffers()[0]
+    longest = _max_chain(ph, min(stored, photons), r0, hs)
+    assert (longest > 512) == (photons == 300_000), longest
+    cacc = before.copy()
+    orc.photon_gather(sc, cam, W, H, r0, hs, ph, heads, nxt, cacc)
+    g, c = (after - before)[..., :3], (cacc - before)[..., :3]
+    assert np.abs(c).max() > 0
+    close = np.all(np.abs(g - c) <= 1e-3 * np.abs(c) + 1e-5, axis=-1)
+    assert close.mean() > 0.995, close.mean()
+    # the brightest caustic pixels (the densest cells: the warp-per-pixel
+    # path at 300k photons) agree as well as the rest
+    lum = c.sum(axis=-1)
+    bright = lum >= np.quantile(lum[lum > 0], 0.9)
+    assert close[bright].mean() > 0.98, close[bright].mean()
+    # a few gather rays refract differently under fast math (glass walks)
+    assert abs(g.sum() - c.sum()) / c.sum() < 5e-3
+    np.testing.assert_array_equal(after[..., 3], before[..., 3])
+
+
 def test_atrous_exact_bit_identical(product, orc, c1):
     import pyoracle as po
     w, sc, cam = c1
