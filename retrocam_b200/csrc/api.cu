@@ -370,6 +370,7 @@ struct SubsetBvh {
     std::vector<int> orig;
     rc_bvh_node root;
     int node_count = 0;
+    int max_leaf = 0;   // most triangles in one leaf
 };
 
 static bool build_subset(const std::vector<rc_triangle>& in, int scene_tris, SubsetBvh& out) {
@@ -380,8 +381,11 @@ static bool build_subset(const std::vector<rc_triangle>& in, int scene_tris, Sub
     if (n == 0 || rc_build_bvh(in.data(), n, tris.data(), nodes.data(), (int)nodes.size(), &nn) != RC_OK || nn < 1)
         return false;
     out.recs.assign(nn, NodeRec{});
-    for (int i = 0; i < nn; ++i)
+    out.max_leaf = 0;
+    for (int i = 0; i < nn; ++i) {
         if (nodes[i].prim_count <= 0) node_record(nodes.data(), nodes[i], out.recs[i]);
+        if (nodes[i].prim_count > out.max_leaf) out.max_leaf = nodes[i].prim_count;
+    }
     out.isect.resize(3 * (size_t)n);
     out.orig.resize(n);
     for (int i = 0; i < n; ++i) {
@@ -408,6 +412,7 @@ static DeviceScene subset_view(const SubsetBvh& b, const DevBuf& nodes, const De
     }
     S.root_ref = b.root.prim_count > 0 ? b.root.prim_start : 0;
     S.root_count = b.root.prim_count;
+    S.max_leaf = b.max_leaf;
     return S;
 }
 
@@ -956,7 +961,7 @@ static int photon_reserve(rc_ctx* ctx, const rc_sppm_params* p) {
         ctx->hash_cap = p->hash_size;
     }
     CK(ensure(ctx->counter, sizeof(unsigned int)));
-    CK(ensure(ctx->ph_queue_len, sizeof(unsigned int)));
+    CK(ensure(ctx->ph_queue_len, 2 * sizeof(unsigned int)));   // queue length, emission work counter
     return RC_OK;
 }
 
@@ -998,6 +1003,9 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     A.spec_orig = (const int*)ctx->sp_orig.ptr;
     A.queue = (float4*)ctx->ph_queue.ptr;
     A.queue_len = (unsigned int*)ctx->ph_queue_len.ptr;
+    A.work = (unsigned int*)ctx->ph_queue_len.ptr + 1;
+    A.refill_lanes = ctx->refill_lanes;
+    A.leaf_quarters = ctx->leaf_quarters;
     A.counters = ctx->counters;
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
     cudaError_t e = timed_launch(

@@ -133,6 +133,11 @@ struct PhotonArgs {
     // split trace (4 float4 each), and their count
     float4* queue;
     unsigned int* queue_len;
+    // work counter of the refill emission kernel (zero before the trace;
+    // null: one thread per photon) and its schedule (see WaveArgs)
+    unsigned int* work;
+    int refill_lanes;
+    int leaf_quarters;
     float4* photons;        // 3 float4 per photon (std430 record)
     int* heads;
     int* next;

@@ -21,6 +21,7 @@
 // entries than the scene has nodes (impossible for a validated tree) sets
 // RC_GUARD_TRAVERSAL_CAP in the context's error word and stops.
 #include "device_common.cuh"
+#include "dyn_trace.cuh"
 
 namespace rc {
 namespace RC_NS {
@@ -154,10 +155,53 @@ struct PhotonStore {
     float3 pos, power, dir;
 };
 
-// photon_trace.comp:205-251: up to 8 segments; glass reflects or refracts by
-// Fresnel, metal mirrors, the first diffuse hit after a specular bounce is
-// stored.  With `have_first` the first segment's hit is given (already
-// traced and counted by the caller).
+// One hit of a photon's walk (photon_trace.comp:213-248): glass reflects or
+// refracts by Fresnel, metal mirrors (both give the next segment in `ray`
+// and return 0), the first diffuse hit after a specular bounce is stored
+// (returns 1, `out` filled), any other diffuse hit ends the walk (2).
+DI int photon_interact(const DeviceScene& S, const Hit& hit, Ray& ray, float3& power, uint32_t& seed, bool& spec,
+                       PhotonStore& out) {
+    const Surf sf = surface(S, ray, hit);
+    const Mat m = load_mat(S, sf.mat);
+    const float3 rd = ray.d;
+    const float3 n = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
+    if (m.transmission > 0.5f) {
+        const bool entering = dot(rd, sf.normal) < 0.0f;
+        const float eta = entering ? (1.0f / m.ior) : m.ior;
+        const float cosI = fabs_(dot(rd, n));
+        const float F = fresnel_schlick(cosI, m.ior);
+        float3 nd;
+        if (rnd(seed) < F) {
+            nd = reflect(rd, n);
+        } else {
+            float3 refr = refract(rd, n, eta);
+            if (dot(refr, refr) < 0.001f) refr = reflect(rd, n);
+            nd = normalize(refr);
+        }
+        ray = make_ray(sf.pos + nd * 2e-3f, nd);
+        spec = true;
+        return 0;
+    }
+    if (m.metallic > 0.5f) {
+        power = power * m.albedo;
+        const float3 nd = reflect(rd, n);
+        ray = make_ray(sf.pos + n * 2e-3f, nd);
+        spec = true;
+        return 0;
+    }
+    if (spec) {
+        out.store = true;
+        out.pos = sf.pos;
+        out.power = power;
+        out.dir = rd;
+        return 1;
+    }
+    return 2;
+}
+
+// photon_trace.comp:205-251: up to 8 segments (photon_interact per hit).
+// With `have_first` the first segment's hit is given (already traced and
+// counted by the caller).
 template <bool kAtParent>
 DI PhotonStore photon_walk(const PhotonArgs& A, const DeviceScene& S, PhotonState st, bool have_first,
                            const Hit& first, Guard& g, uint32_t& rays) {
@@ -173,41 +217,7 @@ DI PhotonStore photon_walk(const PhotonArgs& A, const DeviceScene& S, PhotonStat
             hit = photon_hit<kAtParent>(S, st.ray, g);
         }
         if (hit.prim < 0) break;
-        const Surf sf = surface(S, st.ray, hit);
-        const Mat m = load_mat(S, sf.mat);
-        const float3 rd = st.ray.d;
-        const float3 n = dot(rd, sf.normal) < 0.0f ? sf.normal : -sf.normal;
-        if (m.transmission > 0.5f) {
-            const bool entering = dot(rd, sf.normal) < 0.0f;
-            const float eta = entering ? (1.0f / m.ior) : m.ior;
-            const float cosI = fabs_(dot(rd, n));
-            const float F = fresnel_schlick(cosI, m.ior);
-            float3 nd;
-            if (rnd(st.seed) < F) {
-                nd = reflect(rd, n);
-            } else {
-                float3 refr = refract(rd, n, eta);
-                if (dot(refr, refr) < 0.001f) refr = reflect(rd, n);
-                nd = normalize(refr);
-            }
-            st.ray = make_ray(sf.pos + nd * 2e-3f, nd);
-            spec = true;
-            continue;
-        }
-        if (m.metallic > 0.5f) {
-            st.power = st.power * m.albedo;
-            const float3 nd = reflect(rd, n);
-            st.ray = make_ray(sf.pos + n * 2e-3f, nd);
-            spec = true;
-            continue;
-        }
-        if (spec) {
-            out.store = true;
-            out.pos = sf.pos;
-            out.power = st.power;
-            out.dir = rd;
-        }
-        break;
+        if (photon_interact(S, hit, st.ray, st.power, st.seed, spec, out) != 0) break;
     }
     return out;
 }
@@ -217,7 +227,7 @@ DI PhotonStore photon_walk(const PhotonArgs& A, const DeviceScene& S, PhotonStat
 // layout (the reference links the photon into its cell here with an
 // atomicExchange on the head; the scan/scatter kernels below build that
 // layout and heads/next from it).  Every lane of the warp calls this.
-DI void store_photons(const PhotonArgs& A, const PhotonStore& s, uint32_t rays, Guard& g) {
+DI void append_photons(const PhotonArgs& A, const PhotonStore& s) {
     const unsigned int mask = __ballot_sync(0xffffffffu, s.store);
     const int lane = threadIdx.x & 31;
     unsigned int base = 0;
@@ -240,6 +250,12 @@ DI void store_photons(const PhotonArgs& A, const PhotonStore& s, uint32_t rays, 
             A.photons[3 * idx + 2] = make_float4(s.dir.x, s.dir.y, s.dir.z, 0.0f);
         }
     }
+}
+
+// append_photons, then the warp's ray and work counters.
+DI void store_photons(const PhotonArgs& A, const PhotonStore& s, uint32_t rays, Guard& g) {
+    append_photons(A, s);
+    const int lane = threadIdx.x & 31;
     const unsigned int rsum = __reduce_add_sync(0xffffffffu, rays);
     if (lane == 0 && rsum) atomicAdd(&A.counters->photon_rays, (unsigned long long)rsum);
     flush_work(g, 0u, 0u, A.counters, true);
@@ -347,6 +363,96 @@ __global__ void __launch_bounds__(256) photon_bounce_kernel(PhotonArgs A) {
         out = photon_walk<kAtParent>(A, A.scene, st, true, h, g, rays);
     }
     store_photons(A, out, rays, g);
+}
+
+// The first phase as a refill kernel (dyn_trace.cuh): a lane emits the next
+// photon (work counter A.work) when its photon is done, walks the specular
+// triangles' tree for the nearest hit, then on a hit the other triangles'
+// tree for any hit before it; photons whose first hit is specular are
+// queued.  The photons, rays and hits are photon_emit_kernel's; one thread
+// per photon ran at 5 of 32 lanes (329 vs 244 us per 2M photons).  The
+// queued walks stay one thread per photon (photon_bounce_kernel): as a
+// refill kernel they were slower (396 vs 310 us), the surface interactions
+// between segments running a few lanes at a time.
+__global__ void __launch_bounds__(128) photon_emit_dyn(PhotonArgs A) {
+    const unsigned int FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const DeviceScene& S = A.scene;
+    const unsigned int total = S.light_count != 0 ? (unsigned int)A.photon_count : 0u;
+    Guard g = {0u, 0u, 0u};
+    uint32_t rays = 0;
+    int2 stk[kDynStack];
+    LaneRay L;
+    L.item = -1;
+    L.top = 0;
+    L.have_node = false;
+    L.leaf.cnt = 0;
+    L.any = false;
+    uint32_t seed = 0u;
+    float3 power = f3(0.0f, 0.0f, 0.0f);
+    Hit hs;
+    hs.t = hs.u = hs.v = 0.0f;
+    hs.prim = -1;
+    bool second = false;   // walking the other triangles for an occluder
+    while (true) {
+        const unsigned int idle = __ballot_sync(FULL, L.item == -1);
+        if (idle) {
+            const int leader = __ffs(idle) - 1;
+            unsigned int base = 0;
+            if (lane == leader) base = atomicAdd(A.work, (unsigned int)__popc(idle));
+            base = __shfl_sync(FULL, base, leader);
+            if (L.item == -1) {
+                const unsigned int i = base + __popc(idle & ((1u << lane) - 1u));
+                L.item = i < total ? (int)i : -2;
+                if (L.item >= 0) {
+                    const PhotonState st = emit_photon(A, S, L.item);
+                    seed = st.seed;
+                    power = st.power;
+                    L.r = st.ray;
+                    second = false;
+                    ++rays;
+                    dyn_start(A.spec, L, 1e30f, false, g);
+                }
+            }
+        }
+        if (__all_sync(FULL, L.item == -2)) break;
+        while (true) {
+            bool busy = L.item >= 0;
+            bool push = false;
+            bool leaf_phase;
+            if (dyn_schedule(L, busy, A.leaf_quarters, leaf_phase) &&
+                dyn_step<false>(step_scene(second, A.spec, A.diff), L, stk, leaf_phase, g)) {
+                if (!second && L.h.prim >= 0) {
+                    hs = L.h;
+                    hs.prim = __ldg(A.spec_orig + hs.prim);
+                    second = true;
+                    dyn_start(A.diff, L, hs.t, true, g);
+                } else {
+                    push = second && L.h.prim < 0;
+                    L.item = -1;
+                    busy = false;
+                }
+            }
+            const unsigned int m = __ballot_sync(FULL, push);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                unsigned int base = 0;
+                if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(m));
+                base = __shfl_sync(FULL, base, leader);
+                if (push) {
+                    float4* q = A.queue + 4 * (size_t)(base + __popc(m & ((1u << lane) - 1u)));
+                    q[0] = make_float4(L.r.o.x, L.r.o.y, L.r.o.z, __uint_as_float(seed));
+                    q[1] = make_float4(L.r.d.x, L.r.d.y, L.r.d.z, power.x);
+                    q[2] = make_float4(power.y, power.z, hs.t, hs.u);
+                    q[3] = make_float4(hs.v, __int_as_float(hs.prim), 0.0f, 0.0f);
+                }
+            }
+            if (__popc(__ballot_sync(FULL, busy)) < A.refill_lanes) break;
+        }
+    }
+    const unsigned int rsum = __reduce_add_sync(FULL, rays);
+    if (lane == 0 && rsum) atomicAdd(&A.counters->photon_rays, (unsigned long long)rsum);
+    flush_work(g, 0u, 0u, A.counters, true);
 }
 #endif
 
@@ -782,6 +888,28 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) 
     const int blocks = (A.photon_count + b - 1) / b;
     if (blocks == 0) return cudaSuccess;
 #if !RC_EXACT
+    if (A.split && A.queue && A.work && A.scene.max_leaf < 0x10000 && A.spec.max_leaf < 0x10000 &&
+        A.diff.max_leaf < 0x10000) {
+        // refill emission: one persistent grid (the stack entries pack a
+        // leaf's triangle count into 16 bits)
+        cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
+        if (e != cudaSuccess) return e;
+        static int grid_emit = 0;
+        if (!grid_emit) {
+            int dev = 0, sms = 148, pe = 1;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, photon_emit_dyn, 128, 0);
+            grid_emit = sms * (pe > 0 ? pe : 1);
+        }
+        photon_emit_dyn<<<grid_emit, 128, 0, s>>>(A);
+        if (A.scene.depth <= 60)
+            photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
+        else
+            photon_bounce_kernel<false><<<blocks, b, 0, s>>>(A);
+        return cudaGetLastError();
+    }
     if (A.split && A.queue) {
         cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
         if (e != cudaSuccess) return e;

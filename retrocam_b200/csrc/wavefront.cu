@@ -22,6 +22,7 @@
 // bit-identical to the oracle.  Kernels are grid-stride loops over device-side
 // queue lengths, launched with a grid that fills the GPU once.
 #include "device_common.cuh"
+#include "dyn_trace.cuh"
 
 namespace rc {
 namespace RC_NS {
@@ -482,40 +483,10 @@ static int grid_for(const void* fn, int block) {
 }
 
 #if !RC_EXACT
-// Persistent trace with dynamic ray fetch (fast build).  Each lane owns one
-// ray at a time and advances it one traversal step per loop iteration: an
-// interior node, parking a reached leaf, or the triangles of a parked leaf
-// (see the leaf phase below).  When fewer than A.refill_lanes lanes are
-// still busy, the idle lanes take the next rays from the work counter (one
-// atomicAdd per warp), so a warp is not held by its slowest ray.  Same rays
-// and results as wf_trace; only the schedule differs.
-
-// Stack entries of the refill trace: the binary walk pushes at most one per
-// level (guarded at 62, as the reference), the 4-wide walk up to three.
-constexpr int kDynStack = 96;
-
-// Pops the next stack entry not culled by the current hit distance.
-DI bool pop_packed(const int2* stk, int& top, float cull, TravNode& n) {
-    while (top > 0) {
-        const int2 e = stk[--top];
-        if (__int_as_float(e.y & (int)0xffff0000) > cull) continue;
-        n.ref = e.x;
-        n.cnt = e.y & 0xffff;
-        return true;
-    }
-    return false;
-}
-
-struct LaneRay {
-    Ray r;
-    Hit h;
-    TravNode node, leaf;
-    bool have_node;
-    bool any;      // shadow ray
-    int item;      // work index, -1 idle, -2 no more work
-    int top;
-};
-
+// Persistent trace with dynamic ray fetch (fast build): the refill state
+// machine of dyn_trace.cuh over the ray queue followed by the shadow queue
+// (one atomicAdd per warp on the work counter per refill).  Same rays and
+// results as wf_trace; only the schedule differs.
 // kWide: interior steps over the 4-wide nodes (scene.nodes4) instead of the
 // binary records.
 template <bool kWide>
@@ -535,9 +506,6 @@ DI void trace_dyn(const WaveArgs& A) {
     const int lane = threadIdx.x & 31;
     Guard g = {0u, 0u, 0u};
     uint32_t closest = 0, shadow = 0;
-    // traversal stack, 8 bytes an entry: (ref, count | entry distance
-    // truncated to its top 16 bits); truncation rounds a positive distance
-    // down, so the pop-time cull `t > hit` never drops a needed entry
     int2 stk[kDynStack];
     LaneRay L;
     L.item = -1;
@@ -545,7 +513,6 @@ DI void trace_dyn(const WaveArgs& A) {
     L.have_node = false;
     L.leaf.cnt = 0;
     L.any = false;
-    int steps = 0;
     while (true) {
         // ---- refill idle lanes ----
         const unsigned int idle = __ballot_sync(FULL, L.item == -1);
@@ -558,30 +525,18 @@ DI void trace_dyn(const WaveArgs& A) {
                 const unsigned int i = base + __popc(idle & ((1u << lane) - 1u));
                 L.item = i < total ? (int)i : -2;
                 if (L.item >= 0) {
-                    float tmax = 1e30f;
                     if ((unsigned int)L.item < nr) {
                         const int p = B.rq[cur][L.item];
                         L.r = make_ray(xyz(B.o[p]), xyz(B.d[p]));
-                        L.any = false;
+                        dyn_start(S, L, 1e30f, false, g);
                         ++closest;
                     } else {
                         const float4* rec = B.srec[prev] + 4 * (L.item - (int)nr);
                         const float4 so = rec[0], sd = rec[1];
                         L.r = make_ray(xyz(so), xyz(sd));
-                        tmax = so.w;
-                        L.any = true;
+                        dyn_start(S, L, so.w, true, g);
                         ++shadow;
                     }
-                    L.h.t = tmax;
-                    L.h.prim = -1;
-                    L.h.u = L.h.v = 0.0f;
-                    L.top = 0;
-                    L.leaf.cnt = 0;
-                    L.node.ref = S.root_ref;
-                    L.node.cnt = S.root_count;
-                    float tmin;
-                    L.have_node = enter_root(S, g, L.r, tmin) && !(tmin > L.h.t);
-                    steps = 0;
                 }
             }
         }
@@ -589,135 +544,24 @@ DI void trace_dyn(const WaveArgs& A) {
         // ---- advance the rays ----
         while (true) {
             bool busy = L.item >= 0;
-            // A lane is blocked when it has a leaf parked and cannot step
-            // on (no node left, or its next node is a leaf too).  Leaves are
-            // tested warp-wide -- every lane with one parked tests it in the
-            // same iteration -- once all busy lanes have one parked or half
-            // of them are blocked; otherwise the unblocked lanes take an
-            // interior step and the blocked ones wait.  Leaf tests and
-            // interior steps never share an iteration.
-            const bool blocked = busy && L.leaf.cnt > 0 && (!L.have_node || L.node.cnt > 0);
-            const unsigned int act = __ballot_sync(FULL, busy);
-            const unsigned int parked = __ballot_sync(FULL, busy && L.leaf.cnt > 0);
-            const unsigned int blk = __ballot_sync(FULL, blocked);
-            const bool leaf_phase = parked == act || 4 * __popc(blk) >= A.leaf_quarters * __popc(act);
-            if (busy && (leaf_phase ? L.leaf.cnt > 0 : !blocked)) {
-                bool done = false;
-                if (leaf_phase) {
-                    for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
-                        float t, u, v;
-                        if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
-                            L.h.t = t;
-                            L.h.u = u;
-                            L.h.v = v;
-                            L.h.prim = i;
-                            if (L.any) {
-                                done = true;
-                                break;
-                            }
-                        }
-                    }
-                    L.leaf.cnt = 0;
-                } else if (L.have_node) {
-                    if (L.node.cnt > 0) {
-                        L.leaf = L.node;
-                        L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
-                    } else if (kWide) {
-                        // 4-wide node: hit children ordered by entry distance,
-                        // the nearest entered, the others pushed far to near
-                        const Node4* n4 = S.nodes4 + L.node.ref;
-                        const float4 lx = __ldg(&n4->lox), hx = __ldg(&n4->hix), ly = __ldg(&n4->loy);
-                        const float4 hy = __ldg(&n4->hiy), lz = __ldg(&n4->loz), hz = __ldg(&n4->hiz);
-                        const int4 cr = __ldg(&n4->ref), cc = __ldg(&n4->cnt);
-                        const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
-                        const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
-                        const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
-                        const int CR[4] = {cr.x, cr.y, cr.z, cr.w}, CC[4] = {cc.x, cc.y, cc.z, cc.w};
-                        float t4[4];
-                        unsigned int key[4];
-#pragma unroll
-                        for (int k = 0; k < 4; ++k) {
-                            const bool hit = CC[k] >= 0 &&
-                                             tslab(g, L.r, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k], t4[k]) &&
-                                             !(t4[k] > L.h.t);
-                            key[k] = hit ? ((__float_as_uint(fmaxf(t4[k], 0.0f)) & ~3u) | (unsigned int)k)
-                                         : 0xffffffffu;
-                        }
-                        cswap(key[0], key[1]);
-                        cswap(key[2], key[3]);
-                        cswap(key[0], key[2]);
-                        cswap(key[1], key[3]);
-                        cswap(key[1], key[2]);
-                        if (key[0] == 0xffffffffu) {
-                            L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
-                        } else {
-#pragma unroll
-                            for (int k = 3; k >= 1; --k) {
-                                if (key[k] != 0xffffffffu) {
-                                    if (L.top < kDynStack) {
-                                        const int s = key[k] & 3u;
-                                        stk[L.top++] = make_int2(CR[s], (CC[s] & 0xffff) |
-                                                                            (__float_as_int(t4[s]) & (int)0xffff0000));
-                                    } else {
-                                        g.flags |= RC_GUARD_TRAVERSAL_CAP;
-                                    }
-                                }
-                            }
-                            const int s0 = key[0] & 3u;
-                            L.node.ref = CR[s0];
-                            L.node.cnt = CC[s0];
-                        }
-                    } else {
-                        const NodeRec* nrec = S.nodes + L.node.ref;
-                        const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
-                        const int4 d = __ldg(&nrec->d);
-                        float tl, tr;
-                        const bool hl = tslab(g, L.r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > L.h.t);
-                        const bool hr = tslab(g, L.r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > L.h.t);
-                        if (hl && hr) {
-                            const bool left_first = tl < tr;
-                            if (L.top < 62) {
-                                const float tf = left_first ? tr : tl;
-                                const int cf = left_first ? d.w : d.y;
-                                stk[L.top++] = make_int2(left_first ? d.z : d.x,
-                                                         (cf & 0xffff) | (__float_as_int(tf) & (int)0xffff0000));
-                            }
-                            L.node.ref = left_first ? d.x : d.z;
-                            L.node.cnt = left_first ? d.y : d.w;
-                        } else if (hl) {
-                            L.node.ref = d.x;
-                            L.node.cnt = d.y;
-                        } else if (hr) {
-                            L.node.ref = d.z;
-                            L.node.cnt = d.w;
-                        } else {
-                            L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
-                        }
-                    }
+            bool leaf_phase;
+            if (dyn_schedule(L, busy, A.leaf_quarters, leaf_phase) && dyn_step<kWide>(S, L, stk, leaf_phase, g)) {
+                const int item = L.item;
+                if ((unsigned int)item < nr) {
+                    const int p = B.rq[cur][item];
+                    B.hit[p] = make_float4(L.h.t, L.h.u, L.h.v, __int_as_float(L.h.prim));
+                } else {
+                    const float4* rec = B.srec[prev] + 4 * (item - (int)nr);
+                    const float4 sd = rec[1], st = rec[2], sl = rec[3];
+                    const int p = __float_as_int(sd.w);
+                    const bool vis = L.h.prim < 0;
+                    const float3 Lc = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
+                    const float3 rr = xyz(B.rad[p]) + xyz(st) * Lc;
+                    B.rad[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
+                    if (__float_as_int(st.w) != 0) B.res[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
                 }
-                if (!L.have_node && L.leaf.cnt == 0) done = true;
-                if (++steps > 4 * S.node_count + 64) {
-                    g.flags |= RC_GUARD_TRAVERSAL_CAP;
-                    done = true;
-                }
-                if (done) {
-                    const int item = L.item;
-                    if ((unsigned int)item < nr) {
-                        const int p = B.rq[cur][item];
-                        B.hit[p] = make_float4(L.h.t, L.h.u, L.h.v, __int_as_float(L.h.prim));
-                    } else {
-                        const float4* rec = B.srec[prev] + 4 * (item - (int)nr);
-                        const float4 sd = rec[1], st = rec[2], sl = rec[3];
-                        const int p = __float_as_int(sd.w);
-                        const bool vis = L.h.prim < 0;
-                        const float3 Lc = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
-                        const float3 rr = xyz(B.rad[p]) + xyz(st) * Lc;
-                        B.rad[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
-                        if (__float_as_int(st.w) != 0) B.res[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
-                    }
-                    L.item = -1;
-                    busy = false;
-                }
+                L.item = -1;
+                busy = false;
             }
             const unsigned int still = __ballot_sync(FULL, busy);
             if (__popc(still) < A.refill_lanes) break;
