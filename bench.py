@@ -8,9 +8,11 @@ of export/RenderPipeline.java:209-239, issued through rc_render_frame.
 
   value  samples/s with the scene resident in HBM (rc_render_frame alone),
          timed with CUDA events on the stream the kernels run on
-  e2e    the same metric through the C ABI with host buffers: per step the
-         scene upload (host -> device, pinned staging) and the read-back of the
-         finished frame (device -> host) are inside the timed region
+  e2e    the same metric through the C ABI with host buffers, as the
+         export path ends: per step the scene upload (host -> device, pinned
+         staging), the frame, the display pass (rc_display: ACES + sRGB to
+         RGBA8, RenderPipeline.applyDisplayPass) and the read-back of that
+         RGBA8 image (device -> host, FrameExporter) are inside the timed region
   roofline  the dominant kernel (render_kernel): algorithmic bytes per launch
          from the kernel's own work counters, divided by its CUDA-event time
   cpu_baseline  the reference's own shaders compiled for the host
@@ -444,15 +446,8 @@ def run_b200(args):
                         "megakernel": api.RC_ENGINE_MEGAKERNEL}[args.engine], args.chunk_paths)
     tuning = ctx.tuning()
 
-    def step(read=False, out=None):
-        if out is None:
-            ctx.render_frame(cam, settings, w.spp, sppm, r0, iters, atrous, read=False)
-        else:
-            api.lib()  # the C ABI with a caller-owned (pinned) host output
-            ctx.check(api.lib().rc_render_frame(ctx.h, api.C.byref(api.camera_struct(cam)),
-                                                api.C.byref(api.rc_settings(*settings)), w.spp,
-                                                api.C.byref(sppm) if sppm is not None else None, r0, iters,
-                                                api.C.byref(atrous), api.C.c_void_p(out)))
+    def step():
+        ctx.render_frame(cam, settings, w.spp, sppm, r0, iters, atrous, read=False)
 
     # ---- device-resident timing ----
     for _ in range(args.warmup):
@@ -485,11 +480,17 @@ def run_b200(args):
     if ctr["error_word"]:
         raise RuntimeError(f"kernel guard raised: {ctr['error_word']:#x}")
 
-    # ---- end to end through the C ABI with host buffers ----
-    out_pinned = torch.empty((w.height, w.width, 4), dtype=torch.float32, pin_memory=True)
-    for _ in range(max(1, args.warmup)):
+    # ---- end to end through the C ABI with host buffers (the export path:
+    # scene upload, frame, display pass, RGBA8 read-back) ----
+    out_pinned = torch.empty((w.height, w.width, 4), dtype=torch.uint8, pin_memory=True)
+
+    def export_step():
         ctx.upload(sc)
-        step(out=out_pinned.data_ptr())
+        step()
+        ctx.check(api.lib().rc_display(ctx.h, 1, 1.0, api.C.c_void_p(out_pinned.data_ptr())))
+
+    for _ in range(max(1, args.warmup)):
+        export_step()
     ctx.reset_counters()
     barrier(dist, device)
     torch.cuda.synchronize()
@@ -497,8 +498,7 @@ def run_b200(args):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        ctx.upload(sc)
-        step(out=out_pinned.data_ptr())
+        export_step()
     e1.record(stream)
     e1.synchronize()
     e_ms = max_over_ranks(e0.elapsed_time(e1), dist, device)
@@ -506,8 +506,9 @@ def run_b200(args):
     e2e = {"value": samples_per_step * world / (e_ms / args.steps / 1e3) / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": ectr["h2d_bytes"] // args.steps,
            "d2h_bytes_per_step": ectr["d2h_bytes"] // args.steps,
-           "includes": "rc_scene_upload (host layout conversion + validation + H2D) and rc_render_frame "
-                       "with the frame read back into pinned host memory"}
+           "includes": "rc_scene_upload (host layout conversion + validation + H2D), rc_render_frame, "
+                       "rc_display (ACES + sRGB to RGBA8) and the RGBA8 frame read back into pinned host "
+                       "memory (the export path's result)"}
 
     # ---- roofline of the dominant kernel ----
     kernel, (k_ms, k_launches) = max(ktimes.items(), key=lambda kv: kv[1][0])

@@ -166,7 +166,8 @@ typedef struct rc_counters {
 #define RC_KERNEL_WF_ACCUMULATE 8  /* wavefront: in-order accumulation, G-buffer */
 #define RC_KERNEL_PHOTON_LAYOUT 9  /* photon map: cell scan, scatter, heads/next */
 #define RC_KERNEL_KPCNN 10         /* learned denoiser: features, 4 convolutions, filter */
-#define RC_KERNEL_KINDS 11
+#define RC_KERNEL_DISPLAY 11       /* ACES + sRGB to RGBA8 (rc_display) */
+#define RC_KERNEL_KINDS 12
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
@@ -496,6 +497,17 @@ int rc_read_buffers(rc_ctx* ctx, float* accum_rgba, uint16_t* gbuffer_rgba16f,
                     uint16_t* albedo_rgba16f, float* variance);
 /* Copies the last denoised/normalised frame (W*H*4 floats). */
 int rc_read_output(rc_ctx* ctx, float* out_rgba);
+/* display.frag:11-41 as the export path runs it (export/RenderPipeline.java:
+ * 244-259, applyDisplayPass into a GL_RGBA8 framebuffer) and the read-back of
+ * export/FrameExporter.java:51-80: the last output (what rc_read_output
+ * returns) divided by max(total_samples, 1) and scaled by exposure -- the
+ * shader's u_totalSamples and u_exposure; the export path passes 1 and 1.0
+ * because the denoiser already normalised -- then the ACES fit and the sRGB
+ * encode, stored as the RGBA8 framebuffer stores a fragment (each channel
+ * round(clamp(v, 0, 1) * 255), NaN as 0, alpha 255), rows top to bottom as
+ * FrameExporter writes them (stbi_flip_vertically_on_write).  out_rgba8:
+ * W*H*4 bytes of host memory, or NULL to keep the image on the device. */
+int rc_display(rc_ctx* ctx, int total_samples, float exposure, uint8_t* out_rgba8);
 /* Copies the photon map of the last trace (any may be NULL): photons
  * (capacity entries), heads (hash_size), next (capacity), counter. */
 int rc_read_photon_map(rc_ctx* ctx, rc_photon* photons, int photon_capacity,

@@ -1,9 +1,9 @@
 """TEST INFRASTRUCTURE (oracle). Builds oracle/_ref/libretrocam_ref.so: the
 reference's own hot-path shaders, compiled on the host.
 
-The five GLSL sources are read where they lie under the reference checkout
+The six GLSL sources are read where they lie under the reference checkout
 (pathtrace.comp, photon_trace.comp, photon_gather.comp,
-post/atrous_denoise.frag, post/p00_normalize.frag), rewritten in memory by the
+post/atrous_denoise.frag, post/p00_normalize.frag, display.frag), rewritten in memory by the
 mechanical transforms below, wrapped in C++ namespaces on top of
 oracle/glsl_compat.h, followed by oracle/ref_dispatch.inc (the dispatch loops
 that stand in for glDispatchCompute / glDrawArrays), and piped to g++ on
@@ -40,6 +40,7 @@ SHADERS = [
     ("phgather", "photon_gather.comp"),
     ("atrous", os.path.join("post", "atrous_denoise.frag")),
     ("p00", os.path.join("post", "p00_normalize.frag")),
+    ("display", "display.frag"),
 ]
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libretrocam_ref.so")

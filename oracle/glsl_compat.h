@@ -138,6 +138,13 @@ inline bool isinf_s(float x) { return (rcx_fbits(x) & 0x7fffffffu) == 0x7f800000
 inline vec3 floor(const vec3& v) { return vec3(floor(v.x), floor(v.y), floor(v.z)); }
 inline vec3 min(const vec3& a, const vec3& b) { return vec3(min(a.x, b.x), min(a.y, b.y), min(a.z, b.z)); }
 inline vec3 max(const vec3& a, const vec3& b) { return vec3(max(a.x, b.x), max(a.y, b.y), max(a.z, b.z)); }
+inline vec3 clamp(const vec3& v, float a, float b) { return vec3(clamp(v.x, a, b), clamp(v.y, a, b), clamp(v.z, a, b)); }
+inline vec3 pow(const vec3& x, const vec3& y) { return vec3(pow(x.x, y.x), pow(x.y, y.y), pow(x.z, y.z)); }
+/* GLSL 4.30 section 8.3: step(edge, x) = x < edge ? 0 : 1; mix(x, y, a) = x * (1 - a) + y * a */
+inline vec3 step(float e, const vec3& x) {
+    return vec3(x.x < e ? 0.0f : 1.0f, x.y < e ? 0.0f : 1.0f, x.z < e ? 0.0f : 1.0f);
+}
+inline vec3 mix(const vec3& x, const vec3& y, const vec3& a) { return x * (vec3(1.0f) - a) + y * a; }
 inline float dot(const vec2& a, const vec2& b) { return a.x * b.x + a.y * b.y; }
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline vec3 cross(const vec3& a, const vec3& b) {

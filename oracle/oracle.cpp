@@ -961,6 +961,41 @@ int or_p00(const float* accum, int W, int H, int total, float exposure, float* o
     return 0;
 }
 
+/* display.frag:11-41 on the export path (export/RenderPipeline.java:244-259)
+ * and the GL_RGBA8 store + FrameExporter read-back (FrameExporter.java:51-80):
+ * ACES fit, sRGB encode by the shader's mix/step, each channel stored as
+ * round(clamp(v, 0, 1) * 255) (NaN as 0), alpha 255, rows written top first
+ * (stbi_flip_vertically_on_write). */
+static inline float aces_fit(float x) {
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    return gclamp((x * (a * x + b)) / (x * (c * x + d) + e), 0.0f, 1.0f);
+}
+static inline float linear_to_srgb(float c) {
+    const float t = c < 0.0031308f ? 0.0f : 1.0f;   /* step(0.0031308, c) */
+    const float lo = 12.92f * c;
+    const float hi = 1.055f * rcx_powf(c, 1.0f / 2.4f) - 0.055f;
+    return lo * (1.0f - t) + hi * t;                /* mix(lo, hi, t) */
+}
+static inline uint8_t unorm8(float v) {
+    if (!(v == v)) v = 0.0f;
+    v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+    return (uint8_t)floor_(v * 255.0f + 0.5f);
+}
+
+int or_display(const float* color, int W, int H, int total, float exposure, uint8_t* out, int nthreads) {
+    const float n = (float)(total > 1 ? total : 1);
+    set_threads(nthreads);
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x) {
+            const float* c = color + 4 * ((long)y * W + x);
+            uint8_t* o = out + 4 * ((long)(H - 1 - y) * W + x);
+            for (int k = 0; k < 3; ++k) o[k] = unorm8(linear_to_srgb(aces_fit(c[k] / n * exposure)));
+            o[3] = 255;
+        }
+    return 0;
+}
+
 /* One à-trous pass. */
 int or_atrous_pass(const float* col, const uint16_t* gbuf, const uint16_t* galb, const float* var, int W,
                    int H, int step, float sc_, float sn, float sd, int N, float exposure, float* out,

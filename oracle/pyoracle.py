@@ -104,6 +104,7 @@ class Oracle:
             "or_p00": (_I, [_VP, _I, _I, _I, _F, _VP, _I]),
             "or_atrous_pass": (_I, [_VP, _VP, _VP, _VP, _I, _I, _I, _F, _F, _F, _I, _F, _VP, _I]),
             "or_denoise": (_I, [_VP, _VP, _VP, _VP, _I, _I, _I, _VP, _VP, _I]),
+            "or_display": (_I, [_VP, _I, _I, _I, _F, _VP, _I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -189,6 +190,12 @@ class Oracle:
         self.lib.or_p00(_p(accum), W, H, total, exposure, _p(out), threads)
         return out
 
+    def display(self, color, W, H, total=1, exposure=1.0, threads=0):
+        """RGBA8 export image (rows top first) of an RGBA32F frame."""
+        out = np.zeros((H, W, 4), np.uint8)
+        self.lib.or_display(_p(np.ascontiguousarray(color, np.float32)), W, H, total, exposure, _p(out), threads)
+        return out
+
     def atrous_pass(self, col, gb, ga, var, W, H, step, sc, sn, sd, N, exposure, threads=0):
         out = np.zeros((H, W, 4), np.float32)
         self.lib.or_atrous_pass(_p(col), _p(gb), _p(ga), _p(var), W, H, step, sc, sn, sd, N, exposure,
@@ -213,6 +220,7 @@ class Reference:
                                           _I, _I, _I]
         lib.ref_p00.argtypes = [_VP, _I, _I, _I, _F, _VP, _I]
         lib.ref_atrous_pass.argtypes = [_VP, _VP, _VP, _VP, _I, _I, _I, _F, _F, _F, _I, _F, _VP, _I, _I, _I]
+        lib.ref_display.argtypes = [_VP, _I, _I, _I, _F, _VP, _I]
 
     def pathtrace(self, scene, cam, settings, W, H, frame, buffers, threads=0, rows=(0, 0)):
         acc, gb, ga, var = buffers
@@ -242,6 +250,11 @@ class Reference:
         self.lib.ref_photon_gather(_p(scene["tris"]), _p(scene["nodes"]), _p(scene["mats"]),
                                    C.byref(camera_struct(cam)), W, H, radius, N, hash_size, frame, _p(ph),
                                    _p(heads), _p(nxt), _p(accum), rows[0], rows[1], threads)
+
+    def display(self, color, W, H, total=1, exposure=1.0, threads=0):
+        out = np.zeros((H, W, 4), np.uint8)
+        self.lib.ref_display(_p(np.ascontiguousarray(color, np.float32)), W, H, total, exposure, _p(out), threads)
+        return out
 
     def atrous_pass(self, col, gb, ga, var, W, H, step, sc, sn, sd, N, exposure, out, rows=(0, 0), threads=0):
         self.lib.ref_atrous_pass(_p(col), _p(gb), _p(ga), _p(var), W, H, step, sc, sn, sd, N, exposure, _p(out),

@@ -98,7 +98,7 @@ class rc_counters(C.Structure):
 
 
 KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",
-                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn")
+                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn", "display")
 RC_ENGINE_MEGAKERNEL = 0
 RC_ENGINE_WAVEFRONT = 1
 RC_ENGINE_WAVEFRONT_STATIC = 2
@@ -143,6 +143,7 @@ _SIGNATURES = {
     "rc_render_frame": (_I, [_VP, _VP, _VP, _I, _VP, _F, _I, _VP, _VP]),
     "rc_read_buffers": (_I, [_VP, _VP, _VP, _VP, _VP]),
     "rc_read_output": (_I, [_VP, _VP]),
+    "rc_display": (_I, [_VP, _I, _F, _VP]),
     "rc_read_photon_map": (_I, [_VP, _VP, _I, _VP, _I, _VP, _VP]),
     "rc_get_counters": (_I, [_VP, _VP]),
     "rc_reset_counters": (_I, [_VP]),
@@ -401,6 +402,17 @@ class Context:
     def read_output(self):
         out = np.zeros((self.height, self.width, 4), np.float32)
         self.check(lib().rc_read_output(self.h, _p(out)))
+        return out
+
+    def display(self, total_samples=1, exposure=1.0, read=True):
+        """RenderPipeline.applyDisplayPass + FrameExporter's read-back: the
+        last output ACES-tonemapped, sRGB-encoded and stored as RGBA8, rows
+        top first (an (H, W, 4) uint8 array; None with read=False)."""
+        if not read:
+            self.check(lib().rc_display(self.h, total_samples, exposure, None))
+            return None
+        out = np.zeros((self.height, self.width, 4), np.uint8)
+        self.check(lib().rc_display(self.h, total_samples, exposure, _p(out)))
         return out
 
     def read_photon_map(self, capacity, hash_size):

@@ -27,6 +27,7 @@ cudaError_t launch_photon_layout(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
+cudaError_t launch_display(const DisplayArgs&, cudaStream_t);
 cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
 cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
@@ -39,6 +40,7 @@ cudaError_t launch_photon_layout(const PhotonArgs&, cudaStream_t);
 cudaError_t launch_photon_gather(const GatherArgs&, cudaStream_t);
 cudaError_t launch_atrous(const AtrousArgs&, cudaStream_t);
 cudaError_t launch_normalize(const NormalizeArgs&, cudaStream_t);
+cudaError_t launch_display(const DisplayArgs&, cudaStream_t);
 cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
 cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
@@ -113,6 +115,7 @@ struct rc_ctx {
     // gather hits per pixel (see GatherArgs::hit_cache); the heavy-pixel
     // list of the fast gather (count, then pixel indices)
     DevBuf gcache, batch_gcache, gheavy;
+    DevBuf disp;   // RGBA8 export image of rc_display
     uint64_t gcache_key = 0;
     bool gcache_valid = false;
     unsigned int scene_gen = 0;
@@ -301,7 +304,7 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
                       &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs, &ctx->sp_nodes,
                       &ctx->sp_isect, &ctx->sp_orig, &ctx->df_nodes, &ctx->df_isect, &ctx->ph_queue,
-                      &ctx->ph_queue_len, &ctx->gcache, &ctx->batch_gcache, &ctx->gheavy})
+                      &ctx->ph_queue_len, &ctx->gcache, &ctx->batch_gcache, &ctx->gheavy, &ctx->disp})
         release(*b);
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -1219,6 +1222,28 @@ int rc_read_output(rc_ctx* ctx, float* out_rgba) {
     const size_t px = (size_t)ctx->width * ctx->height;
     CK(cudaSetDevice(ctx->device));
     CK(copy_d2h(ctx, out_rgba, ctx->result, px * sizeof(float4)));
+    return rc_synchronize(ctx);
+}
+
+int rc_display(rc_ctx* ctx, int total_samples, float exposure, uint8_t* out_rgba8) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    const size_t px = (size_t)ctx->width * ctx->height;
+    CK(cudaSetDevice(ctx->device));
+    CK(ensure(ctx->disp, px * sizeof(uchar4)));
+    DisplayArgs A;
+    A.color = ctx->result;
+    A.out = (uchar4*)ctx->disp.ptr;
+    A.width = ctx->width;
+    A.height = ctx->height;
+    A.total_samples = total_samples;
+    A.exposure = exposure;
+    const bool ex = ctx->math_mode == RC_MATH_EXACT;
+    const cudaError_t e = timed_launch(ctx, RC_KERNEL_DISPLAY, [&] {
+        return ex ? exact::launch_display(A, ctx->stream) : fast::launch_display(A, ctx->stream);
+    });
+    if (e != cudaSuccess) return launch_err(ctx, e, "display");
+    if (!out_rgba8) return RC_OK;
+    CK(copy_d2h(ctx, out_rgba8, ctx->disp.ptr, px * sizeof(uchar4)));
     return rc_synchronize(ctx);
 }
 

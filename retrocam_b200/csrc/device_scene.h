@@ -203,6 +203,16 @@ struct NormalizeArgs {
     float exposure;
 };
 
+// display.frag on the export path (rc_display): RGBA32F in, RGBA8 out with
+// the rows in file order (top first).
+struct DisplayArgs {
+    const float4* color;
+    uchar4* out;
+    int width, height;
+    int total_samples;
+    float exposure;
+};
+
 // Wavefront path state, structure of arrays over the paths of one chunk
 // (path p = tiled pixel j + NPIX * (channel + C * sample)).  Queues hold
 // path indices; counters: qlen[0..1] ray queues, qlen[2..3] shadow queues.

@@ -16,6 +16,7 @@
 //   atrous_kernel         post/atrous_denoise.frag (p00_normalize fused
 //                         into the first pass)
 //   normalize_kernel      post/p00_normalize.frag  (denoiser disabled)
+//   display_kernel        display.frag + the export framebuffer's RGBA8 store
 //
 // Every traversal loop is bounded: a traversal that pops more stack
 // entries than the scene has nodes (impossible for a validated tree) sets
@@ -871,6 +872,42 @@ __global__ void normalize_kernel(NormalizeArgs A) {
     A.out[i] = make_float4(c.x / n * A.exposure, c.y / n * A.exposure, c.z / n * A.exposure, 1.0f);
 }
 
+// display.frag:11-41 (ACES fit, sRGB encode) and the GL_RGBA8 store of the
+// export framebuffer (each channel round(clamp(v, 0, 1) * 255), NaN as 0),
+// one thread per pixel, the row written at H-1-y: the order FrameExporter
+// writes (stbi_flip_vertically_on_write).  Exact math follows the shader's
+// operations in order (mix(x, y, a) = x * (1 - a) + y * a, step(e, x) =
+// x < e ? 0 : 1, GLSL clamp = min(max)).
+DI float aces_fit(float x) {
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    return gclamp((x * (a * x + b)) / (x * (c * x + d) + e), 0.0f, 1.0f);
+}
+
+DI float linear_to_srgb(float c) {
+    const float t = c < 0.0031308f ? 0.0f : 1.0f;
+    const float lo = 12.92f * c;
+    const float hi = 1.055f * powf_(c, 1.0f / 2.4f) - 0.055f;
+    return lo * (1.0f - t) + hi * t;
+}
+
+DI unsigned char unorm8(float v) {
+    if (!(v == v)) v = 0.0f;
+    v = v < 0.0f ? 0.0f : (v > 1.0f ? 1.0f : v);
+    return (unsigned char)floorf(v * 255.0f + 0.5f);
+}
+
+__global__ void __launch_bounds__(256) display_kernel(DisplayArgs A) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= A.width) return;
+    const float n = (float)(A.total_samples > 1 ? A.total_samples : 1);
+    const float4 c = __ldg(A.color + (long)y * A.width + x);
+    const float r = linear_to_srgb(aces_fit(c.x / n * A.exposure));
+    const float g = linear_to_srgb(aces_fit(c.y / n * A.exposure));
+    const float b = linear_to_srgb(aces_fit(c.z / n * A.exposure));
+    A.out[(long)(A.height - 1 - y) * A.width + x] = make_uchar4(unorm8(r), unorm8(g), unorm8(b), 255);
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -974,6 +1011,12 @@ cudaError_t launch_atrous(const AtrousArgs& A, cudaStream_t s) {
 
 cudaError_t launch_normalize(const NormalizeArgs& A, cudaStream_t s) {
     normalize_kernel<<<(A.count + 255) / 256, 256, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_display(const DisplayArgs& A, cudaStream_t s) {
+    const dim3 grid((A.width + 255) / 256, A.height);
+    display_kernel<<<grid, 256, 0, s>>>(A);
     return cudaGetLastError();
 }
 

@@ -437,6 +437,47 @@ def test_gather_fast_matches_oracle_on_its_map(product, orc, c1, photons):
     np.testing.assert_array_equal(after[..., 3], before[..., 3])
 
 
+def test_display_exact_matches_oracle(product, orc, c1):
+    """rc_display (the export path's display pass and RGBA8 read-back):
+    exact math gives the oracle's bytes for the denoised frame, with the
+    export path's uniforms (1 sample, exposure 1) and with others; the image
+    is written rows top first, and a call that keeps the image on the device
+    leaves the next read unchanged."""
+    w, sc, cam = c1
+    W, H = 96, 64
+    p = product.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, 4)
+        out = ctx.denoise(p)
+        img = ctx.display()
+        assert img.shape == (H, W, 4) and img.dtype == np.uint8
+        np.testing.assert_array_equal(img, orc.display(out, W, H, 1, 1.0))
+        assert (img[..., 3] == 255).all() and img[..., :3].std() > 10
+        np.testing.assert_array_equal(ctx.display(4, 1.5), orc.display(out, W, H, 4, 1.5))
+        assert ctx.display(read=False) is None
+        np.testing.assert_array_equal(ctx.display(), img)
+        assert ctx.counters()["error_word"] == 0
+
+
+def test_display_fast_close_and_exported_png(product, orc, c1, tmp_path):
+    """Fast math (approximate divide and pow) stays within one step of the
+    8-bit code; export_frame writes the same bytes as a PNG."""
+    from retrocam_b200 import export
+    w, sc, cam = c1
+    W, H = 96, 64
+    p = product.rc_atrous_params(1, 3, 1.0, 64.0, 1.0, 0, 1.0)
+    with _ctx(product, W, H, product.RC_MATH_FAST) as ctx:
+        ctx.upload(sc)
+        ctx.render(cam, (1, 1.0), 0, 4)
+        out = ctx.denoise(p)
+        img = export.export_frame(ctx, str(tmp_path / "out" / "frame.png"))
+    ref = orc.display(out, W, H, 1, 1.0)
+    d = np.abs(img.astype(np.int32) - ref.astype(np.int32))
+    assert d.max() <= 1 and (d == 0).mean() > 0.99, (d.max(), (d == 0).mean())
+    np.testing.assert_array_equal(export.read_png(str(tmp_path / "out" / "frame.png")), img)
+
+
 def test_atrous_exact_bit_identical(product, orc, c1):
     import pyoracle as po
     w, sc, cam = c1

@@ -101,3 +101,19 @@ def test_atrous_gating(orc, ref, scenes_built):
               po.AtrousParams(1, 9, 1.0, 64.0, 0.15, 0, 1.0),   # iterations clamp to 5
               po.AtrousParams(1, 0, 1.0, 64.0, 0.15, 0, 1.0)):  # and to 1
         assert _eq(orc.denoise(*bufs, 32, 32, 4, p), ref.denoise(*bufs, 32, 32, 4, p))
+
+
+@pytest.mark.parametrize("total,exposure", [(1, 1.0), (16, 1.3), (0, 0.7)])
+def test_display_bit_identical(orc, ref, total, exposure):
+    """display.frag (ACES fit, sRGB encode) and the RGBA8 export store, on
+    log-normal HDR values plus the edges: zero, the sRGB knee 0.0031308 and
+    its neighbour, 1, half-float max, a negative value."""
+    rng = np.random.default_rng(3)
+    W, H = 97, 61
+    c = np.exp(rng.normal(-1.5, 2.0, (H, W, 4))).astype(np.float32)
+    c[0, :8, 0] = [0.0, 1e-6, 0.0031308, 0.0031307, 1.0, 65504.0, -0.5, 3.0]
+    a = orc.display(c, W, H, total, exposure)
+    assert np.array_equal(a, ref.display(c, W, H, total, exposure))
+    assert (a[..., 3] == 255).all()
+    # rows top first: flipping the buffer flips the image
+    assert np.array_equal(a[::-1], orc.display(np.ascontiguousarray(c[::-1]), W, H, total, exposure))
