@@ -437,6 +437,38 @@ def test_gather_fast_matches_oracle_on_its_map(product, orc, c1, photons):
     np.testing.assert_array_equal(after[..., 3], before[..., 3])
 
 
+def test_scene_file_render_matches_oracle(product, orc):
+    """A scene read from a file in the reference's scene format (boxes,
+    rotated boxes, spheres, an emissive box) renders with the oracle's bits
+    under exact math."""
+    import pyoracle as po
+    from retrocam_b200 import scene_json as sj
+    from retrocam_b200 import scenes
+    text = """{"materials": [
+      {"name": "White", "albedo": [0.73, 0.73, 0.73], "roughness": 0.5, "ior": 1.5},
+      {"name": "Lamp", "albedo": [1.0, 0.95, 0.85], "emission": [1.0, 0.95, 0.85], "emissionStrength": 15,
+       "roughness": 0.5, "ior": 1.5},
+      {"name": "Gold", "albedo": [0.95, 0.85, 0.55], "metallic": 1, "roughness": 0.1, "ior": 1.5},
+      {"name": "Glass", "albedo": [1, 1, 1], "roughness": 0, "ior": 1.5, "transmission": 1}],
+     "objects": [
+      {"name": "Floor", "type": "BOX", "px": 0.5, "py": 0, "pz": 0.5, "sx": 1, "sy": 0.02, "sz": 1, "materialIndex": 0},
+      {"name": "Back", "type": "BOX", "px": 0.5, "py": 0.5, "pz": 1.2, "sx": 1, "sy": 1, "sz": 0.02, "materialIndex": 0},
+      {"name": "Light", "type": "BOX", "px": 0.5, "py": 1.1, "pz": 0.5, "sx": 0.2, "sy": 0.02, "sz": 0.2, "materialIndex": 1},
+      {"name": "Block", "type": "BOX", "px": 0.3, "py": 0.25, "pz": 0.6, "sx": 0.15, "sy": 0.25, "sz": 0.15,
+       "ry": 22.5, "materialIndex": 2},
+      {"name": "Ball", "type": "SPHERE", "px": 0.7, "py": 0.2, "pz": 0.4, "sx": 0.2, "stacks": 12, "slices": 20,
+       "materialIndex": 3}]}"""
+    desc = sj.loads(text).to_scene_desc()
+    cam = scenes.camera(scenes.CORNELL_ORBIT, scenes.LensDesc(), orc)
+    W, H = 48, 32
+    cpu, _ = orc.render(scenes.build_scene(desc, orc, po.MAT), cam, (1, 1.0), W, H, 0, 2)
+    with _ctx(product, W, H, product.RC_MATH_EXACT) as ctx:
+        ctx.upload(product.build_scene(desc))
+        ctx.render(cam, (1, 1.0), 0, 2)
+        _same_images(ctx.read_buffers(), cpu)
+        assert ctx.counters()["error_word"] == 0
+
+
 def test_display_exact_matches_oracle(product, orc, c1):
     """rc_display (the export path's display pass and RGBA8 read-back):
     exact math gives the oracle's bytes for the denoised frame, with the
