@@ -508,6 +508,12 @@ int rc_read_output(rc_ctx* ctx, float* out_rgba);
  * FrameExporter writes them (stbi_flip_vertically_on_write).  out_rgba8:
  * W*H*4 bytes of host memory, or NULL to keep the image on the device. */
 int rc_display(rc_ctx* ctx, int total_samples, float exposure, uint8_t* out_rgba8);
+/* rc_display on frame `frame` (0-based) of the last rc_render_frames batch,
+ * whose finished frames stay on the device: the export loop displays and
+ * writes every frame it renders (RenderPipeline.tickVideoFrame,
+ * export/RenderPipeline.java:150-185).  RC_ERR_INVALID_ARG outside the
+ * batch. */
+int rc_display_frame(rc_ctx* ctx, int frame, int total_samples, float exposure, uint8_t* out_rgba8);
 /* Copies the photon map of the last trace (any may be NULL): photons
  * (capacity entries), heads (hash_size), next (capacity), counter. */
 int rc_read_photon_map(rc_ctx* ctx, rc_photon* photons, int photon_capacity,

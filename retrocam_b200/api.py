@@ -144,6 +144,7 @@ _SIGNATURES = {
     "rc_read_buffers": (_I, [_VP, _VP, _VP, _VP, _VP]),
     "rc_read_output": (_I, [_VP, _VP]),
     "rc_display": (_I, [_VP, _I, _F, _VP]),
+    "rc_display_frame": (_I, [_VP, _I, _I, _F, _VP]),
     "rc_read_photon_map": (_I, [_VP, _VP, _I, _VP, _I, _VP, _VP]),
     "rc_get_counters": (_I, [_VP, _VP]),
     "rc_reset_counters": (_I, [_VP]),
@@ -413,6 +414,12 @@ class Context:
             return None
         out = np.zeros((self.height, self.width, 4), np.uint8)
         self.check(lib().rc_display(self.h, total_samples, exposure, _p(out)))
+        return out
+
+    def display_frame(self, frame, total_samples=1, exposure=1.0):
+        """display() on frame `frame` of the last render_frames batch."""
+        out = np.zeros((self.height, self.width, 4), np.uint8)
+        self.check(lib().rc_display_frame(self.h, frame, total_samples, exposure, _p(out)))
         return out
 
     def read_photon_map(self, capacity, hash_size):

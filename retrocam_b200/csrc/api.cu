@@ -116,6 +116,7 @@ struct rc_ctx {
     // list of the fast gather (count, then pixel indices)
     DevBuf gcache, batch_gcache, gheavy;
     DevBuf disp;   // RGBA8 export image of rc_display
+    int batch_frames = 0;   // frames of the last rc_render_frames kept in `frames`
     uint64_t gcache_key = 0;
     bool gcache_valid = false;
     unsigned int scene_gen = 0;
@@ -1225,13 +1226,12 @@ int rc_read_output(rc_ctx* ctx, float* out_rgba) {
     return rc_synchronize(ctx);
 }
 
-int rc_display(rc_ctx* ctx, int total_samples, float exposure, uint8_t* out_rgba8) {
-    if (!ctx) return RC_ERR_INVALID_ARG;
+static int display_from(rc_ctx* ctx, const float4* color, int total_samples, float exposure, uint8_t* out_rgba8) {
     const size_t px = (size_t)ctx->width * ctx->height;
     CK(cudaSetDevice(ctx->device));
     CK(ensure(ctx->disp, px * sizeof(uchar4)));
     DisplayArgs A;
-    A.color = ctx->result;
+    A.color = color;
     A.out = (uchar4*)ctx->disp.ptr;
     A.width = ctx->width;
     A.height = ctx->height;
@@ -1245,6 +1245,19 @@ int rc_display(rc_ctx* ctx, int total_samples, float exposure, uint8_t* out_rgba
     if (!out_rgba8) return RC_OK;
     CK(copy_d2h(ctx, out_rgba8, ctx->disp.ptr, px * sizeof(uchar4)));
     return rc_synchronize(ctx);
+}
+
+int rc_display(rc_ctx* ctx, int total_samples, float exposure, uint8_t* out_rgba8) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    return display_from(ctx, ctx->result, total_samples, exposure, out_rgba8);
+}
+
+int rc_display_frame(rc_ctx* ctx, int frame, int total_samples, float exposure, uint8_t* out_rgba8) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (frame < 0 || frame >= ctx->batch_frames)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_display_frame: frame %d of a batch of %d", frame, ctx->batch_frames);
+    const size_t px = (size_t)ctx->width * ctx->height;
+    return display_from(ctx, (const float4*)ctx->frames.ptr + (size_t)frame * px, total_samples, exposure, out_rgba8);
 }
 
 int rc_read_photon_map(rc_ctx* ctx, rc_photon* photons, int photon_capacity, int32_t* heads, int hash_size,
@@ -1512,6 +1525,7 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
         if (r != RC_OK) return r;
     }
     CK(ensure(ctx->frames, (size_t)n_frames * px * sizeof(float4)));
+    ctx->batch_frames = n_frames;   // rc_display_frame's range (valid once this call succeeds)
     CK(cudaStreamSynchronize(ctx->stream));
     // ---- the sequence ----
     if (any_sppm) CK(ensure(ctx->gcache, px * sizeof(float4)));
