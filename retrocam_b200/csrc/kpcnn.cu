@@ -72,15 +72,16 @@ struct ConvArgs {
     unsigned int* err;
 };
 
-// Shared memory of the persistent convolution: three row buffers (the tile
-// being multiplied, the tile whose rows are in flight, and the one the
-// previous MMAs just released), the weights, and one mbarrier per TMEM
-// accumulator.
-constexpr int kRowBufs = 3;
+// Shared memory of the convolution: a ring of five staged image rows (the
+// three of the tile being multiplied, the one in flight for the next tile,
+// and the one the previous tile's MMAs may still read), the weights, and
+// one mbarrier per TMEM accumulator.  A slot is one row of kHalo pixels,
+// channel-group-major: [CIN/8][kPStride][16 B].
+constexpr int kSlots = 5;
 
 template <int CIN>
 struct ConvSmem {
-    alignas(128) uint4 rows[kRowBufs][3 * (CIN / 8) * kPStride];
+    alignas(128) uint4 rows[kSlots][(CIN / 8) * kPStride];
     alignas(128) uint4 wts[9 * (CIN / 8) * kCo];
     uint64_t mbar[2];
     uint32_t tmem;
@@ -96,36 +97,35 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Rows y-1..y+1, pixels x0-1 .. x0+128 of tile t into `rows` (zeros outside
+// Image row y (pixels x0-1 .. x0+128) of image n into a slot (zeros outside
 // the image), as asynchronous copies; the caller commits the group.
 template <int CIN>
-__device__ __forceinline__ void stage_rows(const ConvArgs& A, uint4* rows, int t, int tiles_x) {
+__device__ __forceinline__ void stage_row(const ConvArgs& A, uint4* slot, int n, int y, int x0) {
     constexpr int G = CIN / 8;
-    const int xt = t % tiles_x, rest = t / tiles_x;
-    const int y = rest % A.h, n = rest / A.h;
-    const int x0 = xt * kTile;
-    const uint32_t base = tc::smem_u32(rows);
-    for (int i = threadIdx.x; i < 3 * kHalo * G; i += 128) {
-        const int r = i / (kHalo * G), rem = i - r * kHalo * G;
-        const int p = rem / G, g = rem - p * G;
-        const int yy = y + r - 1, xx = x0 + p - 1;
-        const bool in = yy >= 0 && yy < A.h && xx >= 0 && xx < A.w;
-        const uint4* src = in ? reinterpret_cast<const uint4*>(A.in + (((size_t)n * A.h + yy) * A.w + xx) * CIN) + g
+    const uint32_t base = tc::smem_u32(slot);
+    const bool row_in = y >= 0 && y < A.h;
+    for (int i = threadIdx.x; i < kHalo * G; i += 128) {
+        const int p = i / G, g = i - p * G;
+        const int xx = x0 + p - 1;
+        const bool in = row_in && xx >= 0 && xx < A.w;
+        const uint4* src = in ? reinterpret_cast<const uint4*>(A.in + (((size_t)n * A.h + y) * A.w + xx) * CIN) + g
                               : reinterpret_cast<const uint4*>(A.in);
-        cp_async16(base + ((r * G + g) * kPStride + p) * 16, src, in ? 16u : 0u);
+        cp_async16(base + (g * kPStride + p) * 16, src, in ? 16u : 0u);
     }
 }
 
+// The 9 taps x CIN/16 k-steps of one tile: rows[dy] is the slot of image row
+// y - 1 + dy; the A operand of tap (dy, dx) is that slot shifted by dx pixels.
 template <int CIN>
-__device__ __forceinline__ void issue_tile(uint32_t rows, uint32_t wts, uint32_t tmem_d, uint64_t* mbar) {
-    constexpr int G = CIN / 8;
+__device__ __forceinline__ void issue_tile(const uint32_t (&rows)[3], uint32_t wts, uint32_t tmem_d, uint64_t* mbar) {
+    constexpr int G = CIN / 8;   // 16-byte channel groups per pixel (two per k-step)
     constexpr uint32_t idesc = tc::idesc_bf16(128, kCo, false, false);
 #pragma unroll 1
     for (int tap = 0; tap < 9; ++tap) {
         const int dy = tap / 3, dx = tap - 3 * dy;
 #pragma unroll
         for (int ks = 0; ks < CIN / 16; ++ks) {
-            const uint64_t a = tc::smem_desc(rows + ((dy * G + 2 * ks) * kPStride + dx) * 16, kPStride * 16, 128);
+            const uint64_t a = tc::smem_desc(rows[dy] + ((2 * ks) * kPStride + dx) * 16, kPStride * 16, 128);
             const uint64_t b = tc::smem_desc(wts + (tap * G + 2 * ks) * kCo * 16, kCo * 16, 128);
             tc::mma_bf16(tmem_d, a, b, idesc, (tap | ks) != 0);
         }
@@ -184,29 +184,36 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&v
     }
 }
 
-// Persistent implicit-GEMM convolution: each CTA keeps the weights in shared
-// memory and walks tiles t_k = blockIdx.x + k * gridDim.x.  Step k copies
-// the rows of t_{k+1} asynchronously into a free buffer, issues the MMAs of
-// t_k (rows landed in step k-1) into one TMEM accumulator, and meanwhile runs
-// the epilogue of t_{k-1} from the other, so row copies, tensor-core work and
-// epilogues of three consecutive tiles overlap.
+// Implicit-GEMM convolution over column strips: CTA s takes a segment of
+// `seg_rows` consecutive image rows of one 128-pixel-wide strip, so the
+// tiles it walks share rows -- tile y needs rows y-1..y+1 and only row y+1 is
+// new.  Step k copies row y_k + 2 (the next tile's new row) asynchronously
+// into the ring slot that tile k-2 last read (its MMAs finished: the
+// epilogue of step k-1 waited for them), issues the MMAs of tile k into one
+// TMEM accumulator, and runs the epilogue of tile k-1 from the other, so row
+// copies, tensor-core work and epilogues of consecutive tiles overlap.
 template <int CIN>
-__global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
+__global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) {
     extern __shared__ __align__(128) unsigned char conv_smem_raw[];
     ConvSmem<CIN>& S = *reinterpret_cast<ConvSmem<CIN>*>(conv_smem_raw);
     constexpr int G = CIN / 8;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int tiles_x = (A.w + kTile - 1) / kTile;
-    const int ntiles = tiles_x * A.h * A.n;
-    const int stride = gridDim.x;
+    const int segs = (A.h + seg_rows - 1) / seg_rows;       // segments per strip
+    const int strip = blockIdx.x / segs;                    // (image, column) strip
+    const int n = strip / tiles_x, xt = strip - n * tiles_x;
+    const int y0 = (blockIdx.x - strip * segs) * seg_rows;
+    const int rows_here = min(seg_rows, A.h - y0);
+    if (n >= A.n || rows_here <= 0) return;
+    const int x0 = xt * kTile;
     if (warp == 0) tc::tmem_alloc(&S.tmem, 64);
     if (tid == 0) {
         tc::mbar_init(&S.mbar[0], 1);
         tc::mbar_init(&S.mbar[1], 1);
     }
     for (int i = tid; i < 9 * G * kCo; i += 128) S.wts[i] = __ldg(reinterpret_cast<const uint4*>(A.wpk) + i);
-    const int t0 = blockIdx.x;
-    if (t0 < ntiles) stage_rows<CIN>(A, S.rows[0], t0, tiles_x);
+    // image row y0 - 1 + j lives in slot j % kSlots
+    for (int j = 0; j < 3; ++j) stage_row<CIN>(A, S.rows[j], n, y0 - 1 + j, x0);
     cp_async_commit();
     tc::fence_before_sync();
     __syncthreads();
@@ -216,22 +223,24 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
     uint32_t phase[2] = {0u, 0u};
     bool ok = true;
     int k = 0;
-    for (int t = t0; t < ntiles && ok; t += stride, ++k) {
+    for (; k < rows_here && ok; ++k) {
         const int acc = k & 1;
-        // rows of t_{k+1}: its buffer was last read by the MMAs of t_{k-2},
-        // whose completion the epilogue of step k-1 waited for
-        const int tn = t + stride;
-        if (tn < ntiles) stage_rows<CIN>(A, S.rows[(k + 1) % kRowBufs], tn, tiles_x);
+        const int y = y0 + k;
+        if (k + 1 < rows_here) stage_row<CIN>(A, S.rows[(k + 3) % kSlots], n, y + 2, x0);
         cp_async_commit();
-        // rows of t_k landed (all but the group just committed)
+        // rows of tile k landed (all but the group just committed)
         cp_async_wait<1>();
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
-        if (tid == 0) issue_tile<CIN>(tc::smem_u32(S.rows[k % kRowBufs]), wts, tmem + acc * 32, &S.mbar[acc]);
+        if (tid == 0) {
+            const uint32_t rows[3] = {tc::smem_u32(S.rows[k % kSlots]), tc::smem_u32(S.rows[(k + 1) % kSlots]),
+                                      tc::smem_u32(S.rows[(k + 2) % kSlots])};
+            issue_tile<CIN>(rows, wts, tmem + acc * 32, &S.mbar[acc]);
+        }
         if (k > 0) {
-            // epilogue of t_{k-1} while the tensor cores work on t_k
+            // epilogue of tile k-1 while the tensor cores work on tile k
             const int pa = acc ^ 1;
             ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
             phase[pa] ^= 1u;
@@ -239,7 +248,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
             if (ok) {
                 float v[32];
                 tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
-                conv_epilogue(A, v, t - stride, tiles_x);
+                conv_epilogue(A, v, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x);
             }
             tc::fence_before_sync();
         }
@@ -252,7 +261,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A) {
         if (ok) {
             float v[32];
             tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
-            conv_epilogue(A, v, t0 + (k - 1) * stride, tiles_x);
+            conv_epilogue(A, v, ((n * A.h) + y0 + k - 1) * tiles_x + xt, tiles_x);
         }
     }
     cp_async_wait<0>();
@@ -605,18 +614,23 @@ static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
             e = cudaFuncSetAttribute(conv3x3_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
-        // shared memory bounds the CTAs per SM (registers allow 7 of 128
-        // threads); TMEM allows 8 of 64 columns; 4 keeps both with room
+        // shared memory bounds the CTAs per SM (3 with 32 input channels);
+        // registers allow 7 of 128 threads and TMEM 8 of 64 columns
         int smem_sm = 0;
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
         per = (int)(smem_sm / (smem + 1024));   // 1 KB reserved per CTA
         if (per < 1) per = 1;
-        if (per > 4) per = 4;
+        if (per > 7) per = 7;
     }
-    const int ntiles = ((A.w + kTile - 1) / kTile) * A.h * A.n;
-    const int grid = ntiles < sms * per ? ntiles : sms * per;
-    if (grid <= 0) return cudaSuccess;
-    conv3x3_kernel<CIN><<<grid, 128, smem, s>>>(A);
+    // one segment per resident CTA: rows per segment so that the strips'
+    // segments fill the GPU once
+    const int strips = ((A.w + kTile - 1) / kTile) * A.n;
+    const int cap = sms * per;
+    if (strips <= 0 || A.h <= 0) return cudaSuccess;
+    int seg_rows = (int)(((long)strips * A.h + cap - 1) / cap);
+    if (seg_rows < 1) seg_rows = 1;
+    const int grid = strips * ((A.h + seg_rows - 1) / seg_rows);
+    conv3x3_kernel<CIN><<<grid, 128, smem, s>>>(A, seg_rows);
     return cudaGetLastError();
 }
 
