@@ -1173,7 +1173,7 @@ int rc_denoise_learned(rc_ctx* ctx, const rc_kpcnn* weights, float* out_rgba) {
                                      ctx->kp_act1.ptr, (float*)ctx->kp_logits.ptr, (float4*)ctx->kp_color.ptr,
                                      ctx->out, ctx->width, ctx->height, &ctx->counters->error_word, ctx->stream);
         },
-        7);
+        6);
     if (e != cudaSuccess) return launch_err(ctx, e, "kpcnn");
     ctx->result = ctx->out;
     if (out_rgba) return rc_read_output(ctx, out_rgba);

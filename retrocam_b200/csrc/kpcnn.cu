@@ -70,7 +70,40 @@ struct ConvArgs {
     int relu;
     int out_f32;
     unsigned int* err;
+    // inference head fused into the epilogue (head_kernel without a
+    // target): the 32 outputs are the logits, head_out gets the filtered
+    // head_color and `out` is not written; null: plain convolution
+    const float4* head_color;
+    float4* head_out;
 };
+
+// The network's head: softmax of 25 logits (in place: the normalised
+// weights) and the 5x5 filter of the noisy colour of image `img` with them,
+// edges clamped.
+__device__ __forceinline__ float3 apply_head(float (&l)[25], const float4* __restrict__ img, int y, int x, int h,
+                                             int w) {
+    float m = l[0];
+#pragma unroll
+    for (int t = 1; t < 25; ++t) m = fmaxf(m, l[t]);
+    float s = 0.0f;
+#pragma unroll
+    for (int t = 0; t < 25; ++t) {
+        l[t] = __expf(l[t] - m);
+        s += l[t];
+    }
+    const float inv = 1.0f / s;
+    float3 o = make_float3(0.0f, 0.0f, 0.0f);
+#pragma unroll
+    for (int t = 0; t < 25; ++t) {
+        l[t] *= inv;
+        const int yy = min(max(y + t / 5 - 2, 0), h - 1), xx = min(max(x + t % 5 - 2, 0), w - 1);
+        const float4 c = __ldg(img + (size_t)yy * w + xx);
+        o.x += l[t] * c.x;
+        o.y += l[t] * c.y;
+        o.z += l[t] * c.z;
+    }
+    return o;
+}
 
 // Shared memory of the convolution: a ring of five staged image rows (the
 // three of the tile being multiplied, the one in flight for the next tile,
@@ -164,6 +197,14 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&v
                 if (!(__bfloat162float(h2.y) > 0.0f)) v[q * 8 + 2 * j + 1] = 0.0f;
             }
         }
+    }
+    if (A.head_color) {
+        float l[25];
+#pragma unroll
+        for (int t = 0; t < 25; ++t) l[t] = v[t];
+        const float3 o = apply_head(l, A.head_color + (size_t)n * A.h * A.w, y, x, A.h, A.w);
+        A.head_out[pix] = make_float4(o.x, o.y, o.z, 1.0f);
+        return;
     }
     if (A.out_f32) {
         float4* o = reinterpret_cast<float4*>(static_cast<float*>(A.out) + pix * 32);
@@ -438,27 +479,8 @@ __global__ void __launch_bounds__(128) head_kernel(HeadArgs A) {
             l[4 * q + 3] = v.w;
         }
         l[24] = lg[6].x;
-        float m = l[0];
-#pragma unroll
-        for (int t = 1; t < 25; ++t) m = fmaxf(m, l[t]);
-        float s = 0.0f;
-#pragma unroll
-        for (int t = 0; t < 25; ++t) {
-            l[t] = __expf(l[t] - m);
-            s += l[t];
-        }
-        const float inv = 1.0f / s;
-        float3 o = make_float3(0.0f, 0.0f, 0.0f);
         const size_t img = (size_t)n * A.h * A.w;
-#pragma unroll
-        for (int t = 0; t < 25; ++t) {
-            l[t] *= inv;
-            const int yy = min(max(y + t / 5 - 2, 0), A.h - 1), xx = min(max(x + t % 5 - 2, 0), A.w - 1);
-            const float4 c = __ldg(A.color + img + (size_t)yy * A.w + xx);
-            o.x += l[t] * c.x;
-            o.y += l[t] * c.y;
-            o.z += l[t] * c.z;
-        }
+        const float3 o = apply_head(l, A.color + img, y, x, A.h, A.w);
         A.out[pix] = make_float4(o.x, o.y, o.z, 1.0f);
         if (A.target) {
             const float4 r = __ldg(A.target + pix);
@@ -698,8 +720,9 @@ cudaError_t run_inference(const float* params, void* packed, const float4* accum
     if (e == cudaSuccess) e = launch_conv({f, w[0], params + kParamB1, a0, nullptr, 1, H, W, 1, 0, err}, 16, s);
     if (e == cudaSuccess) e = launch_conv({a0, w[1], params + kParamB2, a1, nullptr, 1, H, W, 1, 0, err}, 32, s);
     if (e == cudaSuccess) e = launch_conv({a1, w[2], params + kParamB3, a0, nullptr, 1, H, W, 1, 0, err}, 32, s);
-    if (e == cudaSuccess) e = launch_conv({a0, w[3], params + kParamBH, logits, nullptr, 1, H, W, 0, 1, err}, 32, s);
-    if (e == cudaSuccess) e = launch_head({logits, color, nullptr, out, nullptr, nullptr, 0.0f, 1, H, W}, s);
+    // the last convolution applies the head in its epilogue (no logits in HBM)
+    if (e == cudaSuccess)
+        e = launch_conv({a0, w[3], params + kParamBH, logits, nullptr, 1, H, W, 0, 1, err, color, out}, 32, s);
     return e;
 }
 
@@ -719,7 +742,7 @@ int rc_kp_conv3x3(const void* in, int cin, const void* wpk, const float* bias, v
     if (!in || !wpk || !out || !err || (cin != 16 && cin != 32) || n <= 0 || h <= 0 || w <= 0)
         return RC_ERR_INVALID_ARG;
     ConvArgs A{static_cast<const __nv_bfloat16*>(in), static_cast<const __nv_bfloat16*>(wpk), bias, out,
-               static_cast<const __nv_bfloat16*>(mask), n, h, w, relu, out_f32, err};
+               static_cast<const __nv_bfloat16*>(mask), n, h, w, relu, out_f32, err, nullptr, nullptr};
     return launch_conv(A, cin, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
 }
 

@@ -11,6 +11,8 @@ import ctypes as C
 import numpy as np
 import pytest
 
+from conftest import bits
+
 pytestmark = pytest.mark.gpu
 
 
@@ -229,6 +231,40 @@ def test_denoise_learned_matches_torch_network(product, T):
     close = np.abs(got - ref) <= 2e-2 * np.abs(ref) + 1e-3
     assert np.mean(np.all(close, axis=-1)) > 0.995
     assert abs(got.mean() - ref.mean()) <= 1e-3 * abs(ref.mean())
+
+
+def test_fused_head_equals_separate_head(product, T):
+    """Inference applies the head in the last convolution's epilogue; the
+    same four convolutions with the logits written out and the separate
+    head kernel (the training path) give the same bits."""
+    import ctypes as C
+    from retrocam_b200 import kpcnn, scenes
+    H, W = 96, 200
+    w = scenes.cornell_variant(4, W, H)
+    params = kpcnn.init_params(2)
+    params[kpcnn.WH:kpcnn.BH] *= 30.0
+    with product.Context(W, H, 0, product.RC_MATH_FAST) as ctx:
+        ctx.upload(product.build_scene(w.scene))
+        ctx.render(product.workload_camera(w), (1, 1.0), 0, 2)
+        feat = T.zeros(1, H, W, 16, dtype=T.bfloat16, device="cuda")
+        color = T.zeros(1, H, W, 4, device="cuda")
+        ctx.kp_features(feat.data_ptr(), color.data_ptr())
+        fused = ctx.denoise_learned(params)
+        ctx.synchronize()
+    stream = T.cuda.current_stream()
+    net = kpcnn.Network(params, T.device("cuda", 0), stream)
+    bf = T.bfloat16
+    a1, a2, a3 = (T.zeros(1, H, W, 32, dtype=bf, device="cuda") for _ in range(3))
+    logits = T.zeros(1, H, W, 32, device="cuda")
+    out = T.zeros(1, H, W, 4, device="cuda")
+    net.conv(feat, 16, 0, a1, relu=True, n=1, h=H, w=W)
+    net.conv(a1, 32, 1, a2, relu=True, n=1, h=H, w=W)
+    net.conv(a2, 32, 2, a3, relu=True, n=1, h=H, w=W)
+    net.conv(a3, 32, 3, logits, relu=False, out_f32=True, n=1, h=H, w=W)
+    assert product.lib().rc_kp_head(_p(logits), _p(color), None, _p(out), None, None, C.c_float(0.0), 1, H, W,
+                                    C.c_void_p(stream.cuda_stream)) == 0
+    net.check()
+    np.testing.assert_array_equal(bits(fused), bits(out[0].cpu().numpy()))
 
 
 def test_features_layout(product, T):
