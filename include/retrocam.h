@@ -167,7 +167,8 @@ typedef struct rc_counters {
 #define RC_KERNEL_PHOTON_LAYOUT 9  /* photon map: cell scan, scatter, heads/next */
 #define RC_KERNEL_KPCNN 10         /* learned denoiser: features, 4 convolutions, filter */
 #define RC_KERNEL_DISPLAY 11       /* ACES + sRGB to RGBA8 (rc_display) */
-#define RC_KERNEL_KINDS 12
+#define RC_KERNEL_VHS 12           /* the VHS chain's passes (rc_post_vhs) */
+#define RC_KERNEL_KINDS 13
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
@@ -497,6 +498,53 @@ int rc_read_buffers(rc_ctx* ctx, float* accum_rgba, uint16_t* gbuffer_rgba16f,
                     uint16_t* albedo_rgba16f, float* variance);
 /* Copies the last denoised/normalised frame (W*H*4 floats). */
 int rc_read_output(rc_ctx* ctx, float* out_rgba);
+/* ---------------------------------------------------------------------------
+ * The VHS chain (post/PostProcessStack.java:149-277, shaders post/p01..p16)
+ * ------------------------------------------------------------------------- */
+
+/* The chain's knobs, as core/RenderSettings.java names them (defaults
+ * there, :49-191; rc_vhs_defaults fills them with every pass off), and the
+ * per-frame values it reads: RenderSettings.frameIndex and TemporalState's
+ * time (s) and AGC gain. */
+typedef struct rc_vhs_params {
+    int32_t enabled;                 /* bit k-1 enables pass pk (p01..p16; p05, p06 have no shader) */
+    int32_t frame_index;
+    float time_s;
+    float agc_gain;
+    float luma_blur_sigma;           /* p01 */
+    float chroma_res_sigma;          /* p02 */
+    float color_temp_bias, color_hue_rot, color_saturation, color_drift_speed;      /* p03 */
+    float dr_black_lift, dr_shadow_crush, dr_highlight_knee, dr_highlight_clip;     /* p04 */
+    float ccd_noise_luma_base, ccd_noise_chroma_scale;                            /* p07 */
+    float ccd_smear_threshold, ccd_smear_intensity;                               /* p08 */
+    int32_t ccd_smear_length;
+    float chroma_bleed_factor;                                                    /* p09 */
+    float timebase_amplitude_px, timebase_freq, timebase_speed;                   /* p10 */
+    float dot_crawl_intensity, dot_crawl_subcarrier, dot_crawl_edge_thresh;       /* p11 */
+    float tape_age, dropout_bright, dropout_burst_rate;                           /* p12 */
+    int32_t head_switch_lines;                                                    /* p13 */
+    float head_switch_jitter, head_switch_ripple, head_switch_chroma;
+    float tracking_severity, tracking_max_displace_px, tracking_fringe_width_px;  /* p14 */
+    float edge_enhance_amount, edge_enhance_core_threshold;                       /* p15 */
+    float interlace_field_offset_px, interlace_comb_strength, interlace_comb_edge_thresh,
+        interlace_line_weighting;                                                 /* p16 */
+} rc_vhs_params;
+
+#define RC_VHS_PASS(k) (1 << ((k) - 1))
+
+/* RenderSettings' defaults, every pass disabled. */
+void rc_vhs_defaults(rc_vhs_params* p);
+/* PostProcessStack.runChain's passes p01..p16 (those enabled, in order) on
+ * the last output (what rc_read_output returns, e.g. rc_denoise_atrous'
+ * p00 + a-trous result), ping-ponging between RGBA32F images as the
+ * reference's PingPongBuffer does; the result becomes the last output (for
+ * rc_read_output and rc_display). */
+int rc_post_vhs(rc_ctx* ctx, const rc_vhs_params* p);
+/* One pass (1..16 except 5, 6) on device RGBA32F images of w x h, on
+ * `stream` (NULL: the default stream); in and out must not overlap. */
+int rc_vhs_pass(int pass, const void* in_rgba, void* out_rgba, int w, int h, const rc_vhs_params* p,
+                void* stream);
+
 /* display.frag:11-41 as the export path runs it (export/RenderPipeline.java:
  * 244-259, applyDisplayPass into a GL_RGBA8 framebuffer) and the read-back of
  * export/FrameExporter.java:51-80: the last output (what rc_read_output

@@ -1,9 +1,10 @@
 """TEST INFRASTRUCTURE (oracle). Builds oracle/_ref/libretrocam_ref.so: the
 reference's own hot-path shaders, compiled on the host.
 
-The six GLSL sources are read where they lie under the reference checkout
+The GLSL sources are read where they lie under the reference checkout
 (pathtrace.comp, photon_trace.comp, photon_gather.comp,
-post/atrous_denoise.frag, post/p00_normalize.frag, display.frag), rewritten in memory by the
+post/atrous_denoise.frag, post/p00_normalize.frag, display.frag and the
+fourteen VHS passes post/p01..p16), rewritten in memory by the
 mechanical transforms below, wrapped in C++ namespaces on top of
 oracle/glsl_compat.h, followed by oracle/ref_dispatch.inc (the dispatch loops
 that stand in for glDispatchCompute / glDrawArrays), and piped to g++ on
@@ -20,7 +21,8 @@ Transforms (each keeps the meaning of the GLSL statement):
   * `T[N](a, b, ...)` array constructors -> `{a, b, ...}`
   * vector constructors with two or more `rand(` calls -> brace init, so the
     calls run left to right as GLSL 4.30 section 6.1.1 requires
-  * swizzles `.rgb/.xyz` -> `.xyz()`, `.xy` -> `.xy()`, `.r/.g/.b` -> `.x/.y/.z`
+  * swizzles `.rgb/.xyz` -> `.xyz()`, `.xy` -> `.xy()`, `.yz` -> `.yz()` (and
+    `v.yz = e;` -> `v.set_yz(e);`), `.r/.g/.b` -> `.x/.y/.z`
   * floating literals get an `f` suffix (GLSL literals are single precision)
 """
 from __future__ import annotations
@@ -41,7 +43,10 @@ SHADERS = [
     ("atrous", os.path.join("post", "atrous_denoise.frag")),
     ("p00", os.path.join("post", "p00_normalize.frag")),
     ("display", "display.frag"),
-]
+] + [(name.split("_")[0], os.path.join("post", name + ".frag")) for name in (
+    "p01_downsample", "p02_chroma_res", "p03_color_matrix", "p04_dynamic_range", "p07_ccd_noise",
+    "p08_ccd_smear", "p09_chroma_bleed", "p10_timebase", "p11_dot_crawl", "p12_dropout", "p13_headswitch",
+    "p14_tracking", "p15_edge_enhance", "p16_interlace")]
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libretrocam_ref.so")
 
@@ -93,6 +98,8 @@ def transform(src: str) -> str:
     # vecN(rand(..), rand(..)) -> vecN{...}
     s = _replace_ctor_parens(s, r"\b(?:vec[234])\s*\(",
                              lambda m, inner: inner.count("rand(") >= 2)
+    s = re.sub(r"(\w+)\.yz\s*=\s*([^;]+);", r"\1.set_yz(\2);", s)   # swizzle write
+    s = re.sub(r"\.yz\b(?!\()", ".yz()", s)
     s = re.sub(r"\.(?:rgb|xyz)\b", ".xyz()", s)
     s = re.sub(r"\.xy\b", ".xy()", s)
     s = re.sub(r"\.r\b", ".x", s)
@@ -109,7 +116,8 @@ def translation_unit(ref_root: str) -> str:
         path = os.path.join(ref_root, SHADER_DIR, rel)
         with open(path, "r", encoding="utf-8") as f:
             body = transform(f.read())
-        prologue = "thread_local uvec3 gl_GlobalInvocationID;\n" if rel.endswith(".comp") else ""
+        prologue = ("thread_local uvec3 gl_GlobalInvocationID;\n" if rel.endswith(".comp")
+                    else "thread_local vec4 gl_FragCoord;\n")
         parts.append(f"namespace glsl {{ namespace {ns} {{\n{prologue}#line 1 \"{rel}\"\n{body}\n}} }}")
     with open(os.path.join(HERE, "ref_dispatch.inc"), "r", encoding="utf-8") as f:
         parts.append('#line 1 "ref_dispatch.inc"\n' + f.read())

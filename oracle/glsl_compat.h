@@ -47,6 +47,7 @@ struct ivec2 {
     ivec2() : x(0), y(0) {}
     ivec2(int a, int b) : x(a), y(b) {}
     explicit ivec2(const uvec2& u);
+    explicit ivec2(const struct vec2& v);
 };
 struct uvec2 {
     uint x, y;
@@ -63,12 +64,16 @@ struct vec2 {
     template <class A, class B> vec2(A a, B b) : x((float)a), y((float)b) {}
     explicit vec2(const ivec2& v) : x((float)v.x), y((float)v.y) {}
 };
+inline ivec2::ivec2(const vec2& v) : x((int)v.x), y((int)v.y) {}
 struct vec3 {
     float x, y, z;
     vec3() : x(0), y(0), z(0) {}
     explicit vec3(float s) : x(s), y(s), z(s) {}
     template <class A, class B, class C> vec3(A a, B b, C c) : x((float)a), y((float)b), z((float)c) {}
+    vec3(float a, const vec2& b) : x(a), y(b.x), z(b.y) {}
     vec2 xy() const { return vec2(x, y); }
+    vec2 yz() const { return vec2(y, z); }
+    void set_yz(const vec2& v) { y = v.x; z = v.y; }   /* the .yz = ... swizzle write */
     vec3 xyz() const { return *this; }
 };
 struct vec4 {
@@ -108,6 +113,8 @@ RCG_BIN(/)
 #undef RCG_BIN
 inline vec2& operator+=(vec2& a, const vec2& b) { a = a + b; return a; }
 inline vec3& operator+=(vec3& a, const vec3& b) { a = a + b; return a; }
+inline vec2& operator*=(vec2& a, float s) { a = a * s; return a; }
+inline vec2& operator/=(vec2& a, float s) { a = a / s; return a; }
 inline vec3& operator*=(vec3& a, const vec3& b) { a = a * b; return a; }
 inline vec3& operator*=(vec3& a, float s) { a = a * s; return a; }
 inline vec3& operator/=(vec3& a, float s) { a = a / s; return a; }
@@ -131,6 +138,19 @@ inline float max(float x, float y) { return (x < y) ? y : x; }
 inline int min(int x, int y) { return (y < x) ? y : x; }
 inline int max(int x, int y) { return (x < y) ? y : x; }
 inline float clamp(float x, float a, float b) { return min(max(x, a), b); }
+inline int clamp(int x, int a, int b) { return min(max(x, a), b); }
+/* GLSL 4.30 section 8.3; round() ties away from zero (the spec leaves the
+ * direction to the implementation) */
+inline float fract(float x) { return x - floor(x); }
+inline float round(float x) { return __builtin_roundf(x); }
+inline float sign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+inline float radians(float d) { return d * 0.017453292519943295f; }
+inline float step(float e, float x) { return x < e ? 0.0f : 1.0f; }
+inline float mix(float x, float y, float a) { return x * (1.0f - a) + y * a; }
+inline float smoothstep(float e0, float e1, float x) {
+    const float t = clamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
 inline bool isnan_s(float x) { return (rcx_fbits(x) & 0x7fffffffu) > 0x7f800000u; }
 inline bool isinf_s(float x) { return (rcx_fbits(x) & 0x7fffffffu) == 0x7f800000u; }
 
@@ -145,6 +165,8 @@ inline vec3 step(float e, const vec3& x) {
     return vec3(x.x < e ? 0.0f : 1.0f, x.y < e ? 0.0f : 1.0f, x.z < e ? 0.0f : 1.0f);
 }
 inline vec3 mix(const vec3& x, const vec3& y, const vec3& a) { return x * (vec3(1.0f) - a) + y * a; }
+inline vec3 mix(const vec3& x, const vec3& y, float a) { return x * (1.0f - a) + y * a; }
+inline vec2 clamp(const vec2& v, const vec2& a, const vec2& b) { return vec2(clamp(v.x, a.x, b.x), clamp(v.y, a.y, b.y)); }
 inline float dot(const vec2& a, const vec2& b) { return a.x * b.x + a.y * b.y; }
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline vec3 cross(const vec3& a, const vec3& b) {
@@ -213,6 +235,7 @@ inline int wrap_index(int i, int n, int wrap) {
     int m = i % n;
     return m < 0 ? m + n : m;
 }
+inline ivec2 textureSize(const sampler2D& s, int) { return ivec2(s.img.w, s.img.h); }
 inline vec4 texel(const sampler2D& s, int ix, int iy) {
     return imageLoad(s.img, ivec2(wrap_index(ix, s.img.w, s.wrap), wrap_index(iy, s.img.h, s.wrap)));
 }

@@ -221,6 +221,7 @@ class Reference:
         lib.ref_p00.argtypes = [_VP, _I, _I, _I, _F, _VP, _I]
         lib.ref_atrous_pass.argtypes = [_VP, _VP, _VP, _VP, _I, _I, _I, _F, _F, _F, _I, _F, _VP, _I, _I, _I]
         lib.ref_display.argtypes = [_VP, _I, _I, _I, _F, _VP, _I]
+        lib.ref_post_pass.argtypes = [_I, _VP, _I, _I, _VP, _VP, _I]
 
     def pathtrace(self, scene, cam, settings, W, H, frame, buffers, threads=0, rows=(0, 0)):
         acc, gb, ga, var = buffers
@@ -250,6 +251,15 @@ class Reference:
         self.lib.ref_photon_gather(_p(scene["tris"]), _p(scene["nodes"]), _p(scene["mats"]),
                                    C.byref(camera_struct(cam)), W, H, radius, N, hash_size, frame, _p(ph),
                                    _p(heads), _p(nxt), _p(accum), rows[0], rows[1], threads)
+
+    def post_pass(self, pass_, color, W, H, params, threads=0):
+        """One VHS pass of the reference's own shader (params: the product's
+        rc_vhs_params ctypes struct, the same layout)."""
+        out = np.zeros((H, W, 4), np.float32)
+        r = self.lib.ref_post_pass(pass_, _p(np.ascontiguousarray(color, np.float32)), W, H, C.byref(params),
+                                   _p(out), threads)
+        assert r == 0, pass_
+        return out
 
     def display(self, color, W, H, total=1, exposure=1.0, threads=0):
         out = np.zeros((H, W, 4), np.uint8)

@@ -79,6 +79,44 @@ class rc_atrous_params(C.Structure):
                 ("exposure", C.c_float)]
 
 
+_VHS_FIELDS = [("enabled", "i"), ("frame_index", "i"), ("time_s", "f"), ("agc_gain", "f"),
+               ("luma_blur_sigma", "f"), ("chroma_res_sigma", "f"),
+               ("color_temp_bias", "f"), ("color_hue_rot", "f"), ("color_saturation", "f"),
+               ("color_drift_speed", "f"), ("dr_black_lift", "f"), ("dr_shadow_crush", "f"),
+               ("dr_highlight_knee", "f"), ("dr_highlight_clip", "f"), ("ccd_noise_luma_base", "f"),
+               ("ccd_noise_chroma_scale", "f"), ("ccd_smear_threshold", "f"), ("ccd_smear_intensity", "f"),
+               ("ccd_smear_length", "i"), ("chroma_bleed_factor", "f"), ("timebase_amplitude_px", "f"),
+               ("timebase_freq", "f"), ("timebase_speed", "f"), ("dot_crawl_intensity", "f"),
+               ("dot_crawl_subcarrier", "f"), ("dot_crawl_edge_thresh", "f"), ("tape_age", "f"),
+               ("dropout_bright", "f"), ("dropout_burst_rate", "f"), ("head_switch_lines", "i"),
+               ("head_switch_jitter", "f"), ("head_switch_ripple", "f"), ("head_switch_chroma", "f"),
+               ("tracking_severity", "f"), ("tracking_max_displace_px", "f"), ("tracking_fringe_width_px", "f"),
+               ("edge_enhance_amount", "f"), ("edge_enhance_core_threshold", "f"),
+               ("interlace_field_offset_px", "f"), ("interlace_comb_strength", "f"),
+               ("interlace_comb_edge_thresh", "f"), ("interlace_line_weighting", "f")]
+
+
+class rc_vhs_params(C.Structure):
+    """The VHS chain's knobs (include/retrocam.h rc_vhs_params)."""
+    _fields_ = [(n, C.c_int32 if t == "i" else C.c_float) for n, t in _VHS_FIELDS]
+
+
+VHS_PASSES = (1, 2, 3, 4, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16)
+
+
+def vhs_defaults(**overrides) -> rc_vhs_params:
+    """RenderSettings' defaults (every pass off), with overrides by field name;
+    `passes=(1, 3, ...)` sets the enabled mask."""
+    p = rc_vhs_params()
+    lib().rc_vhs_defaults(C.byref(p))
+    for k, v in overrides.items():
+        if k == "passes":
+            p.enabled = sum(1 << (i - 1) for i in v)
+        else:
+            setattr(p, k, v)
+    return p
+
+
 class rc_tuning(C.Structure):
     _fields_ = [("engine", C.c_int32), ("chunk_paths", C.c_int32), ("wide_bvh", C.c_int32),
                 ("trace_block", C.c_int32), ("shade_block", C.c_int32), ("photon_block", C.c_int32),
@@ -98,7 +136,7 @@ class rc_counters(C.Structure):
 
 
 KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",
-                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn", "display")
+                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn", "display", "vhs")
 RC_ENGINE_MEGAKERNEL = 0
 RC_ENGINE_WAVEFRONT = 1
 RC_ENGINE_WAVEFRONT_STATIC = 2
@@ -145,6 +183,9 @@ _SIGNATURES = {
     "rc_read_output": (_I, [_VP, _VP]),
     "rc_display": (_I, [_VP, _I, _F, _VP]),
     "rc_display_frame": (_I, [_VP, _I, _I, _F, _VP]),
+    "rc_vhs_defaults": (None, [_VP]),
+    "rc_post_vhs": (_I, [_VP, _VP]),
+    "rc_vhs_pass": (_I, [_I, _VP, _VP, _I, _I, _VP, _VP]),
     "rc_read_photon_map": (_I, [_VP, _VP, _I, _VP, _I, _VP, _VP]),
     "rc_get_counters": (_I, [_VP, _VP]),
     "rc_reset_counters": (_I, [_VP]),
@@ -415,6 +456,12 @@ class Context:
         out = np.zeros((self.height, self.width, 4), np.uint8)
         self.check(lib().rc_display(self.h, total_samples, exposure, _p(out)))
         return out
+
+    def post_vhs(self, params: rc_vhs_params, read=False):
+        """rc_post_vhs: the enabled VHS passes on the last output (which they
+        replace); returns it when `read`."""
+        self.check(lib().rc_post_vhs(self.h, C.byref(params)))
+        return self.read_output() if read else None
 
     def display_frame(self, frame, total_samples=1, exposure=1.0):
         """display() on frame `frame` of the last render_frames batch."""

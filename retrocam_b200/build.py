@@ -6,6 +6,7 @@
                   contraction, the approximate divide within 2 ulp)
   api.cu          C ABI, device half
   noalloc.cu      allocation-free à-trous entry point
+  post_vhs.cu     the VHS chain (exact-math flags in both modes)
   kpcnn.cu        learned denoiser (tcgen05 BF16 convolutions)
   host_scene.cpp  C ABI, host half (-ffp-contract=off: Java float rules)
 
@@ -75,6 +76,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
             o = os.path.join(BUILD, name + ".o")
             _run(common + ["-c", os.path.join(CSRC, name + ".cu"), "-o", o], log)
             objs.append(o)
+        # the VHS chain: exact arithmetic in every math mode
+        o = os.path.join(BUILD, "post_vhs.o")
+        _run(common + ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false", "-c",
+                       os.path.join(CSRC, "post_vhs.cu"), "-o", o], log)
+        objs.append(o)
         o = os.path.join(BUILD, "host_scene.o")
         _run(["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall"] + inc +
              ["-c", os.path.join(CSRC, "host_scene.cpp"), "-o", o], log)

@@ -46,6 +46,11 @@ cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace fast
+namespace vhs {
+bool has_pass(int pass);
+cudaError_t launch_pass(int pass, const float4* in, float4* out, int w, int h, const rc_vhs_params& p,
+                        cudaStream_t s);
+}  // namespace vhs
 namespace kp {
 cudaError_t launch_features(const float4* accum, const ushort4* gbuf, const ushort4* galb, __nv_bfloat16* feat,
                             float4* color, int count, cudaStream_t s);
@@ -1224,6 +1229,24 @@ int rc_read_output(rc_ctx* ctx, float* out_rgba) {
     CK(cudaSetDevice(ctx->device));
     CK(copy_d2h(ctx, out_rgba, ctx->result, px * sizeof(float4)));
     return rc_synchronize(ctx);
+}
+
+int rc_post_vhs(rc_ctx* ctx, const rc_vhs_params* p) {
+    if (!ctx || !p) return RC_ERR_INVALID_ARG;
+    CK(cudaSetDevice(ctx->device));
+    // PingPongBuffer: each pass reads the previous result and writes the other image
+    const float4* src = ctx->result;
+    for (int k = 1; k <= 16; ++k) {
+        if (!(p->enabled & RC_VHS_PASS(k)) || !vhs::has_pass(k)) continue;
+        float4* dst = (src == ctx->ping) ? ctx->pong : ctx->ping;
+        const cudaError_t e = timed_launch(ctx, RC_KERNEL_VHS, [&] {
+            return vhs::launch_pass(k, src, dst, ctx->width, ctx->height, *p, ctx->stream);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "vhs pass");
+        src = dst;
+    }
+    ctx->result = const_cast<float4*>(src);
+    return RC_OK;
 }
 
 static int display_from(rc_ctx* ctx, const float4* color, int total_samples, float exposure, uint8_t* out_rgba8) {

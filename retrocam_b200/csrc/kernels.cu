@@ -492,7 +492,9 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
     const int W = A.img.width, H = A.img.height;
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0, hits = 0;
+#if !RC_EXACT
     bool heavy = false;
+#endif
     if (px < W && py < H) {
         const DeviceScene& S = A.scene;
         const CamParams& cam = A.cam;

@@ -19,9 +19,13 @@ per batch of up to `batch_frames` frames) and each is displayed with
 math: the same bits without SPPM, and up to the photon-hash insertion order
 with it).
 
+With `vhs`, each frame runs the VHS chain (rc_post_vhs) between the
+denoiser and the display pass, as PostProcessStack.runChain does.
+
 Not built: MP4/MOV encoding through ffmpeg (RenderFormat.VIDEO_*), JPEG
-files, the free camera, and TemporalState's autofocus hunting (the lens
-focuses at exactly lens.focusDist) -- all outside the render path.
+files, the free camera, and TemporalState's autofocus hunting and AGC
+dynamics (the lens focuses at exactly lens.focusDist; the AGC gain is the
+value given) -- all outside the render path.
 """
 from __future__ import annotations
 
@@ -220,12 +224,31 @@ def plan(job: RenderJob, orbit: Orbit, lens: Lens, scene: SceneFile):
     return out
 
 
+def vhs_for_frame(vhs, frame: int, time_s: float, lens: Lens):
+    """The chain's per-frame knobs: frame index (the caller's start plus the
+    frame), TemporalState.time (the canonical frame time) and the keyframed
+    post settings (saturation, colour temperature, tape age)."""
+    import ctypes as C
+    p = api.rc_vhs_params()
+    C.memmove(C.byref(p), C.byref(vhs), C.sizeof(p))
+    p.frame_index = vhs.frame_index + frame
+    p.time_s = time_s
+    p.color_saturation = lens.saturation
+    p.color_temp_bias = lens.color_temp
+    p.tape_age = lens.tape_age
+    return p
+
+
 def run_job(ctx, job: RenderJob, scene: SceneFile, orbit: Orbit | None = None, lens: Lens | None = None,
             settings=(1, 1.0), sppm: scenes.SppmDesc | None = scenes.SppmDesc(), r0: float = 0.02,
-            atrous: scenes.AtrousDesc = scenes.AtrousDesc(), batched: bool = True, batch_frames: int = 32):
+            atrous: scenes.AtrousDesc = scenes.AtrousDesc(), batched: bool = True, batch_frames: int = 32,
+            vhs=None):
     """Renders the job through the context and writes its PNG files;
     returns their paths.  SPPM (when given and the scene has lights) runs one
-    photon pass per sample, as accumulateFrame does."""
+    photon pass per sample, as accumulateFrame does.  `vhs` (an
+    api.rc_vhs_params with passes enabled) runs the VHS chain on each
+    denoised frame before the display pass, as PostProcessStack.runChain
+    does (frame by frame; its AGC gain stays the value given)."""
     orbit = orbit or Orbit()
     lens = lens or Lens()
     frames = plan(job, orbit, lens, scene)
@@ -244,7 +267,9 @@ def run_job(ctx, job: RenderJob, scene: SceneFile, orbit: Orbit | None = None, l
     sp = api.rc_sppm_params(sppm.photons, sppm.hash_size, sppm.alpha) if sppm and sc["light_count"] > 0 else None
     iters = spp if sp is not None else 0
     tl = job.timeline
-    can_batch = batched and not (tl and (tl.has_scene_object_tracks() or tl.has_track("post.exposure")))
+    use_vhs = vhs is not None and vhs.enabled != 0
+    can_batch = batched and not use_vhs and not (tl and (tl.has_scene_object_tracks() or
+                                                          tl.has_track("post.exposure")))
     if can_batch:
         ap = api.atrous_params(replace(atrous, exposure=lens.exposure if not tl else frames[0][2].exposure))
         for b0 in range(0, len(frames), batch_frames):
@@ -256,11 +281,13 @@ def run_job(ctx, job: RenderJob, scene: SceneFile, orbit: Orbit | None = None, l
                 export.write_png(path, ctx.display_frame(i))
                 paths.append(path)
         return paths
-    for f, (_, o, ln, sf) in enumerate(frames):
+    for f, (t, o, ln, sf) in enumerate(frames):
         if sf is not uploaded:
             upload(sf)
         ap = api.atrous_params(replace(atrous, exposure=ln.exposure))
         ctx.render_frame(camera_of(o, ln), settings, spp, sp, r0, iters, ap, read=False)
+        if use_vhs:
+            ctx.post_vhs(vhs_for_frame(vhs, f, t, ln))
         path = job.frame_path(f)
         export.write_png(path, ctx.display())
         paths.append(path)

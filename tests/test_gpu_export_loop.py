@@ -78,3 +78,23 @@ def test_scene_object_track_moves_the_object(product, tmp_path):
                          product.atrous_params(scenes.AtrousDesc()), read=False)
         np.testing.assert_array_equal(first, ctx.display())
     assert not np.array_equal(first, export.read_png(paths[-1]))
+
+
+def test_vhs_chain_in_the_loop(product, ref, orc, tmp_path):
+    """With the VHS chain, each frame is render -> denoise -> chain (frame
+    index and time of that frame) -> display; frame 1 equals the chain of the
+    reference's pass shaders on that frame's denoised image."""
+    vhs = product.vhs_defaults(passes=(3, 7, 10, 16), frame_index=100, agc_gain=2.0)
+    job = el.RenderJob(str(tmp_path / "v" / "clip"), True, 2, duration_s=0.125, fps=24.0)
+    with product.Context(W, H, 0, product.RC_MATH_EXACT) as ctx:
+        paths = el.run_job(ctx, job, _scene(), sppm=None, vhs=vhs)
+        ctx.render_frame(el.camera_of(el.Orbit(), el.Lens()), (1, 1.0), 2, None, 0.02, 0,
+                         product.atrous_params(scenes.AtrousDesc()), read=False)
+        den = ctx.read_output()
+    p = el.vhs_for_frame(vhs, 1, job.frame_time(1), el.Lens())
+    assert (p.frame_index, p.time_s) == (101, job.frame_time(1))
+    want = den
+    for k in (3, 7, 10, 16):
+        want = ref.post_pass(k, want, W, H, p)
+    np.testing.assert_array_equal(export.read_png(paths[1]), orc.display(want, W, H, 1, 1.0))
+    assert not np.array_equal(export.read_png(paths[0]), export.read_png(paths[1]))   # the noise moved
