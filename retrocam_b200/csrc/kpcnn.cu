@@ -106,11 +106,13 @@ __device__ __forceinline__ float3 apply_head(float (&l)[25], const float4* __res
 }
 
 // Shared memory of the convolution: a ring of five staged image rows (the
-// three of the tile being multiplied, the one in flight for the next tile,
-// and the one the previous tile's MMAs may still read), the weights, and
+// three of the tile being multiplied and the new rows of the next two tiles,
+// in flight; the previous tile's first row gives its slot up once that
+// tile's MMAs are done), the weights, and
 // one mbarrier per TMEM accumulator.  A slot is one row of kHalo pixels,
 // channel-group-major: [CIN/8][kPStride][16 B].
-constexpr int kSlots = 5;
+constexpr int kAhead = 2;             // row copies in flight ahead of the tile
+constexpr int kSlots = 3 + kAhead;
 
 template <int CIN>
 struct ConvSmem {
@@ -228,10 +230,10 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&v
 // Implicit-GEMM convolution over column strips: CTA s takes a segment of
 // `seg_rows` consecutive image rows of one 128-pixel-wide strip, so the
 // tiles it walks share rows -- tile y needs rows y-1..y+1 and only row y+1 is
-// new.  Step k copies row y_k + 2 (the next tile's new row) asynchronously
-// into the ring slot that tile k-2 last read (its MMAs finished: the
-// epilogue of step k-1 waited for them), issues the MMAs of tile k into one
-// TMEM accumulator, and runs the epilogue of tile k-1 from the other, so row
+// new.  Step k issues the MMAs of tile k into one TMEM accumulator, waits for
+// tile k-1's MMAs, copies row y_k + 3 (the new row of tile k+2) asynchronously
+// into the ring slot tile k-1 read first, and runs the epilogue of tile k-1
+// from the other accumulator; a row copy has two steps to land, and row
 // copies, tensor-core work and epilogues of consecutive tiles overlap.
 template <int CIN>
 __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) {
@@ -252,10 +254,16 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
         tc::mbar_init(&S.mbar[0], 1);
         tc::mbar_init(&S.mbar[1], 1);
     }
-    for (int i = tid; i < 9 * G * kCo; i += 128) S.wts[i] = __ldg(reinterpret_cast<const uint4*>(A.wpk) + i);
-    // image row y0 - 1 + j lives in slot j % kSlots
+    for (int i = tid; i < 9 * G * kCo; i += 128)
+        cp_async16(tc::smem_u32(&S.wts[i]), reinterpret_cast<const uint4*>(A.wpk) + i, 16u);
+    // image row y0 - 1 + j lives in slot j % kSlots; group 0 = the weights and
+    // the rows of tile 0, group a = the new row of tile a (a < kAhead)
     for (int j = 0; j < 3; ++j) stage_row<CIN>(A, S.rows[j], n, y0 - 1 + j, x0);
     cp_async_commit();
+    for (int a = 1; a < kAhead; ++a) {
+        if (a < rows_here) stage_row<CIN>(A, S.rows[2 + a], n, y0 + 1 + a, x0);
+        cp_async_commit();
+    }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
@@ -267,10 +275,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
     for (; k < rows_here && ok; ++k) {
         const int acc = k & 1;
         const int y = y0 + k;
-        if (k + 1 < rows_here) stage_row<CIN>(A, S.rows[(k + 3) % kSlots], n, y + 2, x0);
-        cp_async_commit();
-        // rows of tile k landed (all but the group just committed)
-        cp_async_wait<1>();
+        // rows of tile k landed (all groups but the newest kAhead - 1)
+        cp_async_wait<kAhead - 1>();
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
@@ -280,12 +286,20 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
                                       tc::smem_u32(S.rows[(k + 2) % kSlots])};
             issue_tile<CIN>(rows, wts, tmem + acc * 32, &S.mbar[acc]);
         }
-        if (k > 0) {
+        if (k == 0) {
+            if (kAhead < rows_here) stage_row<CIN>(A, S.rows[2 + kAhead], n, y + 1 + kAhead, x0);
+            cp_async_commit();
+        } else {
             // epilogue of tile k-1 while the tensor cores work on tile k
             const int pa = acc ^ 1;
             ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
             phase[pa] ^= 1u;
             tc::fence_after_sync();
+            // tile k-1's MMAs are done with its first row: that slot takes
+            // the new row of tile k + kAhead
+            if (ok && k + kAhead < rows_here)
+                stage_row<CIN>(A, S.rows[(k + 2 + kAhead) % kSlots], n, y + 1 + kAhead, x0);
+            cp_async_commit();
             if (ok) {
                 float v[32];
                 tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);

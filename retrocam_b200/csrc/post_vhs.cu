@@ -134,14 +134,34 @@ struct Frag {
 // ---------------------------------------------------------------------------
 // the passes: each returns fragColor.rgb (alpha is 1 for every pass)
 // ---------------------------------------------------------------------------
+// Tap weights that depend only on the tap and the uniforms (the Gaussians
+// of p01/p02, the 0.70^i decay of p08): one block computes each once, by
+// the shader's own expression, into shared memory.
+constexpr int kWeightTaps = 151;
+DI int p02_radius(const rc_vhs_params& P) {
+    const float sigma = gmax(P.chroma_res_sigma, 0.5f);
+    return imin(imax((int)(sigma * 2.5f + 0.5f), 1), 32);
+}
+DI void fill_weights(int pass, const rc_vhs_params& P, float* wtab) {
+    for (int j = threadIdx.x; j < kWeightTaps; j += blockDim.x) {
+        if (pass == 1 && j < 9) {
+            wtab[j] = gauss((float)(j - 4), gmax(P.luma_blur_sigma, 0.01f));
+        } else if (pass == 2) {
+            const int r = p02_radius(P);
+            if (j <= 2 * r) wtab[j] = gauss((float)(j - r), gmax(P.chroma_res_sigma, 0.5f));
+        } else if (pass == 8 && j >= 1) {
+            wtab[j] = rcx_powf(0.70f, (float)j);
+        }
+    }
+}
+
 // p01_downsample.frag: 9-tap horizontal Gaussian
-DI V3 p01(const Tex& t, const Frag& f, const rc_vhs_params& P) {
+DI V3 p01(const Tex& t, const Frag& f, const rc_vhs_params& P, const float* wtab) {
     const float tsx = 1.0f / (float)t.w;
-    const float sigma = gmax(P.luma_blur_sigma, 0.01f);
     V3 sum = v3(0.0f, 0.0f, 0.0f);
     float wt = 0.0f;
     for (int i = -4; i <= 4; i++) {
-        const float w = gauss((float)i, sigma);
+        const float w = wtab[i + 4];
         sum = sum + tex(t, f.u + (float)i * tsx, f.v + 0.0f) * w;
         wt += w;
     }
@@ -149,14 +169,13 @@ DI V3 p01(const Tex& t, const Frag& f, const rc_vhs_params& P) {
 }
 
 // p02_chroma_res.frag: Gaussian blur of Cb/Cr only
-DI V3 p02(const Tex& t, const Frag& f, const rc_vhs_params& P) {
+DI V3 p02(const Tex& t, const Frag& f, const rc_vhs_params& P, const float* wtab) {
     const float tsx = 1.0f / (float)t.w;
-    const float sigma = gmax(P.chroma_res_sigma, 0.5f);
-    const int radius = imin(imax((int)(sigma * 2.5f + 0.5f), 1), 32);
+    const int radius = p02_radius(P);
     const float lumaY = ycc5(tex(t, f.u, f.v)).x;
     float cb = 0.0f, cr = 0.0f, wt = 0.0f;
     for (int i = -radius; i <= radius; i++) {
-        const float w = gauss((float)i, sigma);
+        const float w = wtab[i + radius];
         const V3 c = ycc5(tex(t, f.u + (float)i * tsx, f.v + 0.0f));
         cb = cb + c.y * w;
         cr = cr + c.z * w;
@@ -240,7 +259,7 @@ DI V3 p07(const Tex& t, const Frag& f, const rc_vhs_params& P) {
 
 // p08_ccd_smear.frag: vertical overflow streaks above and below bright pixels
 DI float luma601(V3 c) { return 0.299f * c.x + 0.587f * c.y + 0.114f * c.z; }
-DI V3 p08(const Tex& t, const Frag& f, const rc_vhs_params& P) {
+DI V3 p08(const Tex& t, const Frag& f, const rc_vhs_params& P, const float* wtab) {
     const V3 base = tex(t, f.u, f.v);
     const float tsy = 1.0f / (float)t.h;
     float pa = 0.0f;
@@ -260,7 +279,7 @@ DI V3 p08(const Tex& t, const Frag& f, const rc_vhs_params& P) {
         if (i > sl) break;
         const float sy = f.v - (float)i * tsy;
         if (sy < 0.0f) break;
-        sa += gmax(0.0f, luma601(tex(t, f.u - 0.0f, sy)) - P.ccd_smear_threshold) * rcx_powf(0.70f, (float)i);
+        sa += gmax(0.0f, luma601(tex(t, f.u - 0.0f, sy)) - P.ccd_smear_threshold) * wtab[i];
         st++;
     }
     const float sc = (st > 0) ? (sa / (float)st) * P.ccd_smear_intensity * 0.25f : 0.0f;
@@ -564,18 +583,23 @@ struct VhsArgs {
 };
 
 __global__ void __launch_bounds__(128) vhs_pass_kernel(VhsArgs A) {
+    __shared__ float wtab[kWeightTaps];
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (A.pass == 1 || A.pass == 2 || A.pass == 8) {   // uniform per launch
+        fill_weights(A.pass, A.p, wtab);
+        __syncthreads();
+    }
     if (x >= A.w) return;
     const Tex t{A.in, A.w, A.h};
     const Frag f{((float)x + 0.5f) / (float)A.w, ((float)y + 0.5f) / (float)A.h, (float)x + 0.5f, (float)y + 0.5f};
     V3 c;
     switch (A.pass) {   // uniform per launch
-        case 1: c = p01(t, f, A.p); break;
-        case 2: c = p02(t, f, A.p); break;
+        case 1: c = p01(t, f, A.p, wtab); break;
+        case 2: c = p02(t, f, A.p, wtab); break;
         case 3: c = p03(t, f, A.p); break;
         case 4: c = p04(t, f, A.p); break;
         case 7: c = p07(t, f, A.p); break;
-        case 8: c = p08(t, f, A.p); break;
+        case 8: c = p08(t, f, A.p, wtab); break;
         case 9: c = p09(t, f, A.p); break;
         case 10: c = p10(t, f, A.p); break;
         case 11: c = p11(t, f, A.p); break;
