@@ -151,17 +151,23 @@ __device__ __forceinline__ void stage_row(const ConvArgs& A, uint4* slot, int n,
 
 // The 9 taps x CIN/16 k-steps of one tile: rows[dy] is the slot of image row
 // y - 1 + dy; the A operand of tap (dy, dx) is that slot shifted by dx pixels.
+// A descriptor's start address is its low 14 bits (address / 16; shared
+// memory is below 256 KB), so the descriptor of base + offset is the base
+// descriptor plus offset / 16: each MMA adds a compile-time constant.
 template <int CIN>
 __device__ __forceinline__ void issue_tile(const uint32_t (&rows)[3], uint32_t wts, uint32_t tmem_d, uint64_t* mbar) {
     constexpr int G = CIN / 8;   // 16-byte channel groups per pixel (two per k-step)
     constexpr uint32_t idesc = tc::idesc_bf16(128, kCo, false, false);
-#pragma unroll 1
+    const uint64_t da[3] = {tc::smem_desc(rows[0], kPStride * 16, 128), tc::smem_desc(rows[1], kPStride * 16, 128),
+                            tc::smem_desc(rows[2], kPStride * 16, 128)};
+    const uint64_t db = tc::smem_desc(wts, kCo * 16, 128);
+#pragma unroll
     for (int tap = 0; tap < 9; ++tap) {
         const int dy = tap / 3, dx = tap - 3 * dy;
 #pragma unroll
         for (int ks = 0; ks < CIN / 16; ++ks) {
-            const uint64_t a = tc::smem_desc(rows[dy] + ((2 * ks) * kPStride + dx) * 16, kPStride * 16, 128);
-            const uint64_t b = tc::smem_desc(wts + (tap * G + 2 * ks) * kCo * 16, kCo * 16, 128);
+            const uint64_t a = da[dy] + (uint64_t)((2 * ks) * kPStride + dx);
+            const uint64_t b = db + (uint64_t)((tap * G + 2 * ks) * kCo);
             tc::mma_bf16(tmem_d, a, b, idesc, (tap | ks) != 0);
         }
     }
@@ -272,15 +278,17 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
     uint32_t phase[2] = {0u, 0u};
     bool ok = true;
     int k = 0;
-    for (; k < rows_here && ok; ++k) {
+    for (; k < rows_here; ++k) {
         const int acc = k & 1;
         const int y = y0 + k;
-        // rows of tile k landed (all groups but the newest kAhead - 1)
+        // rows of tile k landed (all groups but the newest kAhead - 1); the
+        // barrier also makes the warps' wait results uniform
         cp_async_wait<kAhead - 1>();
         tc::fence_async_smem();
         tc::fence_before_sync();
-        __syncthreads();
+        ok = __syncthreads_and(ok);
         tc::fence_after_sync();
+        if (!ok) break;
         if (tid == 0) {
             const uint32_t rows[3] = {tc::smem_u32(S.rows[k % kSlots]), tc::smem_u32(S.rows[(k + 1) % kSlots]),
                                       tc::smem_u32(S.rows[(k + 2) % kSlots])};
@@ -290,9 +298,11 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
             if (kAhead < rows_here) stage_row<CIN>(A, S.rows[2 + kAhead], n, y + 1 + kAhead, x0);
             cp_async_commit();
         } else {
-            // epilogue of tile k-1 while the tensor cores work on tile k
+            // epilogue of tile k-1 while the tensor cores work on tile k;
+            // each warp waits for tile k-1's MMAs itself, so warps 1-3 need
+            // not wait for thread 0 to finish issuing tile k
             const int pa = acc ^ 1;
-            ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
+            ok = __all_sync(0xffffffffu, tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
             phase[pa] ^= 1u;
             tc::fence_after_sync();
             // tile k-1's MMAs are done with its first row: that slot takes
@@ -309,6 +319,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
         }
     }
     // epilogue of the last tile
+    ok = __syncthreads_and(ok);
     if (ok && k > 0) {
         const int pa = (k - 1) & 1;
         ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));

@@ -582,33 +582,34 @@ struct VhsArgs {
     rc_vhs_params p;
 };
 
+// One instantiation per pass, so each pass gets the registers it needs
+// (the multi-tap passes bound the occupancy of a single switch kernel).
+template <int K>
 __global__ void __launch_bounds__(128) vhs_pass_kernel(VhsArgs A) {
     __shared__ float wtab[kWeightTaps];
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (A.pass == 1 || A.pass == 2 || A.pass == 8) {   // uniform per launch
-        fill_weights(A.pass, A.p, wtab);
+    if (K == 1 || K == 2 || K == 8) {
+        fill_weights(K, A.p, wtab);
         __syncthreads();
     }
     if (x >= A.w) return;
     const Tex t{A.in, A.w, A.h};
     const Frag f{((float)x + 0.5f) / (float)A.w, ((float)y + 0.5f) / (float)A.h, (float)x + 0.5f, (float)y + 0.5f};
     V3 c;
-    switch (A.pass) {   // uniform per launch
-        case 1: c = p01(t, f, A.p, wtab); break;
-        case 2: c = p02(t, f, A.p, wtab); break;
-        case 3: c = p03(t, f, A.p); break;
-        case 4: c = p04(t, f, A.p); break;
-        case 7: c = p07(t, f, A.p); break;
-        case 8: c = p08(t, f, A.p, wtab); break;
-        case 9: c = p09(t, f, A.p); break;
-        case 10: c = p10(t, f, A.p); break;
-        case 11: c = p11(t, f, A.p); break;
-        case 12: c = p12(t, f, A.p); break;
-        case 13: c = p13(t, f, A.p); break;
-        case 14: c = p14(t, f, A.p); break;
-        case 15: c = p15(t, f, A.p); break;
-        default: c = p16(t, f, A.p); break;
-    }
+    if (K == 1) c = p01(t, f, A.p, wtab);
+    else if (K == 2) c = p02(t, f, A.p, wtab);
+    else if (K == 3) c = p03(t, f, A.p);
+    else if (K == 4) c = p04(t, f, A.p);
+    else if (K == 7) c = p07(t, f, A.p);
+    else if (K == 8) c = p08(t, f, A.p, wtab);
+    else if (K == 9) c = p09(t, f, A.p);
+    else if (K == 10) c = p10(t, f, A.p);
+    else if (K == 11) c = p11(t, f, A.p);
+    else if (K == 12) c = p12(t, f, A.p);
+    else if (K == 13) c = p13(t, f, A.p);
+    else if (K == 14) c = p14(t, f, A.p);
+    else if (K == 15) c = p15(t, f, A.p);
+    else c = p16(t, f, A.p);
     A.out[(size_t)y * A.w + x] = make_float4(c.x, c.y, c.z, 1.0f);
 }
 
@@ -617,7 +618,24 @@ bool has_pass(int pass) { return pass >= 1 && pass <= 16 && pass != 5 && pass !=
 cudaError_t launch_pass(int pass, const float4* in, float4* out, int w, int h, const rc_vhs_params& p,
                         cudaStream_t s) {
     VhsArgs A{in, out, w, h, pass, p};
-    vhs_pass_kernel<<<dim3((w + 127) / 128, h), 128, 0, s>>>(A);
+    const dim3 grid((w + 127) / 128, h);
+    switch (pass) {
+        case 1: vhs_pass_kernel<1><<<grid, 128, 0, s>>>(A); break;
+        case 2: vhs_pass_kernel<2><<<grid, 128, 0, s>>>(A); break;
+        case 3: vhs_pass_kernel<3><<<grid, 128, 0, s>>>(A); break;
+        case 4: vhs_pass_kernel<4><<<grid, 128, 0, s>>>(A); break;
+        case 7: vhs_pass_kernel<7><<<grid, 128, 0, s>>>(A); break;
+        case 8: vhs_pass_kernel<8><<<grid, 128, 0, s>>>(A); break;
+        case 9: vhs_pass_kernel<9><<<grid, 128, 0, s>>>(A); break;
+        case 10: vhs_pass_kernel<10><<<grid, 128, 0, s>>>(A); break;
+        case 11: vhs_pass_kernel<11><<<grid, 128, 0, s>>>(A); break;
+        case 12: vhs_pass_kernel<12><<<grid, 128, 0, s>>>(A); break;
+        case 13: vhs_pass_kernel<13><<<grid, 128, 0, s>>>(A); break;
+        case 14: vhs_pass_kernel<14><<<grid, 128, 0, s>>>(A); break;
+        case 15: vhs_pass_kernel<15><<<grid, 128, 0, s>>>(A); break;
+        case 16: vhs_pass_kernel<16><<<grid, 128, 0, s>>>(A); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
