@@ -174,7 +174,9 @@ typedef struct rc_counters {
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
 #define RC_ENGINE_WAVEFRONT 1   /* per-bounce kernels over compacted path queues;
                                    fast math traces with a persistent kernel
-                                   that refills idle lanes with new rays */
+                                   that refills idle lanes with new rays
+                                   (chunks of rc_tuning.refill_min_paths
+                                   paths or more; smaller ones grid-stride) */
 #define RC_ENGINE_WAVEFRONT_STATIC 2 /* as above, traced with a grid-stride loop */
 
 /* rc_tuning.wide_bvh bits: which rays traverse the 4-wide copy of the BVH
@@ -205,6 +207,9 @@ typedef struct rc_tuning {
     int32_t leaf_quarters; /* RC_ENGINE_WAVEFRONT trace: a warp tests its parked leaves
                               once this many quarters of its busy lanes cannot step on
                               (or all have a leaf parked), 1..4 (0 = 2) */
+    int32_t refill_min_paths; /* RC_ENGINE_WAVEFRONT, fast math: chunks of fewer paths are
+                                 traced with the grid-stride loop, where a launch holds
+                                 about one wave of rays (0 = 1048576; 1 = always refill) */
 } rc_tuning;
 
 /* error_word bits. */

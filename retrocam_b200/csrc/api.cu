@@ -109,6 +109,7 @@ struct rc_ctx {
     int trace_block = 128, shade_block = 128, photon_block = 128;
     int photon_full_first = 0;
     int refill_lanes = 16, leaf_quarters = 2;
+    int refill_min_paths = 1 << 20;
     DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
         wf_qlen;
     int wf_capacity = 0;
@@ -705,11 +706,12 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
         t->chunk_paths < 0 || (t->wide_bvh & ~(RC_WIDE_PATHS | RC_WIDE_PHOTONS)) || !valid_block(t->trace_block) ||
         !valid_block(t->shade_block) || !valid_block(t->photon_block) ||
         (t->photon_full_first != 0 && t->photon_full_first != 1) || t->refill_lanes < 0 || t->refill_lanes > 32 ||
-        t->leaf_quarters < 0 || t->leaf_quarters > 4)
+        t->leaf_quarters < 0 || t->leaf_quarters > 4 || t->refill_min_paths < 0)
         return fail(ctx, RC_ERR_INVALID_ARG,
-                    "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d first %d refill %d leaf %d", t->engine,
-                    t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block,
-                    t->photon_full_first, t->refill_lanes, t->leaf_quarters);
+                    "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d first %d refill %d leaf %d "
+                    "refill_min %d",
+                    t->engine, t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block,
+                    t->photon_full_first, t->refill_lanes, t->leaf_quarters, t->refill_min_paths);
     ctx->engine = t->engine;
     ctx->chunk_paths = t->chunk_paths;
     ctx->wide_bvh = t->wide_bvh;
@@ -719,6 +721,7 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
     ctx->photon_full_first = t->photon_full_first;
     ctx->refill_lanes = t->refill_lanes ? t->refill_lanes : 16;
     ctx->leaf_quarters = t->leaf_quarters ? t->leaf_quarters : 2;
+    ctx->refill_min_paths = t->refill_min_paths ? t->refill_min_paths : (1 << 20);
     return RC_OK;
 }
 
@@ -734,6 +737,7 @@ int rc_get_tuning(rc_ctx* ctx, rc_tuning* out) {
     out->photon_full_first = ctx->photon_full_first;
     out->refill_lanes = ctx->refill_lanes;
     out->leaf_quarters = ctx->leaf_quarters;
+    out->refill_min_paths = ctx->refill_min_paths;
     return RC_OK;
 }
 
@@ -818,6 +822,7 @@ static WaveArgs wave_args(rc_ctx* ctx, const DeviceScene& scene, int nee_enabled
     A.npix = tiles_x * tiles_y * 32;
     A.counters = ctx->counters;
     A.dynamic_fetch = ctx->engine == RC_ENGINE_WAVEFRONT ? 1 : 0;
+    A.refill_min_paths = ctx->refill_min_paths;
     A.refill_lanes = ctx->refill_lanes;
     A.leaf_quarters = ctx->leaf_quarters;
     A.bounce = 0;
@@ -1590,9 +1595,10 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
                                 &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len, &ctx->gcache,
                                 &ctx->batch_gcache, &ctx->gheavy})
             key = fnv1a(key, &b->ptr, sizeof(void*));
-        const int shape[9] = {ctx->chunk_paths,  ctx->wide_bvh,       ctx->trace_block,
-                              ctx->shade_block,  ctx->photon_block,   ctx->width,
-                              ctx->photon_full_first, ctx->refill_lanes, ctx->leaf_quarters};
+        const int shape[10] = {ctx->chunk_paths,  ctx->wide_bvh,       ctx->trace_block,
+                               ctx->shade_block,  ctx->photon_block,   ctx->width,
+                               ctx->photon_full_first, ctx->refill_lanes, ctx->leaf_quarters,
+                               ctx->refill_min_paths};
         key = fnv1a(key, shape, sizeof(shape));
         if (!ctx->graph_exec || ctx->graph_key != key) {
             if (ctx->graph_exec) {

@@ -260,6 +260,7 @@ struct WaveArgs {
     int paths;         // paths of the chunk (all segments)
     int bounce;
     int dynamic_fetch; // fast build: persistent trace kernel with ray refill
+    int refill_min_paths;  // ... for chunks of at least this many paths
     int refill_lanes;  // refill when fewer lanes than this are busy (1..32)
     int leaf_quarters; // leaf phase once this many quarters of the busy lanes are blocked (1..4)
     DevCounters* counters;

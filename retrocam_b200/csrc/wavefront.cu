@@ -628,7 +628,10 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
     const int c = block_class(block), b = 64 << c;
 #if !RC_EXACT
     // the refill trace packs leaf counts into 16 bits of a stack entry
-    if (A.dynamic_fetch && A.scene.max_leaf < 0x10000) {
+    // chunks below refill_min_paths hold about one wave of rays per launch,
+    // where the refill bookkeeping costs more than it recovers (854x480 at
+    // 1 spp: trace 0.264 ms grid-stride vs 0.306 ms refill; they tie at 2 spp)
+    if (A.dynamic_fetch && A.paths >= A.refill_min_paths && A.scene.max_leaf < 0x10000) {
         if (A.scene.nodes4)
             wf_trace_dyn4<<<grids().dyn4[c], b, 0, s>>>(A);
         else

@@ -33,10 +33,14 @@ def _ctx(product, W, H, mode, engine="wavefront"):
         ctx.set_engine(product.RC_ENGINE_MEGAKERNEL)
     elif engine == "wavefront_small_chunks":
         ctx.set_engine(product.RC_ENGINE_WAVEFRONT, 5000)   # several chunks per call
+        ctx.set_tuning(refill_min_paths=1)
     elif engine == "wavefront_static":
         ctx.set_engine(product.RC_ENGINE_WAVEFRONT_STATIC)
     else:
+        # the refill trace even for the tests' small chunks (by default
+        # chunks below 2^20 paths are traced grid-stride)
         ctx.set_engine(product.RC_ENGINE_WAVEFRONT)
+        ctx.set_tuning(refill_min_paths=1)
     return ctx
 
 
@@ -61,13 +65,13 @@ def test_tuning_roundtrip_and_validation(product):
         t = ctx.tuning()
         assert t == {"engine": product.RC_ENGINE_WAVEFRONT, "chunk_paths": 0, "wide_bvh": 0,
                      "trace_block": 128, "shade_block": 128, "photon_block": 128, "photon_full_first": 0,
-                     "refill_lanes": 16, "leaf_quarters": 2}
+                     "refill_lanes": 16, "leaf_quarters": 2, "refill_min_paths": 1 << 20}
         ctx.set_tuning(engine=product.RC_ENGINE_WAVEFRONT_STATIC, wide_bvh=3, trace_block=256, shade_block=64)
         t = ctx.tuning()
         assert (t["engine"], t["wide_bvh"], t["trace_block"], t["shade_block"]) == (2, 3, 256, 64)
         for bad in ({"engine": 7}, {"chunk_paths": -1}, {"wide_bvh": 4}, {"trace_block": 96},
                     {"photon_block": 512}, {"photon_full_first": 2},
-                    {"refill_lanes": 33}, {"leaf_quarters": 5}):
+                    {"refill_lanes": 33}, {"leaf_quarters": 5}, {"refill_min_paths": -1}):
             with pytest.raises(product.RetroCamError) as e:
                 ctx.set_tuning(**bad)
             assert e.value.code == product.RC_ERR_INVALID_ARG
