@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "device_scene.h"
+#include "host_checks.h"
 #include "retrocam.h"
 
 namespace rc {
@@ -1144,6 +1145,8 @@ int rc_denoise_atrous(rc_ctx* ctx, const rc_atrous_params* p, float* out_rgba) {
 int rc_kp_features(rc_ctx* ctx, void* feat, void* color) {
     if (!ctx) return RC_ERR_INVALID_ARG;
     if (!feat || !color) return fail(ctx, RC_ERR_INVALID_ARG, "rc_kp_features: null buffer");
+    if (!rc::aligned_to(feat, 16) || !rc::aligned_to(color, 16))
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_kp_features: buffers must be 16-byte aligned");
     CK(cudaSetDevice(ctx->device));
     const cudaError_t e = timed_launch(ctx, RC_KERNEL_KPCNN, [&] {
         return kp::launch_features(ctx->img.accum, ctx->img.gbuf, ctx->img.galb, static_cast<__nv_bfloat16*>(feat),

@@ -42,6 +42,7 @@
 #include <stdint.h>
 
 #include "retrocam.h"
+#include "host_checks.h"
 #include "tc_sm100.cuh"
 
 namespace rc {
@@ -766,6 +767,9 @@ int rc_kp_conv3x3(const void* in, int cin, const void* wpk, const float* bias, v
                   const void* mask, int n, int h, int w, unsigned int* err, void* stream) {
     if (!in || !wpk || !out || !err || (cin != 16 && cin != 32) || n <= 0 || h <= 0 || w <= 0)
         return RC_ERR_INVALID_ARG;
+    if (!rc::aligned_to(in, 16) || !rc::aligned_to(wpk, 16) || !rc::aligned_to(out, 16) ||
+        !rc::aligned_to(mask, 16) || !rc::aligned_to(bias, 4) || !rc::aligned_to(err, 4))
+        return RC_ERR_INVALID_ARG;
     ConvArgs A{static_cast<const __nv_bfloat16*>(in), static_cast<const __nv_bfloat16*>(wpk), bias, out,
                static_cast<const __nv_bfloat16*>(mask), n, h, w, relu, out_f32, err, nullptr, nullptr};
     return launch_conv(A, cin, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
@@ -775,6 +779,9 @@ int rc_kp_wgrad(const void* x, int cin, const void* dy, float* dw, float* db, in
                 unsigned int* err, void* stream) {
     if (!x || !dy || !dw || !db || !err || (cin != 16 && cin != 32) || n <= 0 || h <= 0 || w <= 0)
         return RC_ERR_INVALID_ARG;
+    if (!rc::aligned_to(x, 16) || !rc::aligned_to(dy, 16) || !rc::aligned_to(dw, 4) || !rc::aligned_to(db, 4) ||
+        !rc::aligned_to(err, 4))
+        return RC_ERR_INVALID_ARG;
     WgradArgs A{static_cast<const __nv_bfloat16*>(x), static_cast<const __nv_bfloat16*>(dy), dw, db, n, h, w, err};
     return launch_wgrad(A, cin, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
 }
@@ -782,6 +789,9 @@ int rc_kp_wgrad(const void* x, int cin, const void* dy, float* dw, float* db, in
 int rc_kp_head(const float* logits, const void* color, const void* target, void* out, void* dlogits,
                double* loss, float grad_scale, int n, int h, int w, void* stream) {
     if (!logits || !color || !out || n <= 0 || h <= 0 || w <= 0 || (dlogits && !target)) return RC_ERR_INVALID_ARG;
+    if (!rc::aligned_to(logits, 16) || !rc::aligned_to(color, 16) || !rc::aligned_to(target, 16) ||
+        !rc::aligned_to(out, 16) || !rc::aligned_to(dlogits, 16) || !rc::aligned_to(loss, 8))
+        return RC_ERR_INVALID_ARG;
     HeadArgs A{logits,
                static_cast<const float4*>(color),
                static_cast<const float4*>(target),
@@ -796,10 +806,10 @@ int rc_kp_head(const float* logits, const void* color, const void* target, void*
 }
 
 int rc_kp_pack(const float* params, void* const* packed7, void* stream) {
-    if (!params || !packed7) return RC_ERR_INVALID_ARG;
+    if (!params || !packed7 || !rc::aligned_to(params, 4)) return RC_ERR_INVALID_ARG;
     __nv_bfloat16* w[7];
     for (int i = 0; i < 7; ++i) {
-        if (!packed7[i]) return RC_ERR_INVALID_ARG;
+        if (!packed7[i] || !rc::aligned_to(packed7[i], 16)) return RC_ERR_INVALID_ARG;
         w[i] = static_cast<__nv_bfloat16*>(packed7[i]);
     }
     return launch_pack(params, w, static_cast<cudaStream_t>(stream)) == cudaSuccess ? RC_OK : RC_ERR_CUDA;
@@ -808,6 +818,8 @@ int rc_kp_pack(const float* params, void* const* packed7, void* stream) {
 int rc_kp_adam(float* params, float* grads, float* m, float* v, int count, float lr, float beta1, float beta2,
                float eps, int step, void* stream) {
     if (!params || !grads || !m || !v || count <= 0 || step < 1) return RC_ERR_INVALID_ARG;
+    if (!rc::aligned_to(params, 4) || !rc::aligned_to(grads, 4) || !rc::aligned_to(m, 4) || !rc::aligned_to(v, 4))
+        return RC_ERR_INVALID_ARG;
     const float c1 = 1.0f / (1.0f - powf(beta1, (float)step)), c2 = 1.0f / (1.0f - powf(beta2, (float)step));
     adam_kernel<<<(count + 255) / 256, 256, 0, static_cast<cudaStream_t>(stream)>>>(params, grads, m, v, count, lr,
                                                                                      beta1, beta2, eps, c1, c2);
@@ -820,6 +832,10 @@ int rc_kp_crop(const void* feat_all, const void* color_all, const void* target_a
     if (!feat_all || !color_all || !target_all || !src || !tgt || !oy || !ox || !feat || !color || !target ||
         batch <= 0 || size <= 0 || size > H || size > W)
         return RC_ERR_INVALID_ARG;
+    for (const void* q : {feat_all, color_all, target_all, (const void*)feat, (const void*)color, (const void*)target})
+        if (!rc::aligned_to(q, 16)) return RC_ERR_INVALID_ARG;
+    for (const void* q : {(const void*)src, (const void*)tgt, (const void*)oy, (const void*)ox})
+        if (!rc::aligned_to(q, 4)) return RC_ERR_INVALID_ARG;
     const dim3 grid((size + 127) / 128, size, batch);
     crop_kernel<<<grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
         static_cast<const __nv_bfloat16*>(feat_all), static_cast<const float4*>(color_all),

@@ -20,6 +20,7 @@
 #include <mutex>
 
 #include "device_scene.h"
+#include "host_checks.h"
 #include "retrocam.h"
 
 namespace rc {
@@ -79,6 +80,9 @@ extern "C" int rc_denoise_atrous_noalloc(const float* accum, const uint16_t* gbu
     if (!accum || !gbuffer || !albedo || !variance || !out || !p || width < 1 || height < 1 ||
         (math_mode != RC_MATH_FAST && math_mode != RC_MATH_EXACT))
         return rc_noalloc_fail(RC_ERR_INVALID_ARG, "rc_denoise_atrous_noalloc: bad arguments");
+    if (!aligned_to(accum, 16) || !aligned_to(out, 16) || !aligned_to(gbuffer, 8) || !aligned_to(albedo, 8) ||
+        !aligned_to(variance, 4))
+        return rc_noalloc_fail(RC_ERR_INVALID_ARG, "rc_denoise_atrous_noalloc: misaligned buffer");
     if ((const void*)out == (const void*)accum)
         return rc_noalloc_fail(RC_ERR_INVALID_ARG, "rc_denoise_atrous_noalloc: out must not alias accum");
     if ((long long)width * height > RC_NOALLOC_MAX_PIXELS)

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "host_checks.h"
 #include "rc_exact_math.h"
 #include "retrocam.h"
 
@@ -693,7 +694,8 @@ void rc_vhs_defaults(rc_vhs_params* p) {
 }
 
 int rc_vhs_pass(int pass, const void* in_rgba, void* out_rgba, int w, int h, const rc_vhs_params* p, void* stream) {
-    if (!rc::vhs::has_pass(pass) || !in_rgba || !out_rgba || !p || w <= 0 || h <= 0 || in_rgba == out_rgba)
+    if (!rc::vhs::has_pass(pass) || !in_rgba || !out_rgba || !p || w <= 0 || h <= 0 || w > 16384 || h > 16384 ||
+        in_rgba == out_rgba || !rc::aligned_to(in_rgba, 16) || !rc::aligned_to(out_rgba, 16))
         return RC_ERR_INVALID_ARG;
     return rc::vhs::launch_pass(pass, static_cast<const float4*>(in_rgba), static_cast<float4*>(out_rgba), w, h, *p,
                                 static_cast<cudaStream_t>(stream)) == cudaSuccess
