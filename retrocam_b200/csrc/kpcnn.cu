@@ -81,8 +81,18 @@ struct ConvArgs {
 // The network's head: softmax of 25 logits (in place: the normalised
 // weights) and the 5x5 filter of the noisy colour of image `img` with them,
 // edges clamped.
-__device__ __forceinline__ float3 apply_head(float (&l)[25], const float4* __restrict__ img, int y, int x, int h,
-                                             int w) {
+// The 5x5 neighbourhood of (y, x) in img (rgb), edges clamped.
+__device__ __forceinline__ void head_taps(const float4* __restrict__ img, int y, int x, int h, int w,
+                                          float3 (&c)[25]) {
+#pragma unroll
+    for (int t = 0; t < 25; ++t) {
+        const int yy = min(max(y + t / 5 - 2, 0), h - 1), xx = min(max(x + t % 5 - 2, 0), w - 1);
+        const float4 v = __ldg(img + (size_t)yy * w + xx);
+        c[t] = make_float3(v.x, v.y, v.z);
+    }
+}
+
+__device__ __forceinline__ float3 head_filter(float (&l)[25], const float3 (&c)[25]) {
     float m = l[0];
 #pragma unroll
     for (int t = 1; t < 25; ++t) m = fmaxf(m, l[t]);
@@ -97,13 +107,18 @@ __device__ __forceinline__ float3 apply_head(float (&l)[25], const float4* __res
 #pragma unroll
     for (int t = 0; t < 25; ++t) {
         l[t] *= inv;
-        const int yy = min(max(y + t / 5 - 2, 0), h - 1), xx = min(max(x + t % 5 - 2, 0), w - 1);
-        const float4 c = __ldg(img + (size_t)yy * w + xx);
-        o.x += l[t] * c.x;
-        o.y += l[t] * c.y;
-        o.z += l[t] * c.z;
+        o.x += l[t] * c[t].x;
+        o.y += l[t] * c[t].y;
+        o.z += l[t] * c[t].z;
     }
     return o;
+}
+
+__device__ __forceinline__ float3 apply_head(float (&l)[25], const float4* __restrict__ img, int y, int x, int h,
+                                             int w) {
+    float3 c[25];
+    head_taps(img, y, x, h, w, c);
+    return head_filter(l, c);
 }
 
 // Shared memory of the convolution: a ring of five staged image rows (the
@@ -175,7 +190,22 @@ __device__ __forceinline__ void issue_tile(const uint32_t (&rows)[3], uint32_t w
     tc::mma_commit(mbar);
 }
 
-__device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&vin)[32], int t, int tiles_x) {
+// The head's radiance taps of this thread's pixel of tile t (HEAD only),
+// loaded before the tile's MMAs are waited for so their latency overlaps.
+template <bool HEAD>
+__device__ __forceinline__ void epilogue_taps(const ConvArgs& A, int t, int tiles_x, float3 (&c)[25]) {
+    if (!HEAD) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int xt = t % tiles_x, rest = t / tiles_x;
+    const int y = rest % A.h, n = rest / A.h;
+    const int x = xt * kTile + warp * 32 + lane;
+    if (x >= A.w) return;
+    head_taps(A.head_color + (size_t)n * A.h * A.w, y, x, A.h, A.w, c);
+}
+
+template <bool HEAD>
+__device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&vin)[32], int t, int tiles_x,
+                                              const float3 (&taps)[25]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int xt = t % tiles_x, rest = t / tiles_x;
     const int y = rest % A.h, n = rest / A.h;
@@ -207,11 +237,11 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&v
             }
         }
     }
-    if (A.head_color) {
+    if (HEAD) {
         float l[25];
 #pragma unroll
         for (int t = 0; t < 25; ++t) l[t] = v[t];
-        const float3 o = apply_head(l, A.head_color + (size_t)n * A.h * A.w, y, x, A.h, A.w);
+        const float3 o = head_filter(l, taps);
         A.head_out[pix] = make_float4(o.x, o.y, o.z, 1.0f);
         return;
     }
@@ -242,7 +272,7 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&v
 // into the ring slot tile k-1 read first, and runs the epilogue of tile k-1
 // from the other accumulator; a row copy has two steps to land, and row
 // copies, tensor-core work and epilogues of consecutive tiles overlap.
-template <int CIN>
+template <int CIN, bool HEAD>
 __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) {
     extern __shared__ __align__(128) unsigned char conv_smem_raw[];
     ConvSmem<CIN>& S = *reinterpret_cast<ConvSmem<CIN>*>(conv_smem_raw);
@@ -303,6 +333,8 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
             // each warp waits for tile k-1's MMAs itself, so warps 1-3 need
             // not wait for thread 0 to finish issuing tile k
             const int pa = acc ^ 1;
+            float3 taps[25];
+            epilogue_taps<HEAD>(A, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x, taps);
             ok = __all_sync(0xffffffffu, tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
             phase[pa] ^= 1u;
             tc::fence_after_sync();
@@ -314,7 +346,7 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
             if (ok) {
                 float v[32];
                 tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
-                conv_epilogue(A, v, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x);
+                conv_epilogue<HEAD>(A, v, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x, taps);
             }
             tc::fence_before_sync();
         }
@@ -323,12 +355,14 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
     ok = __syncthreads_and(ok);
     if (ok && k > 0) {
         const int pa = (k - 1) & 1;
+        float3 taps[25];
+        epilogue_taps<HEAD>(A, ((n * A.h) + y0 + k - 1) * tiles_x + xt, tiles_x, taps);
         ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
         tc::fence_after_sync();
         if (ok) {
             float v[32];
             tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
-            conv_epilogue(A, v, ((n * A.h) + y0 + k - 1) * tiles_x + xt, tiles_x);
+            conv_epilogue<HEAD>(A, v, ((n * A.h) + y0 + k - 1) * tiles_x + xt, tiles_x, taps);
         }
     }
     cp_async_wait<0>();
@@ -644,10 +678,10 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
-template <int CIN>
+template <int CIN, bool HEAD>
 static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
     // resident CTAs per SM, found (and the shared-memory limit raised) once
-    // per device
+    // per device and instantiation
     static int per_device[64] = {};
     const size_t smem = sizeof(ConvSmem<CIN>) + 128;
     int dev = 0, sms = 148;
@@ -656,10 +690,10 @@ static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
     int scratch = 0;
     int& per = dev >= 0 && dev < 64 ? per_device[dev] : scratch;
     if (per == 0) {
-        cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<CIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
+        cudaError_t e = cudaFuncSetAttribute(conv3x3_kernel<CIN, HEAD>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(conv3x3_kernel<CIN>, cudaFuncAttributePreferredSharedMemoryCarveout,
+            e = cudaFuncSetAttribute(conv3x3_kernel<CIN, HEAD>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
         // shared memory bounds the CTAs per SM (3 with 32 input channels);
@@ -678,12 +712,15 @@ static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
     int seg_rows = (int)(((long)strips * A.h + cap - 1) / cap);
     if (seg_rows < 1) seg_rows = 1;
     const int grid = strips * ((A.h + seg_rows - 1) / seg_rows);
-    conv3x3_kernel<CIN><<<grid, 128, smem, s>>>(A, seg_rows);
+    conv3x3_kernel<CIN, HEAD><<<grid, 128, smem, s>>>(A, seg_rows);
     return cudaGetLastError();
 }
 
+// The fused head (A.head_color) is a 32-channel instantiation of its own,
+// so its 25 prefetched taps do not raise the other layers' registers.
 cudaError_t launch_conv(const ConvArgs& A, int cin, cudaStream_t s) {
-    return cin == 16 ? launch_conv_t<16>(A, s) : launch_conv_t<32>(A, s);
+    if (A.head_color) return cin == 32 ? launch_conv_t<32, true>(A, s) : cudaErrorInvalidValue;
+    return cin == 16 ? launch_conv_t<16, false>(A, s) : launch_conv_t<32, false>(A, s);
 }
 
 cudaError_t launch_wgrad(const WgradArgs& A, int cin, cudaStream_t s) {
