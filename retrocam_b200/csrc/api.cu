@@ -56,7 +56,7 @@ namespace kp {
 cudaError_t launch_features(const float4* accum, const ushort4* gbuf, const ushort4* galb, __nv_bfloat16* feat,
                             float4* color, int count, cudaStream_t s);
 size_t packed_bytes();
-cudaError_t run_inference(const float* params, void* packed, const float4* accum, const ushort4* gbuf,
+cudaError_t run_inference(const float* params, void* packed, bool repack, const float4* accum, const ushort4* gbuf,
                           const ushort4* galb, void* feat, void* act0, void* act1, float* logits, float4* color,
                           float4* out, int W, int H, unsigned int* err, cudaStream_t s);
 }  // namespace kp
@@ -134,6 +134,7 @@ struct rc_ctx {
     // learned denoiser scratch
     DevBuf kp_feat, kp_act0, kp_act1, kp_logits, kp_color, kp_params, kp_packed;
     std::vector<float> kp_host;   // parameters last uploaded to kp_params
+    void* kp_packed_at = nullptr; // kp_packed holds kp_host packed (its address then)
     cudaGraphExec_t graph_exec = nullptr;
     uint64_t graph_key = 0;
     unsigned long long graph_launches = 0;
@@ -1175,19 +1176,30 @@ int rc_denoise_learned(rc_ctx* ctx, const rc_kpcnn* weights, float* out_rgba) {
     const bool same = ctx->kp_host.size() == (size_t)RC_KPCNN_PARAMS &&
                       memcmp(ctx->kp_host.data(), weights->params, RC_KPCNN_PARAMS * sizeof(float)) == 0;
     if (!same) {
+        ctx->kp_packed_at = nullptr;
         ctx->kp_host.assign(weights->params, weights->params + RC_KPCNN_PARAMS);
-        CK(copy_h2d(ctx, ctx->kp_params.ptr, ctx->kp_host.data(), RC_KPCNN_PARAMS * sizeof(float)));
+        const cudaError_t ce = copy_h2d(ctx, ctx->kp_params.ptr, ctx->kp_host.data(), RC_KPCNN_PARAMS * sizeof(float));
+        if (ce != cudaSuccess) {
+            ctx->kp_host.clear();
+            return launch_err(ctx, ce, "kpcnn parameter upload");
+        }
     }
+    // the packed bf16 weights are redone only when the parameters changed
+    const bool repack = ctx->kp_packed_at != ctx->kp_packed.ptr;
     const cudaError_t e = timed_launch(
         ctx, RC_KERNEL_KPCNN,
         [&] {
-            return kp::run_inference((const float*)ctx->kp_params.ptr, ctx->kp_packed.ptr, ctx->img.accum,
+            return kp::run_inference((const float*)ctx->kp_params.ptr, ctx->kp_packed.ptr, repack, ctx->img.accum,
                                      ctx->img.gbuf, ctx->img.galb, ctx->kp_feat.ptr, ctx->kp_act0.ptr,
                                      ctx->kp_act1.ptr, (float*)ctx->kp_logits.ptr, (float4*)ctx->kp_color.ptr,
                                      ctx->out, ctx->width, ctx->height, &ctx->counters->error_word, ctx->stream);
         },
-        6);
-    if (e != cudaSuccess) return launch_err(ctx, e, "kpcnn");
+        repack ? 6 : 5);
+    if (e != cudaSuccess) {
+        ctx->kp_packed_at = nullptr;
+        return launch_err(ctx, e, "kpcnn");
+    }
+    ctx->kp_packed_at = ctx->kp_packed.ptr;
     ctx->result = ctx->out;
     if (out_rgba) return rc_read_output(ctx, out_rgba);
     return RC_OK;

@@ -764,9 +764,11 @@ size_t packed_bytes() {
     return b;
 }
 
-// Inference over one W x H frame: pack, features, three hidden
-// convolutions, the head convolution and the filter (7 launches).
-cudaError_t run_inference(const float* params, void* packed, const float4* accum, const ushort4* gbuf,
+// Inference over one W x H frame: the weight packing (only with `repack`:
+// the packed copy is kept between calls with the same parameters),
+// features, three hidden convolutions and the head convolution with the
+// filter in its epilogue (5 launches, 6 with the packing).
+cudaError_t run_inference(const float* params, void* packed, bool repack, const float4* accum, const ushort4* gbuf,
                           const ushort4* galb, void* feat, void* act0, void* act1, float* logits, float4* color,
                           float4* out, int W, int H, unsigned int* err, cudaStream_t s) {
     __nv_bfloat16* w[7];
@@ -775,7 +777,7 @@ cudaError_t run_inference(const float* params, void* packed, const float4* accum
         w[i] = p;
         p += kPackedElems[i];
     }
-    cudaError_t e = launch_pack(params, w, s);
+    cudaError_t e = repack ? launch_pack(params, w, s) : cudaSuccess;
     if (e == cudaSuccess) e = launch_features(accum, gbuf, galb, static_cast<__nv_bfloat16*>(feat), color, W * H, s);
     const __nv_bfloat16* f = static_cast<const __nv_bfloat16*>(feat);
     __nv_bfloat16* a0 = static_cast<__nv_bfloat16*>(act0);

@@ -307,3 +307,32 @@ def test_shipped_weights_beat_atrous_on_held_out_variant(product, T):
         a = kpcnn.relmse(ctx.denoise(product.atrous_params(scenes.AtrousDesc())), ref)
         l_ = kpcnn.relmse(ctx.denoise_learned(params), ref)
     assert l_ < 1e-2 and l_ < 0.5 * a, (l_, a)
+
+
+def test_weights_repacked_only_when_they_change(product, T):
+    """A context keeps the packed weights between calls with the same
+    parameters (one launch fewer) and repacks when they change: alternating
+    two parameter vectors on one context gives each vector's own output."""
+    from retrocam_b200 import kpcnn, scenes
+    H, W = 64, 160
+    w = scenes.cornell_variant(6, W, H)
+    pa, pb = kpcnn.init_params(3), kpcnn.init_params(4)
+    pa[kpcnn.WH:kpcnn.BH] *= 30.0
+    pb[kpcnn.WH:kpcnn.BH] *= 30.0
+    outs = {}
+    for name, p in (("a", pa), ("b", pb)):
+        with product.Context(W, H, 0, product.RC_MATH_FAST) as ctx:
+            ctx.upload(product.build_scene(w.scene))
+            ctx.render(product.workload_camera(w), (1, 1.0), 0, 2)
+            outs[name] = ctx.denoise_learned(p)
+    with product.Context(W, H, 0, product.RC_MATH_FAST) as ctx:
+        ctx.upload(product.build_scene(w.scene))
+        ctx.render(product.workload_camera(w), (1, 1.0), 0, 2)
+        seq = []
+        for p in (pa, pa, pb, pb, pa):
+            n0 = ctx.counters()["kernel_launches"]
+            seq.append((ctx.denoise_learned(p), ctx.counters()["kernel_launches"] - n0))
+    assert [n for _, n in seq] == [6, 5, 6, 5, 6]
+    for (img, _), name in zip(seq, "aabba"):
+        np.testing.assert_array_equal(bits(img), bits(outs[name]))
+    assert not np.array_equal(bits(outs["a"]), bits(outs["b"]))
