@@ -36,6 +36,8 @@
 //                        clamped), and for training the relative-MSE loss
 //                        (x-r)^2/(r^2+0.01) with its gradient w.r.t. logits.
 //   features / crop / pack / adam   small SIMT kernels.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -124,8 +126,9 @@ __device__ __forceinline__ float3 apply_head(float (&l)[25], const float4* __res
 // Shared memory of the convolution: a ring of five staged image rows (the
 // three of the tile being multiplied and the new rows of the next two tiles,
 // in flight; the previous tile's first row gives its slot up once that
-// tile's MMAs are done), the weights, and
-// one mbarrier per TMEM accumulator.  A slot is one row of kHalo pixels,
+// tile's MMAs are done), the weights, and the mbarriers: one per ring slot
+// (its row has landed), one per TMEM accumulator for "MMAs done" and one per
+// accumulator for "epilogue read it".  A slot is one row of kHalo pixels,
 // channel-group-major: [CIN/8][kPStride][16 B].
 constexpr int kAhead = 2;             // row copies in flight ahead of the tile
 constexpr int kSlots = 3 + kAhead;
@@ -134,35 +137,21 @@ template <int CIN>
 struct ConvSmem {
     alignas(128) uint4 rows[kSlots][(CIN / 8) * kPStride];
     alignas(128) uint4 wts[9 * (CIN / 8) * kCo];
+    uint64_t full[kSlots];
     uint64_t mbar[2];
+    uint64_t empty[2];
     uint32_t tmem;
 };
 
-// 16-byte asynchronous global -> shared copy; src_bytes 0 writes zeros.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Image row y (pixels x0-1 .. x0+128) of image n into a slot (zeros outside
-// the image), as asynchronous copies; the caller commits the group.
+// Image row y (pixels x0-1 .. x0+128) of image n into a slot, as CIN/8 TMA
+// boxes of 8 channels x kHalo pixels (channel group g lands at [g][0..129]);
+// pixels and rows outside the image read as zero.  One thread.
 template <int CIN>
-__device__ __forceinline__ void stage_row(const ConvArgs& A, uint4* slot, int n, int y, int x0) {
+__device__ __forceinline__ void produce_row(const void* tmap, uint4* slot, uint64_t* full, int n, int y, int x0) {
     constexpr int G = CIN / 8;
-    const uint32_t base = tc::smem_u32(slot);
-    const bool row_in = y >= 0 && y < A.h;
-    for (int i = threadIdx.x; i < kHalo * G; i += 128) {
-        const int p = i / G, g = i - p * G;
-        const int xx = x0 + p - 1;
-        const bool in = row_in && xx >= 0 && xx < A.w;
-        const uint4* src = in ? reinterpret_cast<const uint4*>(A.in + (((size_t)n * A.h + y) * A.w + xx) * CIN) + g
-                              : reinterpret_cast<const uint4*>(A.in);
-        cp_async16(base + (g * kPStride + p) * 16, src, in ? 16u : 0u);
-    }
+    tc::mbar_arrive_expect_tx(full, G * kHalo * 16);
+#pragma unroll
+    for (int g = 0; g < G; ++g) tc::tma_load_4d(tc::smem_u32(slot + g * kPStride), tmap, 8 * g, x0 - 1, y, n, full);
 }
 
 // The 9 taps x CIN/16 k-steps of one tile: rows[dy] is the slot of image row
@@ -267,17 +256,25 @@ __device__ __forceinline__ void conv_epilogue(const ConvArgs& A, const float (&v
 // Implicit-GEMM convolution over column strips: CTA s takes a segment of
 // `seg_rows` consecutive image rows of one 128-pixel-wide strip, so the
 // tiles it walks share rows -- tile y needs rows y-1..y+1 and only row y+1 is
-// new.  Step k issues the MMAs of tile k into one TMEM accumulator, waits for
-// tile k-1's MMAs, copies row y_k + 3 (the new row of tile k+2) asynchronously
-// into the ring slot tile k-1 read first, and runs the epilogue of tile k-1
-// from the other accumulator; a row copy has two steps to land, and row
-// copies, tensor-core work and epilogues of consecutive tiles overlap.
+// new.  Thread 0 is the producer and the MMA issuer: at step k it waits for
+// the rows of tile k (TMA, per-slot mbarrier) and for the epilogues of tile
+// k-2 to have read accumulator k&1, issues the MMAs of tile k, and once tile
+// k-1's MMAs are done loads the new row of tile k+2 into the slot tile k-1
+// read first.  Every warp drains its quarter of tile k-1's accumulator in
+// the meantime, so no step passes a CTA-wide barrier.  All waits are
+// bounded; a timeout sets RC_GUARD_MMA_WAIT and the CTA winds down after
+// waiting (bounded) for the copies and MMAs it started.
 template <int CIN, bool HEAD>
-__global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) {
+__global__ void __launch_bounds__(128)
+    conv3x3_kernel(ConvArgs A, int seg_rows, const __grid_constant__ CUtensorMap tmap) {
     extern __shared__ __align__(128) unsigned char conv_smem_raw[];
-    ConvSmem<CIN>& S = *reinterpret_cast<ConvSmem<CIN>*>(conv_smem_raw);
+    // TMA destinations start on 128-byte boundaries (the launch adds 128
+    // bytes of slack for this)
+    unsigned char* smem_base = conv_smem_raw + ((128u - (tc::smem_u32(conv_smem_raw) & 127u)) & 127u);
+    ConvSmem<CIN>& S = *reinterpret_cast<ConvSmem<CIN>*>(smem_base);
     constexpr int G = CIN / 8;
-    const int tid = threadIdx.x, warp = tid >> 5;
+    constexpr uint32_t FULL = 0xffffffffu;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int tiles_x = (A.w + kTile - 1) / kTile;
     const int segs = (A.h + seg_rows - 1) / seg_rows;       // segments per strip
     const int strip = blockIdx.x / segs;                    // (image, column) strip
@@ -286,90 +283,106 @@ __global__ void __launch_bounds__(128) conv3x3_kernel(ConvArgs A, int seg_rows) 
     const int rows_here = min(seg_rows, A.h - y0);
     if (n >= A.n || rows_here <= 0) return;
     const int x0 = xt * kTile;
+    const void* tm = &tmap;
     if (warp == 0) tc::tmem_alloc(&S.tmem, 64);
     if (tid == 0) {
-        tc::mbar_init(&S.mbar[0], 1);
-        tc::mbar_init(&S.mbar[1], 1);
-    }
-    for (int i = tid; i < 9 * G * kCo; i += 128)
-        cp_async16(tc::smem_u32(&S.wts[i]), reinterpret_cast<const uint4*>(A.wpk) + i, 16u);
-    // image row y0 - 1 + j lives in slot j % kSlots; group 0 = the weights and
-    // the rows of tile 0, group a = the new row of tile a (a < kAhead)
-    for (int j = 0; j < 3; ++j) stage_row<CIN>(A, S.rows[j], n, y0 - 1 + j, x0);
-    cp_async_commit();
-    for (int a = 1; a < kAhead; ++a) {
-        if (a < rows_here) stage_row<CIN>(A, S.rows[2 + a], n, y0 + 1 + a, x0);
-        cp_async_commit();
+        for (int i = 0; i < kSlots; ++i) tc::mbar_init(&S.full[i], 1);
+        for (int a = 0; a < 2; ++a) {
+            tc::mbar_init(&S.mbar[a], 1);
+            tc::mbar_init(&S.empty[a], 4);    // one arrival per warp
+        }
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tmem = S.tmem;
     const uint32_t wts = tc::smem_u32(S.wts);
-    uint32_t phase[2] = {0u, 0u};
-    bool ok = true;
+    // image row y0 - 1 + j lives in slot j % kSlots, its fill number j / kSlots
+    int produced = -1, consumed = -1;   // thread 0: rows loaded / waited for
+    if (tid == 0) {
+        // the weights ride on the first row's barrier (whose one arrival is
+        // produce_row's)
+        tc::mbar_expect_tx(&S.full[0], 9 * G * kCo * 16);
+        tc::bulk_load(wts, A.wpk, 9 * G * kCo * 16, &S.full[0]);
+        for (int j = 0; j < 3 + kAhead - 1 && j < rows_here + 2; ++j) {
+            produce_row<CIN>(tm, S.rows[j], &S.full[j], n, y0 - 1 + j, x0);
+            produced = j;
+        }
+    }
+    bool ok = true;       // warp-uniform
+    bool ok0 = true;      // thread 0's own waits
     int k = 0;
     for (; k < rows_here; ++k) {
         const int acc = k & 1;
         const int y = y0 + k;
-        // rows of tile k landed (all groups but the newest kAhead - 1); the
-        // barrier also makes the warps' wait results uniform
-        cp_async_wait<kAhead - 1>();
-        tc::fence_async_smem();
-        tc::fence_before_sync();
-        ok = __syncthreads_and(ok);
-        tc::fence_after_sync();
-        if (!ok) break;
         if (tid == 0) {
-            const uint32_t rows[3] = {tc::smem_u32(S.rows[k % kSlots]), tc::smem_u32(S.rows[(k + 1) % kSlots]),
-                                      tc::smem_u32(S.rows[(k + 2) % kSlots])};
-            issue_tile<CIN>(rows, wts, tmem + acc * 32, &S.mbar[acc]);
+            // rows k..k+2 of tile k (only row k+2 is new after tile 0)
+            for (int j = k == 0 ? 0 : k + 2; j <= k + 2 && ok0; ++j) {
+                ok0 = tc::mbar_wait(&S.full[j % kSlots], (uint32_t)(j / kSlots) & 1u, kWaitTries);
+                if (ok0) consumed = j;
+            }
+            // accumulator acc was last read by the epilogues of tile k-2
+            if (ok0 && k >= 2) ok0 = tc::mbar_wait(&S.empty[acc], (uint32_t)((k - 2) >> 1) & 1u, kWaitTries);
+            if (ok0) {
+                tc::fence_after_sync();
+                const uint32_t rows[3] = {tc::smem_u32(S.rows[k % kSlots]), tc::smem_u32(S.rows[(k + 1) % kSlots]),
+                                          tc::smem_u32(S.rows[(k + 2) % kSlots])};
+                issue_tile<CIN>(rows, wts, tmem + acc * 32, &S.mbar[acc]);
+            }
         }
         if (k == 0) {
-            if (kAhead < rows_here) stage_row<CIN>(A, S.rows[2 + kAhead], n, y + 1 + kAhead, x0);
-            cp_async_commit();
-        } else {
-            // epilogue of tile k-1 while the tensor cores work on tile k;
-            // each warp waits for tile k-1's MMAs itself, so warps 1-3 need
-            // not wait for thread 0 to finish issuing tile k
-            const int pa = acc ^ 1;
-            float3 taps[25];
-            epilogue_taps<HEAD>(A, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x, taps);
-            ok = __all_sync(0xffffffffu, tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
-            phase[pa] ^= 1u;
-            tc::fence_after_sync();
-            // tile k-1's MMAs are done with its first row: that slot takes
-            // the new row of tile k + kAhead
-            if (ok && k + kAhead < rows_here)
-                stage_row<CIN>(A, S.rows[(k + 2 + kAhead) % kSlots], n, y + 1 + kAhead, x0);
-            cp_async_commit();
-            if (ok) {
-                float v[32];
-                tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
-                conv_epilogue<HEAD>(A, v, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x, taps);
+            if (tid == 0 && ok0 && kAhead < rows_here) {
+                produce_row<CIN>(tm, S.rows[2 + kAhead], &S.full[2 + kAhead], n, y + 1 + kAhead, x0);
+                produced = 2 + kAhead;
             }
-            tc::fence_before_sync();
+            ok = __all_sync(FULL, ok0);
+            if (!ok) break;
+            continue;
         }
+        // epilogue of tile k-1 while the tensor cores work on tile k
+        const int pa = acc ^ 1;
+        float3 taps[25];
+        epilogue_taps<HEAD>(A, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x, taps);
+        ok = __all_sync(FULL, ok0 && tc::mbar_wait(&S.mbar[pa], (uint32_t)((k - 1) >> 1) & 1u, kWaitTries));
+        if (!ok) break;
+        tc::fence_after_sync();
+        // tile k-1's MMAs are done with its first row: that slot takes the
+        // new row of tile k + kAhead
+        if (tid == 0 && k + kAhead < rows_here) {
+            const int j = k + 2 + kAhead;
+            produce_row<CIN>(tm, S.rows[j % kSlots], &S.full[j % kSlots], n, y + 1 + kAhead, x0);
+            produced = j;
+        }
+        float v[32];
+        tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&S.empty[pa]);
+        conv_epilogue<HEAD>(A, v, ((n * A.h) + y - 1) * tiles_x + xt, tiles_x, taps);
     }
     // epilogue of the last tile
-    ok = __syncthreads_and(ok);
     if (ok && k > 0) {
         const int pa = (k - 1) & 1;
         float3 taps[25];
         epilogue_taps<HEAD>(A, ((n * A.h) + y0 + k - 1) * tiles_x + xt, tiles_x, taps);
-        ok = __syncthreads_and(tc::mbar_wait(&S.mbar[pa], phase[pa], kWaitTries));
-        tc::fence_after_sync();
+        ok = __all_sync(FULL, tc::mbar_wait(&S.mbar[pa], (uint32_t)((k - 1) >> 1) & 1u, kWaitTries));
         if (ok) {
+            tc::fence_after_sync();
             float v[32];
             tc::tmem_ld32(tmem + pa * 32 + (static_cast<uint32_t>(warp * 32) << 16), v);
             conv_epilogue<HEAD>(A, v, ((n * A.h) + y0 + k - 1) * tiles_x + xt, tiles_x, taps);
         }
     }
-    cp_async_wait<0>();
+    ok = __syncthreads_and(ok);
     if (!ok) {
-        if (tid == 0) atomicOr(A.err, RC_GUARD_MMA_WAIT);
-        // give MMAs still in flight a bounded time before the columns go
-        for (int a = 0; a < 2; ++a) (void)tc::mbar_wait(&S.mbar[a], phase[a], kWaitTries);
+        if (tid == 0) {
+            atomicOr(A.err, RC_GUARD_MMA_WAIT);
+            // rows still in flight land before the shared memory is released
+            for (int j = consumed + 1; j <= produced; ++j)
+                (void)tc::mbar_wait(&S.full[j % kSlots], (uint32_t)(j / kSlots) & 1u, kWaitTries);
+        }
+        // MMAs still in flight get a bounded time before the columns go
+        for (int a = 0; a < 2; ++a) (void)tc::mbar_wait(&S.mbar[a], (uint32_t)(k >> 1) & 1u, kWaitTries);
     }
     tc::fence_before_sync();
     __syncthreads();
@@ -678,6 +691,38 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+// cuTensorMapEncodeTiled from the driver (the library links only the
+// runtime), looked up once.
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// A convolution's input as a 4-D tensor map (channels, pixels, rows, images;
+// NHWC bf16) read in boxes of 8 channels x kHalo pixels of one row, no
+// swizzle, zeros outside.  The ABI checks that the input is 16-byte
+// aligned; every row pitch is a multiple of 16 bytes (CIN * 2 per pixel).
+template <int CIN>
+static cudaError_t conv_tensor_map(const ConvArgs& A, CUtensorMap* m) {
+    const PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return cudaErrorNotSupported;
+    const cuuint64_t dims[4] = {(cuuint64_t)CIN, (cuuint64_t)A.w, (cuuint64_t)A.h, (cuuint64_t)A.n};
+    const cuuint64_t strides[3] = {(cuuint64_t)CIN * 2, (cuuint64_t)A.w * CIN * 2, (cuuint64_t)A.h * A.w * CIN * 2};
+    const cuuint32_t box[4] = {8, (cuuint32_t)kHalo, 1, 1};
+    const cuuint32_t elem[4] = {1, 1, 1, 1};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(A.in), dims, strides, box,
+                           elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 template <int CIN, bool HEAD>
 static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
     // resident CTAs per SM, found (and the shared-memory limit raised) once
@@ -712,7 +757,10 @@ static cudaError_t launch_conv_t(const ConvArgs& A, cudaStream_t s) {
     int seg_rows = (int)(((long)strips * A.h + cap - 1) / cap);
     if (seg_rows < 1) seg_rows = 1;
     const int grid = strips * ((A.h + seg_rows - 1) / seg_rows);
-    conv3x3_kernel<CIN, HEAD><<<grid, 128, smem, s>>>(A, seg_rows);
+    CUtensorMap tmap;
+    const cudaError_t te = conv_tensor_map<CIN>(A, &tmap);
+    if (te != cudaSuccess) return te;
+    conv3x3_kernel<CIN, HEAD><<<grid, 128, smem, s>>>(A, seg_rows, tmap);
     return cudaGetLastError();
 }
 
