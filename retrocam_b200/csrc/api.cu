@@ -373,9 +373,12 @@ static void isect_record(const rc_triangle& t, float4* out3) {
     out3[2] = make_float4(t.v2[0] - t.v0[0], t.v2[1] - t.v0[1], t.v2[2] - t.v0[2], 0.0f);
 }
 
-// A BVH (the reference's SAH builder) over a subset of the scene's
-// triangles, in the kernels' layout, with each subset triangle's index in
-// the full scene.
+// A BVH over a subset of the scene's triangles, in the kernels' layout,
+// with each subset triangle's index in the full scene.  Only the fast
+// build's photon trace walks these, and any BVH gives its walks the same
+// hits (ties aside), so they come from a binned SAH builder of their own --
+// the reference's builder took about 10 ms for the export scene's 7,936
+// specular triangles, most of an upload's host time.
 struct SubsetBvh {
     std::vector<NodeRec> recs;
     std::vector<float4> isect;
@@ -385,13 +388,165 @@ struct SubsetBvh {
     int max_leaf = 0;   // most triangles in one leaf
 };
 
+// Binned SAH: 16 bins over the centroid extent of each axis, split where
+// (left area x count + right area x count) is least, a leaf of at
+// most 4 triangles when no split beats the leaf's cost (and always at 2 or
+// fewer); an all-in-one-bin node is split at the median index.  Nodes in
+// pre-order from the root at 0, each interior node's children adjacent.
+struct BinnedBuilder {
+    struct Box {
+        float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        // plain compares (a NaN coordinate is skipped), which compile to
+        // min/max instructions where fminf/fmaxf are library calls
+        void grow(const Box& b) {
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = b.lo[a] < lo[a] ? b.lo[a] : lo[a];
+                hi[a] = b.hi[a] > hi[a] ? b.hi[a] : hi[a];
+            }
+        }
+        void grow(const float* p) {
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = p[a] < lo[a] ? p[a] : lo[a];
+                hi[a] = p[a] > hi[a] ? p[a] : hi[a];
+            }
+        }
+        float area() const {
+            if (!(hi[0] >= lo[0])) return 0.0f;
+            const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+            return dx * dy + dy * dz + dz * dx;
+        }
+    };
+    std::vector<Box> tb;          // triangle boxes
+    std::vector<float> cen;       // centroids, 3 per triangle
+    std::vector<int> idx;
+    std::vector<rc_bvh_node> nodes;
+
+    void set_node(int ni, const Box& b) {
+        for (int a = 0; a < 3; ++a) {
+            nodes[ni].aabb_min[a] = b.lo[a];
+            nodes[ni].aabb_max[a] = b.hi[a];
+        }
+    }
+
+    void build(int ni, int begin, int end) {
+        Box nb, cb;
+        for (int i = begin; i < end; ++i) {
+            nb.grow(tb[idx[i]]);
+            cb.grow(&cen[3 * (size_t)idx[i]]);
+        }
+        set_node(ni, nb);
+        const int n = end - begin;
+        auto leaf = [&] {
+            nodes[ni].left_child = nodes[ni].right_child = -1;
+            nodes[ni].prim_start = begin;
+            nodes[ni].prim_count = n;
+        };
+        if (n <= 2) return leaf();
+        int axis = 0;
+        float ext = cb.hi[0] - cb.lo[0];
+        for (int a = 1; a < 3; ++a)
+            if (cb.hi[a] - cb.lo[a] > ext) {
+                ext = cb.hi[a] - cb.lo[a];
+                axis = a;
+            }
+        int mid = begin + n / 2;
+        if (ext > 0.0f) {
+            constexpr int kBins = 16;
+            int best = -1;
+            float best_cost = INFINITY, scale = 0.0f;
+            // one pass bins every axis
+            Box bb[3][kBins];
+            int bc[3][kBins] = {};
+            float sa[3];
+            for (int a = 0; a < 3; ++a) {
+                const float ea = cb.hi[a] - cb.lo[a];
+                sa[a] = ea > 0.0f ? kBins / ea : 0.0f;
+            }
+            for (int i = begin; i < end; ++i) {
+                const int t = idx[i];
+                const float* c = &cen[3 * (size_t)t];
+                for (int a = 0; a < 3; ++a) {
+                    int b = (int)((c[a] - cb.lo[a]) * sa[a]);
+                    b = b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+                    bb[a][b].grow(tb[t]);
+                    ++bc[a][b];
+                }
+            }
+            for (int a = 0; a < 3; ++a) {
+                if (!(sa[a] > 0.0f)) continue;
+                float right_area[kBins];
+                int right_count[kBins];
+                Box acc;
+                int cnt = 0;
+                for (int b = kBins - 1; b > 0; --b) {
+                    acc.grow(bb[a][b]);
+                    cnt += bc[a][b];
+                    right_area[b] = acc.area();
+                    right_count[b] = cnt;
+                }
+                Box left;
+                int lc = 0;
+                for (int b = 1; b < kBins; ++b) {
+                    left.grow(bb[a][b - 1]);
+                    lc += bc[a][b - 1];
+                    if (lc == 0 || right_count[b] == 0) continue;
+                    const float cost = left.area() * lc + right_area[b] * right_count[b];
+                    if (cost < best_cost) {
+                        best_cost = cost;
+                        best = b;
+                        axis = a;
+                        scale = sa[a];
+                    }
+                }
+            }
+            auto bin_of = [&](int t) {
+                const int b = (int)((cen[3 * (size_t)t + axis] - cb.lo[axis]) * scale);
+                return b < 0 ? 0 : (b >= kBins ? kBins - 1 : b);
+            };
+            // traversal cost ~ one triangle test: split when it beats testing all
+            if (best < 0 || (n <= 4 && best_cost >= nb.area() * (n - 1))) {
+                if (n <= 4) return leaf();
+            } else {
+                int* p = std::partition(idx.data() + begin, idx.data() + end, [&](int t) { return bin_of(t) < best; });
+                mid = (int)(p - idx.data());
+            }
+        } else if (n <= 4) {
+            return leaf();
+        }
+        if (mid <= begin || mid >= end) mid = begin + n / 2;
+        const int l = (int)nodes.size();
+        nodes.emplace_back();
+        nodes.emplace_back();
+        nodes[ni].left_child = l;
+        nodes[ni].right_child = l + 1;
+        nodes[ni].prim_start = 0;
+        nodes[ni].prim_count = 0;
+        build(l, begin, mid);
+        build(l + 1, mid, end);
+    }
+};
+
 static bool build_subset(const std::vector<rc_triangle>& in, int scene_tris, SubsetBvh& out) {
     const int n = (int)in.size();
+    if (n == 0) return false;
+    BinnedBuilder B;
+    B.tb.resize(n);
+    B.cen.resize(3 * (size_t)n);
+    B.idx.resize(n);
+    for (int i = 0; i < n; ++i) {
+        B.tb[i].grow(in[i].v0);
+        B.tb[i].grow(in[i].v1);
+        B.tb[i].grow(in[i].v2);
+        for (int a = 0; a < 3; ++a) B.cen[3 * (size_t)i + a] = (in[i].v0[a] + in[i].v1[a] + in[i].v2[a]) * (1.0f / 3.0f);
+        B.idx[i] = i;
+    }
+    B.nodes.reserve(2 * (size_t)n);
+    B.nodes.emplace_back();
+    B.build(0, 0, n);
     std::vector<rc_triangle> tris(n);
-    std::vector<rc_bvh_node> nodes(2 * (size_t)n + 1);
-    int nn = 0;
-    if (n == 0 || rc_build_bvh(in.data(), n, tris.data(), nodes.data(), (int)nodes.size(), &nn) != RC_OK || nn < 1)
-        return false;
+    for (int i = 0; i < n; ++i) tris[i] = in[B.idx[i]];
+    const std::vector<rc_bvh_node>& nodes = B.nodes;
+    const int nn = (int)nodes.size();
     out.recs.assign(nn, NodeRec{});
     out.max_leaf = 0;
     for (int i = 0; i < nn; ++i) {
@@ -653,15 +808,29 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     //      the specular (metal or glass) triangles and over the others ----
     ctx->photon_split = false;
     if (tri_count > 0 && tri_count <= kSplitMaxTris && light_count > 0) {
-        std::vector<rc_triangle> spec, diff;
+        std::vector<char> is_spec(tri_count), is_diff(tri_count);
+        int n_spec = 0;
         for (int i = 0; i < tri_count; ++i) {
             const rc_material& m = mats[tris[i].mat_index];
-            rc_triangle t = tris[i];
-            memcpy(&t.pad6, &i, sizeof(int));
-            (m.metallic > 0.5f || m.transmission > 0.5f ? spec : diff).push_back(t);
+            is_spec[i] = m.metallic > 0.5f || m.transmission > 0.5f;
+            is_diff[i] = !is_spec[i];
+            n_spec += is_spec[i];
         }
+        auto make = [&](const std::vector<char>& keep, int count, SubsetBvh& out) {
+            std::vector<rc_triangle> sub;
+            sub.reserve(count);
+            for (int i = 0; i < tri_count; ++i) {
+                if (!keep[i]) continue;
+                rc_triangle t = tris[i];
+                memcpy(&t.pad6, &i, sizeof(int));
+                sub.push_back(t);
+            }
+            return build_subset(sub, tri_count, out);
+        };
         SubsetBvh sb, db;
-        if (!spec.empty() && !diff.empty() && build_subset(spec, tri_count, sb) && build_subset(diff, tri_count, db)) {
+        const bool built = n_spec > 0 && n_spec < tri_count && make(is_spec, n_spec, sb) &&
+                           make(is_diff, tri_count - n_spec, db);
+        if (built) {
             CK(ensure(ctx->sp_nodes, sb.recs.size() * sizeof(NodeRec)));
             CK(ensure(ctx->sp_isect, sb.isect.size() * sizeof(float4)));
             CK(ensure(ctx->sp_orig, sb.orig.size() * sizeof(int)));
