@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "device_scene.h"
@@ -692,6 +693,41 @@ int rc_get_kernel_times(rc_ctx* ctx, double* ms_out, uint64_t* launches_out) {
 // host SAH builds at upload).
 static const int kSplitMaxTris = 1 << 18;
 
+// The photon trace's first-segment split (fast build): BVHs over the
+// specular (metal or glass) triangles and over the others, each triangle's
+// scene index kept.  Host work only, on the caller's arrays.
+static bool build_split(const rc_triangle* tris, int tri_count, const rc_material* mats, SubsetBvh& sb,
+                        SubsetBvh& db) {
+    std::vector<char> is_spec(tri_count);
+    int n_spec = 0;
+    for (int i = 0; i < tri_count; ++i) {
+        const rc_material& m = mats[tris[i].mat_index];
+        is_spec[i] = m.metallic > 0.5f || m.transmission > 0.5f;
+        n_spec += is_spec[i];
+    }
+    if (n_spec == 0 || n_spec == tri_count) return false;
+    auto make = [&](bool spec, int count, SubsetBvh& out) {
+        std::vector<rc_triangle> sub;
+        sub.reserve(count);
+        for (int i = 0; i < tri_count; ++i) {
+            if ((is_spec[i] != 0) != spec) continue;
+            rc_triangle t = tris[i];
+            memcpy(&t.pad6, &i, sizeof(int));
+            sub.push_back(t);
+        }
+        return build_subset(sub, tri_count, out);
+    };
+    return make(true, n_spec, sb) && make(false, tri_count - n_spec, db);
+}
+
+// Joins a helper thread on every way out of the scope.
+struct JoinOnExit {
+    std::thread t;
+    ~JoinOnExit() {
+        if (t.joinable()) t.join();
+    }
+};
+
 int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const rc_bvh_node* nodes,
                     int node_count, const rc_material* mats, int material_count, const rc_light* lights,
                     int light_count, float total_light_power) {
@@ -730,6 +766,13 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     for (int i = 0; i < tri_count; ++i)
         if (tris[i].mat_index < 0 || tris[i].mat_index >= material_count)
             return fail(ctx, RC_ERR_BAD_SCENE, "triangle %d: material %d out of range", i, tris[i].mat_index);
+    // the photon-split BVHs build on a helper thread while the rest of the
+    // upload converts and copies
+    const bool want_split = tri_count > 0 && tri_count <= kSplitMaxTris && light_count > 0;
+    SubsetBvh sb, db;
+    bool built = false;
+    JoinOnExit split_job;
+    if (want_split) split_job.t = std::thread([&] { built = build_split(tris, tri_count, mats, sb, db); });
     // ---- convert to the kernels' layout ----
     std::vector<NodeRec> recs(node_count);
     memset(recs.data(), 0, recs.size() * sizeof(NodeRec));
@@ -807,29 +850,8 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     // ---- first-segment split of the photon trace (fast build): BVHs over
     //      the specular (metal or glass) triangles and over the others ----
     ctx->photon_split = false;
-    if (tri_count > 0 && tri_count <= kSplitMaxTris && light_count > 0) {
-        std::vector<char> is_spec(tri_count), is_diff(tri_count);
-        int n_spec = 0;
-        for (int i = 0; i < tri_count; ++i) {
-            const rc_material& m = mats[tris[i].mat_index];
-            is_spec[i] = m.metallic > 0.5f || m.transmission > 0.5f;
-            is_diff[i] = !is_spec[i];
-            n_spec += is_spec[i];
-        }
-        auto make = [&](const std::vector<char>& keep, int count, SubsetBvh& out) {
-            std::vector<rc_triangle> sub;
-            sub.reserve(count);
-            for (int i = 0; i < tri_count; ++i) {
-                if (!keep[i]) continue;
-                rc_triangle t = tris[i];
-                memcpy(&t.pad6, &i, sizeof(int));
-                sub.push_back(t);
-            }
-            return build_subset(sub, tri_count, out);
-        };
-        SubsetBvh sb, db;
-        const bool built = n_spec > 0 && n_spec < tri_count && make(is_spec, n_spec, sb) &&
-                           make(is_diff, tri_count - n_spec, db);
+    if (want_split) {
+        split_job.t.join();
         if (built) {
             CK(ensure(ctx->sp_nodes, sb.recs.size() * sizeof(NodeRec)));
             CK(ensure(ctx->sp_isect, sb.isect.size() * sizeof(float4)));
