@@ -417,10 +417,13 @@ struct BinnedBuilder {
             return dx * dy + dy * dz + dz * dx;
         }
     };
-    std::vector<Box> tb;          // triangle boxes
-    std::vector<float> cen;       // centroids, 3 per triangle
-    std::vector<int> idx;
+    const std::vector<Box>& tb;   // triangle boxes
+    const std::vector<float>& cen;  // centroids, 3 per triangle
+    std::vector<int>& idx;        // triangle order; a builder owns a range of it
     std::vector<rc_bvh_node> nodes;
+
+    BinnedBuilder(const std::vector<Box>& t, const std::vector<float>& c, std::vector<int>& i)
+        : tb(t), cen(c), idx(i) {}
 
     void set_node(int ni, const Box& b) {
         for (int a = 0; a < 3; ++a) {
@@ -429,7 +432,9 @@ struct BinnedBuilder {
         }
     }
 
-    void build(int ni, int begin, int end) {
+    // `spawn` levels below this one build their right subtree on a thread
+    // of its own (into its own node array, appended afterwards).
+    void build(int ni, int begin, int end, int spawn) {
         Box nb, cb;
         for (int i = begin; i < end; ++i) {
             nb.grow(tb[idx[i]]);
@@ -522,30 +527,51 @@ struct BinnedBuilder {
         nodes[ni].right_child = l + 1;
         nodes[ni].prim_start = 0;
         nodes[ni].prim_count = 0;
-        build(l, begin, mid);
-        build(l + 1, mid, end);
+        if (spawn <= 0 || n < 4096) {
+            build(l, begin, mid, 0);
+            build(l + 1, mid, end, 0);
+            return;
+        }
+        BinnedBuilder right(tb, cen, idx);
+        right.nodes.reserve(2 * (size_t)(end - mid));
+        right.nodes.emplace_back();
+        std::thread job([&] { right.build(0, mid, end, spawn - 1); });
+        build(l, begin, mid, spawn - 1);
+        job.join();
+        // the right subtree's root takes slot l + 1, its other nodes follow
+        const int base = (int)nodes.size() - 1;
+        auto place = [&](int j) { return j == 0 ? l + 1 : base + j; };
+        for (size_t j = 0; j < right.nodes.size(); ++j) {
+            rc_bvh_node m = right.nodes[j];
+            if (m.prim_count <= 0) {
+                m.left_child = place(m.left_child);
+                m.right_child = place(m.right_child);
+            }
+            if (j == 0) nodes[l + 1] = m;
+            else nodes.push_back(m);
+        }
     }
 };
 
 static bool build_subset(const std::vector<rc_triangle>& in, int scene_tris, SubsetBvh& out) {
     const int n = (int)in.size();
     if (n == 0) return false;
-    BinnedBuilder B;
-    B.tb.resize(n);
-    B.cen.resize(3 * (size_t)n);
-    B.idx.resize(n);
+    std::vector<BinnedBuilder::Box> tb(n);
+    std::vector<float> cen(3 * (size_t)n);
+    std::vector<int> idx(n);
     for (int i = 0; i < n; ++i) {
-        B.tb[i].grow(in[i].v0);
-        B.tb[i].grow(in[i].v1);
-        B.tb[i].grow(in[i].v2);
-        for (int a = 0; a < 3; ++a) B.cen[3 * (size_t)i + a] = (in[i].v0[a] + in[i].v1[a] + in[i].v2[a]) * (1.0f / 3.0f);
-        B.idx[i] = i;
+        tb[i].grow(in[i].v0);
+        tb[i].grow(in[i].v1);
+        tb[i].grow(in[i].v2);
+        for (int a = 0; a < 3; ++a) cen[3 * (size_t)i + a] = (in[i].v0[a] + in[i].v1[a] + in[i].v2[a]) * (1.0f / 3.0f);
+        idx[i] = i;
     }
+    BinnedBuilder B(tb, cen, idx);
     B.nodes.reserve(2 * (size_t)n);
     B.nodes.emplace_back();
-    B.build(0, 0, n);
+    B.build(0, 0, n, 2);   // up to four subtrees at once
     std::vector<rc_triangle> tris(n);
-    for (int i = 0; i < n; ++i) tris[i] = in[B.idx[i]];
+    for (int i = 0; i < n; ++i) tris[i] = in[idx[i]];
     const std::vector<rc_bvh_node>& nodes = B.nodes;
     const int nn = (int)nodes.size();
     out.recs.assign(nn, NodeRec{});
