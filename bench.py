@@ -13,18 +13,31 @@ of export/RenderPipeline.java:209-239, issued through rc_render_frame.
          staging), the frame, the display pass (rc_display: ACES + sRGB to
          RGBA8, RenderPipeline.applyDisplayPass) and the read-back of that
          RGBA8 image (device -> host, FrameExporter) are inside the timed region
-  roofline  the dominant kernel (render_kernel): algorithmic bytes per launch
-         from the kernel's own work counters, divided by its CUDA-event time
+  roofline  the dominant kernel (the wavefront trace): algorithmic bytes per
+         launch from the kernel's own work counters (32 B per box test, 36 B
+         per triangle test), divided by its CUDA-event time, against the
+         measured HBM copy bandwidth; `bound` and `limiter` come from the
+         committed ncu summary of the same kernel (the scene is cache-resident,
+         so the kernel is issue-bound, not HBM-bound), `traffic` its DRAM
+         bytes per launch
+  exact_math  the same frame in the bit-exact build, and how many pixels of
+         the fast build agree with it within 1e-4 at 1 spp
+  cornell_small  the small Cornell box (256x256 x 16 spp) on the B200
+  time_to_relmse  the metric's second half (64 held-out Cornell variants,
+         every integer spp to 16, a 5x5 box filter as control); one GPU only
   cpu_baseline  the reference's own shaders compiled for the host
          (oracle/_ref, OpenMP over all host cores) on a bounded sample of the
-         same workload, extrapolated to a full frame
+         same workload: 1/16 of the frame (its centre eighth of rows at half
+         the spp, with the SPPM and à-trous work in proportion), timed whole
 
 Multi-GPU: one process per GPU (torchrun); each rank renders its own frame
 (independent replicas, no collective on the data path); timing is the max over
 ranks and value counts the samples of all ranks (weak scaling).
 
 `--impl reference` times the reference's own CPU shaders on this host and
-prints the same line with "impl": "reference" (rank 0 only).
+prints the same line with "impl": "reference" (rank 0 only): each step is
+the 1/16 sample above, timed whole; the line adds the same sample with the
+host C library's transcendental functions and a whole small-Cornell frame.
 """
 from __future__ import annotations
 
@@ -60,22 +73,32 @@ KERNEL_SYMBOL = {"render": "render_kernel", "wf_trace": "wf_trace", "wf_shade": 
 
 
 def algorithmic_bytes(kernel: str, ctr: dict, samples: int) -> float:
-    """Bytes the kernel must move at minimum for the work its counters record:
-    32 B per ray-box test (6 floats + 2 ints), 36 B per ray-triangle test
-    (v0, e1, e2), 104 B per shaded hit (3 normals + material index + the 64-B
-    material), 80 B per light record, 20 B per pixel sample (accum + variance
-    read-modify-write), and for the wavefront stages the path state they must
-    read and write (48 B per closest-hit ray, 96 B per shadow ray)."""
+    """Bytes the kernel must move at minimum for the work its counters record,
+    in the path's own units: 32 B per ray-box test (6 floats + 2 ints), 36 B
+    per ray-triangle test (v0, e1, e2), 104 B per shaded hit (3 normals +
+    material index + the 64-B material), 80 B per light record, 20 B per
+    pixel sample (accum + variance read-modify-write).  The wavefront's own
+    path-state traffic (a design choice, not the algorithm's) is reported
+    apart by `state_bytes`."""
     trav = BYTES_NODE_TEST * ctr["node_tests"] + BYTES_TRI_TEST * ctr["tri_tests"]
     if kernel == "render":
         return (trav + BYTES_SURFACE_HIT * ctr["surface_hits"] + BYTES_LIGHT_SAMPLE * ctr["light_samples"]
                 + BYTES_SAMPLE_RMW * samples)
     if kernel == "wf_trace":
-        return trav + 48 * ctr["closest_rays"] + 96 * ctr["shadow_rays"]
+        return trav
     if kernel == "wf_shade":
         return (BYTES_SURFACE_HIT + 160) * ctr["surface_hits"] + BYTES_LIGHT_SAMPLE * ctr["light_samples"]
     if kernel in ("photon_trace", "photon_gather"):
         return BYTES_NODE_TEST * ctr["photon_node_tests"] + BYTES_TRI_TEST * ctr["photon_tri_tests"]
+    return 0.0
+
+
+def state_bytes(kernel: str, ctr: dict) -> float:
+    """Path state the wavefront trace reads and writes per ray (origin and
+    direction in, hit record out: 48 B per closest ray; shadow record in,
+    radiance read-modify-write: 96 B per shadow ray)."""
+    if kernel == "wf_trace":
+        return 48 * ctr["closest_rays"] + 96 * ctr["shadow_rays"]
     return 0.0
 
 
@@ -119,8 +142,8 @@ def parse_args(argv=None):
     ap.add_argument("--chunk-paths", type=int, default=0, help="wavefront paths in flight (0: default)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the time-to-relMSE comparison")
-    ap.add_argument("--quality-variants", type=int, default=8, help="held-out Cornell variants for time-to-relMSE")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--quality-variants", type=int, default=64, help="held-out Cornell variants for time-to-relMSE")
+    ap.add_argument("--no-exact", action="store_true", help="skip the exact-math line")
     ap.add_argument("--spp", type=int, default=0, help="override spp (profiling of a small case)")
     ap.add_argument("--sppm-iterations", type=int, default=-1, help="override SPPM iterations")
     return ap.parse_args(argv)
@@ -233,19 +256,27 @@ def workload_setup(name, args=None):
     return w, sppm, atrous
 
 
-def read_traffic(kernel: str, workload: str):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary
-    (profiles/ncu_<kernel>_<workload>.md, line 'traffic_bytes_per_launch: N')."""
+PROFILE_FIELDS = ("traffic_bytes_per_launch", "bound", "simt_efficiency", "issue_active", "dram_throughput",
+                  "l1_hit_rate", "warps_active")
+
+
+def read_profile(kernel: str, workload: str) -> dict:
+    """The machine-readable lines ('key: value') of the committed ncu summary
+    profiles/ncu_<kernel>_<workload>.md: DRAM bytes per launch and the
+    limiter counters of the same kernel."""
     path = os.path.join(REPO, "profiles", f"ncu_{kernel}_{workload}.md")
+    out = {}
     if not os.path.exists(path):
-        return None
+        return out
     for line in open(path):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        key, _, val = line.strip().partition(":")
+        if key in PROFILE_FIELDS and val.strip():
+            v = val.strip().split()[0]
             try:
-                return float(line.split(":", 1)[1].strip().split()[0])
+                out[key] = float(v)
             except ValueError:
-                return None
-    return None
+                out[key] = v
+    return out
 
 
 def hbm_peak():
@@ -260,94 +291,134 @@ def hbm_peak():
 # ---------------------------------------------------------------------------
 # CPU baseline: the reference shaders compiled for the host (oracle/_ref)
 # ---------------------------------------------------------------------------
-def cpu_reference_sample(w, budget_s: float, threads: int = 0):
-    """Times the reference's own shaders (pathtrace, photon trace, gather,
-    à-trous) on a bounded sample of the workload on all host cores and
-    extrapolates the time of one full frame.  Returns (frame_seconds, info)."""
+class ReferenceFrame:
+    """A bounded sample of a workload on the reference's own shaders compiled
+    for the host (oracle/_ref; the oracle's restatement where that library
+    is absent), OpenMP over the host's cores: the frame restricted to its
+    `H/8` centre rows and `spp/2` samples -- 1/16 of the frame -- with the
+    SPPM work in the same proportion (one iteration of the full photon count
+    for the export frame's 16 iterations per 128 spp: same hash density and
+    chain lengths) and the à-trous passes over those rows.  Per sample it
+    does the export path's work in its order (trace photons, render the
+    iteration's samples, gather, shrink the radius; denoise), so samples/s
+    of the sample is samples/s of the frame."""
+
+    def __init__(self, w, threads: int = 0, libm: bool = False):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import pyoracle as po
+        from retrocam_b200 import scenes
+        self.po = po
+        self.orc, self.ref = po.load(build=False)
+        if libm:
+            self.ref = po.load_reference_libm()
+            if self.ref is None:
+                raise RuntimeError("oracle/_ref/libretrocam_ref_libm.so is missing")
+        self.kind = "reference" if self.ref is not None else "port"
+        self.w = w
+        self.sc = scenes.build_scene(w.scene, self.orc, po.MAT)
+        self.cam = scenes.camera(w.orbit, w.lens, self.orc)
+        self.cores = threads or os.cpu_count()
+        W, H = w.width, w.height
+        self.rows = max(8, H // 8)
+        self.r0 = H // 2 - self.rows // 2
+        self.spp = max(1, w.spp // 2)
+        self.frac = (self.rows / H) * (self.spp / w.spp)
+        self.iters, self.photons = 0, 0
+        if w.sppm is not None and self.sc["light_count"] > 0:
+            total = w.sppm.photons * w.sppm.iterations * self.frac
+            self.iters = max(1, round(w.sppm.iterations * self.frac))
+            self.photons = int(round(total / self.iters))
+        self.bufs = po.alloc_images(W, H)
+        self.samples = self.rows * W * self.spp
+
+    def describe(self) -> str:
+        w = self.w
+        d = (f"{self.kind} shaders on {self.cores} host threads: {self.rows} centre rows x {w.width} px x "
+             f"{self.spp} spp ({'3 LCA paths' if any(w.lens.lca_delta) else '1 path'} per sample)")
+        if self.iters:
+            d += f", {self.iters} SPPM iteration(s) of {self.photons} photons with the gather over those rows"
+        if w.atrous is not None and w.atrous.enabled:
+            d += f", {w.atrous.iterations} a-trous passes over those rows"
+        return d + f" = 1/{round(1 / self.frac)} of one {w.width}x{w.height}x{w.spp}-spp frame, timed in full"
+
+    def step(self) -> float:
+        """Runs the sample once; returns its wall seconds."""
+        w, sc, cam, ref, orc = self.w, self.sc, self.cam, self.ref, self.orc
+        W, H = w.width, w.height
+        rows = (self.r0, self.r0 + self.rows)
+        settings = (w.nee_enabled, w.nee_firefly_clamp)
+        acc = self.bufs[0]
+        t0 = time.perf_counter()
+        radius = w.sppm.r0 if w.sppm is not None else 0.0
+        blocks = self.iters if self.iters else 1
+        for k in range(blocks):
+            s0, s1 = k * self.spp // blocks, (k + 1) * self.spp // blocks
+            if self.iters:
+                seed = k * 7919 + 6271
+                if ref is not None:
+                    ph, hd, nx, _ = ref.photon_trace(sc, self.photons, radius, seed, w.sppm.hash_size,
+                                                     threads=self.cores)
+                else:
+                    ph, hd, nx, _, _ = orc.photon_trace(sc, self.photons, radius, seed, w.sppm.hash_size,
+                                                        threads=self.cores)
+            for f in range(s0, s1):
+                if ref is not None:
+                    ref.pathtrace(sc, cam, settings, W, H, f, self.bufs, threads=self.cores, rows=rows)
+                else:
+                    orc.render(sc, cam, settings, W, H, f, 1, buffers=self.bufs, rows=rows, threads=self.cores)
+            if self.iters:
+                if ref is not None:
+                    ref.photon_gather(sc, cam, W, H, radius, self.photons, w.sppm.hash_size, 0, ph, hd, nx, acc,
+                                      threads=self.cores, rows=rows)
+                else:
+                    orc.photon_gather(sc, cam, W, H, radius, w.sppm.hash_size, ph, hd, nx, acc,
+                                      threads=self.cores)
+                radius = orc.lib.or_sppm_next_radius(radius, k, w.sppm.alpha)
+        if w.atrous is not None and w.atrous.enabled:
+            a = orc.p00(acc, W, H, self.spp, w.atrous.exposure)
+            out = np.zeros((H, W, 4), np.float32)
+            for i in range(w.atrous.iterations):
+                if ref is not None:
+                    ref.atrous_pass(a, self.bufs[1], self.bufs[2], self.bufs[3], W, H, 1 << i,
+                                    w.atrous.sigma_color, w.atrous.sigma_normal, w.atrous.sigma_depth, self.spp,
+                                    w.atrous.exposure, out, rows=rows, threads=self.cores)
+                else:
+                    out = orc.atrous_pass(a, self.bufs[1], self.bufs[2], self.bufs[3], W, H, 1 << i,
+                                          w.atrous.sigma_color, w.atrous.sigma_normal, w.atrous.sigma_depth,
+                                          self.spp, w.atrous.exposure, threads=self.cores)
+                a, out = out, a
+        return time.perf_counter() - t0
+
+
+def cpu_full_frame(name: str, threads: int = 0) -> dict:
+    """A whole frame of a small workload on the compiled reference (the
+    small Cornell box: 256x256 x 16 spp, no SPPM, no denoiser), timed once
+    after one untimed frame."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import pyoracle as po
     from retrocam_b200 import scenes
     orc, ref = po.load(build=False)
-    kind = "reference"
-    if ref is None:
-        kind = "port"
+    w = scenes.WORKLOADS[name]()
     sc = scenes.build_scene(w.scene, orc, po.MAT)
     cam = scenes.camera(w.orbit, w.lens, orc)
-    W, H, spp = w.width, w.height, w.spp
     cores = threads or os.cpu_count()
-    bufs = po.alloc_images(W, H)
     settings = (w.nee_enabled, w.nee_firefly_clamp)
 
-    def render_rows(rows, frame):
+    def frame():
+        bufs = po.alloc_images(w.width, w.height)
+        t0 = time.perf_counter()
         if ref is not None:
-            ref.pathtrace(sc, cam, settings, W, H, frame, bufs, threads=cores, rows=rows)
+            ref.render(sc, cam, settings, w.width, w.height, 0, w.spp, buffers=bufs, threads=cores)
         else:
-            orc.render(sc, cam, settings, W, H, frame, 1, buffers=bufs, rows=rows, threads=cores)
+            orc.render(sc, cam, settings, w.width, w.height, 0, w.spp, buffers=bufs, threads=cores)
+        return time.perf_counter() - t0
 
-    # path tracer: grow the row count until ~40% of the budget is spent
-    render_rows((0, 16), 0)  # frame 0 (writes the G-buffer); warm
-    rows, t = 16, 0.0
-    while True:
-        t0 = time.perf_counter()
-        render_rows((H // 2 - rows // 2, H // 2 + rows // 2), 1)
-        t = time.perf_counter() - t0
-        if t > 0.4 * budget_s / 2 or rows >= H:
-            break
-        rows = min(H, rows * 2)
-    t_sample = t / (rows * W)             # seconds per pixel-sample (centre rows)
-    t_render = t_sample * W * H * spp
-    info = {"render_rows": rows, "render_s": t}
-    t_frame = t_render
-    if w.sppm is not None and sc["light_count"] > 0:
-        n_ph = 50_000
-        while True:
-            t0 = time.perf_counter()
-            if ref is not None:
-                ph, hd, nx, cnt = ref.photon_trace(sc, n_ph, w.sppm.r0, 6271, w.sppm.hash_size, threads=cores)
-            else:
-                ph, hd, nx, cnt, _ = orc.photon_trace(sc, n_ph, w.sppm.r0, 6271, w.sppm.hash_size, threads=cores)
-            tp = time.perf_counter() - t0
-            if tp > 0.15 * budget_s / 2 or n_ph >= w.sppm.photons:
-                break
-            n_ph = min(w.sppm.photons, n_ph * 4)
-        t_trace = tp / n_ph * w.sppm.photons * w.sppm.iterations
-        g_rows = max(8, rows // 2)
-        t0 = time.perf_counter()
-        if ref is not None:
-            ref.photon_gather(sc, cam, W, H, w.sppm.r0, n_ph, w.sppm.hash_size, 0, ph, hd, nx, bufs[0],
-                              threads=cores, rows=(H // 2 - g_rows // 2, H // 2 + g_rows // 2))
-        else:
-            orc.photon_gather(sc, cam, W, H, w.sppm.r0, w.sppm.hash_size, ph, hd, nx, bufs[0], threads=cores)
-            g_rows = H
-        tg = time.perf_counter() - t0
-        t_gather = tg / (g_rows * W) * W * H * w.sppm.iterations
-        t_frame += t_trace + t_gather
-        info.update({"photons": n_ph, "photon_s": tp, "gather_rows": g_rows, "gather_s": tg})
-    if w.atrous is not None and w.atrous.enabled:
-        a_rows = max(8, rows // 2)
-        out = np.zeros((H, W, 4), np.float32)
-        col = orc.p00(bufs[0], W, H, 1, 1.0)
-        t0 = time.perf_counter()
-        if ref is not None:
-            ref.atrous_pass(col, bufs[1], bufs[2], bufs[3], W, H, 16, w.atrous.sigma_color, w.atrous.sigma_normal,
-                            w.atrous.sigma_depth, 1, 1.0, out, rows=(H // 2 - a_rows // 2, H // 2 + a_rows // 2),
-                            threads=cores)
-        else:
-            orc.atrous_pass(col, bufs[1], bufs[2], bufs[3], W, H, 16, w.atrous.sigma_color, w.atrous.sigma_normal,
-                            w.atrous.sigma_depth, 1, 1.0, threads=cores)
-            a_rows = H
-        ta = time.perf_counter() - t0
-        t_frame += ta / (a_rows * W) * W * H * w.atrous.iterations
-        info.update({"atrous_rows": a_rows, "atrous_s": ta})
-    desc = (f"{kind} shaders on {cores} host threads: pathtrace {rows} centre rows x {W} px x 1 spp "
-            f"({'3 LCA paths/sample' if any(w.lens.lca_delta) else '1 path/sample'})")
-    if "photons" in info:
-        desc += f"; photon trace {info['photons']} photons; gather {info['gather_rows']} rows"
-    if "atrous_rows" in info:
-        desc += f"; a-trous {info['atrous_rows']} rows x 1 pass"
-    desc += f"; extrapolated to {W}x{H}x{spp} spp" + (
-        f" + {w.sppm.iterations} SPPM iterations" if w.sppm is not None else "") + " + full denoise"
-    return t_frame, {"kind": kind, "cores": cores, "sample": desc, "detail": info}
+    frame()
+    t = frame()
+    n = w.width * w.height * w.spp
+    return {"workload": name, "value": n / t / 1e6, "unit": UNIT, "ms_per_frame": t * 1e3, "samples": n,
+            "kind": "reference" if ref is not None else "port", "cores": cores,
+            "sample": f"the whole {w.width}x{w.height}x{w.spp}-spp frame"}
 
 
 # ---------------------------------------------------------------------------
@@ -358,41 +429,62 @@ def run_reference(args):
     if rank != 0:
         return 0
     w, _, _ = workload_setup(args.workload, args)
-    samples = w.width * w.height * w.spp
-    budget = max(2.0, min(args.cpu_seconds, 240.0 / max(1, args.steps + args.warmup)))
+    rf = ReferenceFrame(w)
     for _ in range(args.warmup):
-        cpu_reference_sample(w, budget)
-    times, info = [], None
-    for _ in range(args.steps):
-        t, info = cpu_reference_sample(w, budget)
-        times.append(t)
-    t_frame = statistics.mean(times)
-    value = samples / t_frame / 1e6
+        rf.step()
+    times = [rf.step() for _ in range(args.steps)]
+    t = statistics.mean(times)
+    value = rf.samples / t / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_frame * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "config": workload_config(w, args),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
-                             "sample": info["sample"]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": rf.cores, "kind": rf.kind,
+                             "sample": rf.describe()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        lm = ReferenceFrame(w, libm=True)
+        lm.step()
+        tl = statistics.mean(lm.step() for _ in range(min(3, args.steps)))
+        line["host_libm"] = {"value": lm.samples / tl / 1e6, "unit": UNIT, "ms_per_step": tl * 1e3,
+                             "sample": "the same sample on the reference shaders built with the host C "
+                                       "library's sinf/cosf/expf/logf/powf (a GL driver would use its own "
+                                       "fast functions) instead of the correctly rounded ones parity uses"}
+    except RuntimeError as e:
+        line["host_libm"] = {"unavailable": str(e)}
+    if w.name != "cornell_small":
+        line["cornell_small_full_frame"] = cpu_full_frame("cornell_small")
     print(json.dumps(line))
     return 0
+
+
+# every integer spp up to 16 (the plain path crosses 1e-2 between 8 and 16),
+# then the octaves above
+QUALITY_SPPS = tuple(range(1, 17)) + (32, 64)
 
 
 def time_to_relmse(args) -> dict:
     """The metric's second half: wall time (render + denoise, one frame at
     854x480) to reach mean relMSE <= 1e-2 against a 4096-spp render, path
     tracer + à-trous vs path tracer + the shipped learned denoiser, on
-    held-out seeded Cornell variants (no dataset exists for this scene)."""
+    held-out seeded Cornell variants (no dataset exists for this scene), at
+    every integer spp from 1 to 16.  A plain 5x5 box average of the noisy
+    image is evaluated beside them as a control."""
     from retrocam_b200 import kpcnn
     seeds = list(range(5000, 5000 + args.quality_variants))
-    rep = kpcnn.evaluate(kpcnn.load(), seeds, spps=(1, 2, 4, 8, 16, 32, 64), ref_spp=4096, log=None)
+    rep = kpcnn.evaluate(kpcnn.load(), seeds, spps=QUALITY_SPPS, ref_spp=4096, log=None)
     t = rep["time_to_threshold"]
-    return {"threshold": rep["threshold"], "ref_spp": rep["ref_spp"], "variants": seeds,
+    box_hit = [s for s, v in zip(rep["spp"], rep["relmse"]["box5"]) if v <= rep["threshold"]]
+    return {"threshold": rep["threshold"], "ref_spp": rep["ref_spp"], "variants": len(seeds),
+            "variant_seeds": [seeds[0], seeds[-1]],
             "plain_atrous": t["atrous"], "learned": t["learned"], "plain_no_denoiser": t["noisy"],
+            "box5_control_spp": box_hit[0] if box_hit else None,
             "learned_speedup": rep["speedup_learned_vs_atrous"],
-            "relmse_at_spp": {"spp": rep["spp"], "atrous": rep["relmse"]["atrous"],
-                              "learned": rep["relmse"]["learned"]}}
+            "relmse_at_spp": {"spp": rep["spp"], "noisy": rep["relmse"]["noisy"],
+                              "atrous": rep["relmse"]["atrous"], "learned": rep["relmse"]["learned"],
+                              "box5": rep["relmse"]["box5"]},
+            "ms_at_spp": {"render": rep["ms"]["render"], "atrous": rep["ms"]["atrous"],
+                          "learned": rep["ms"]["learned"]}}
 
 
 def workload_config(w, args):
@@ -415,6 +507,83 @@ def workload_config(w, args):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def device_timed(step, steps: int, warmup: int, stream) -> float:
+    """Milliseconds per step on `stream` (CUDA events, synchronize on both
+    sides) after `warmup` untimed steps."""
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def exact_math_line(args, w, sc, cam, sppm, atrous, fast_ctx, stream, device) -> dict:
+    """The same frame in the exact build (no contraction, IEEE divide and
+    square root, correctly rounded transcendentals, the reference's
+    traversal order: the oracle's bits, so per-pixel agreement with the
+    reference's shaders at any spp), timed like the headline; and, at 1 spp,
+    how many pixels of the benchmarked fast build agree with it within
+    1e-4 relative."""
+    from retrocam_b200 import api
+    settings = (w.nee_enabled, w.nee_firefly_clamp)
+    iters = w.sppm.iterations if w.sppm is not None else 0
+    r0 = w.sppm.r0 if w.sppm is not None else 0.05
+    with api.Context(w.width, w.height, device.index, api.RC_MATH_EXACT) as ex:
+        ex.set_stream(stream.cuda_stream)
+        ex.upload(sc)
+        steps = max(1, min(args.steps, 5))
+        ms = device_timed(lambda: ex.render_frame(cam, settings, w.spp, sppm, r0, iters, atrous, read=False),
+                          steps, max(3, min(args.warmup, 3)), stream)
+        if ex.counters()["error_word"]:
+            raise RuntimeError("kernel guard raised in the exact build")
+        ex.reset()
+        ex.render(cam, settings, 0, 1)
+        a_ex = ex.read_buffers()[0]
+        tuning = ex.tuning()
+    fast_ctx.reset()
+    fast_ctx.render(cam, settings, 0, 1)
+    a_fa = fast_ctx.read_buffers()[0]
+    rel = np.abs(a_fa[..., :3] - a_ex[..., :3]) / np.maximum(np.abs(a_ex[..., :3]), 1e-3)
+    within = np.all(rel <= 1e-4, axis=-1)
+    return {"value": w.width * w.height * w.spp / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms,
+            "steps": steps, "engine": tuning["engine"],
+            "fast_vs_exact_1spp": {"pixels_within_1e-4_rel": float(within.mean()),
+                                   "pixels_bit_identical": float(np.all(a_fa[..., :3].view(np.uint32) ==
+                                                                        a_ex[..., :3].view(np.uint32),
+                                                                        axis=-1).mean()),
+                                   "image_mean_rel_diff": float(abs(a_fa[..., :3].mean() - a_ex[..., :3].mean()) /
+                                                                a_ex[..., :3].mean())}}
+
+
+def small_cornell_line(args, stream, device) -> dict:
+    """The small Cornell box (256x256, 16 spp, no SPPM, no denoiser) on the
+    B200, device-resident, autotuned shape; the reference arm times the
+    same whole frame on the host."""
+    from retrocam_b200 import api, autotune, scenes
+    w = scenes.cornell_small()
+    sc = api.build_scene(w.scene)
+    cam = api.workload_camera(w)
+    settings = (w.nee_enabled, w.nee_firefly_clamp)
+    with api.Context(w.width, w.height, device.index, api.RC_MATH_FAST) as c:
+        c.set_stream(stream.cuda_stream)
+        c.upload(sc)
+        import torch
+        key = autotune.cache_key(torch.cuda.get_device_name(device), w.width, w.height, api.RC_MATH_FAST,
+                                 autotune.scene_signature(sc))
+        t = autotune.TuningCache().get(key)
+        if t:
+            c.set_tuning(**t)
+        ms = device_timed(lambda: c.render(cam, settings, 0, w.spp), max(args.steps, 10), max(args.warmup, 3), stream)
+    return {"value": w.width * w.height * w.spp / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_frame": ms,
+            "config": "256x256, 16 spp, 6 bounces, 35 mm f/16, 36 triangles"}
+
+
 def run_b200(args):
     import torch
     from retrocam_b200 import api, build
@@ -516,20 +685,27 @@ def run_b200(args):
     avg_launch_s = (k_ms / max(1, k_launches)) / 1e3
     peak, peak_kind = hbm_peak()
     achieved = per_launch_bytes / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
-    traffic = read_traffic(KERNEL_SYMBOL.get(kernel, kernel), w.name)
+    prof = read_profile(KERNEL_SYMBOL.get(kernel, kernel), w.name)
+    traffic = prof.get("traffic_bytes_per_launch")
     fp32 = fp32_roofline(kernel, ctr, k_launches, avg_launch_s, local_rank)
     rays = ctr["closest_rays"] + ctr["shadow_rays"] + ctr["photon_rays"] + ctr["gather_rays"]
     kernels_total_ms = sum(v[0] for v in ktimes.values())
+    roofline = {"bound": prof.get("bound", "hbm"), "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                "kernel": KERNEL_SYMBOL.get(kernel, kernel), "algorithmic_bytes_per_launch": per_launch_bytes,
+                "state_bytes_per_launch": state_bytes(kernel, ctr) / max(1, k_launches),
+                "traffic_over_algorithmic": (traffic / per_launch_bytes) if traffic and per_launch_bytes else None,
+                "avg_launch_ms": avg_launch_s * 1e3, "launches": k_launches,
+                "limiter": {k: prof[k] for k in ("simt_efficiency", "issue_active", "dram_throughput",
+                                                 "l1_hit_rate", "warps_active") if k in prof},
+                "fp32": fp32}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, no dataset)",
         "config": dict(workload_config(w, args), tuning=tuning),
         "e2e": e2e,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": KERNEL_SYMBOL.get(kernel, kernel), "algorithmic_bytes_per_launch": per_launch_bytes,
-                     "avg_launch_ms": avg_launch_s * 1e3, "launches": k_launches, "fp32": fp32},
+        "roofline": roofline,
         "mrays_per_s": rays / (t_ms / 1e3) / 1e6,
         "kernel_ms": {k: v[0] / args.steps for k, v in ktimes.items()},
         "kernel_share": {k: (v[0] / kernels_total_ms if kernels_total_ms else 0.0) for k, v in ktimes.items()},
@@ -539,12 +715,18 @@ def run_b200(args):
                               ("camera_paths", "closest_rays", "shadow_rays", "photon_rays", "gather_rays",
                                "node_tests", "tri_tests", "surface_hits", "light_samples")},
     }
-    if rank == 0 and not args.no_quality:
+    if world == 1 and not args.no_exact:
+        line["exact_math"] = exact_math_line(args, w, sc, cam, sppm, atrous, ctx, stream, device)
+    if world == 1 and args.workload != "cornell_small":
+        line["cornell_small"] = small_cornell_line(args, stream, device)
+    if rank == 0 and world == 1 and not args.no_quality:
         line["time_to_relmse"] = time_to_relmse(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        t_frame, info = cpu_reference_sample(w, args.cpu_seconds)
-        line["cpu_baseline"] = {"value": samples_per_step / t_frame / 1e6, "unit": UNIT, "cores": info["cores"],
-                                "kind": info["kind"], "sample": info["sample"]}
+        rf = ReferenceFrame(w)
+        rf.step()
+        t_cpu = rf.step()
+        line["cpu_baseline"] = {"value": rf.samples / t_cpu / 1e6, "unit": UNIT, "cores": rf.cores,
+                                "kind": rf.kind, "sample": rf.describe(), "ms": t_cpu * 1e3}
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()

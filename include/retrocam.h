@@ -151,7 +151,10 @@ typedef struct rc_counters {
     uint64_t h2d_bytes;      /* host -> device bytes copied by this context */
     uint64_t d2h_bytes;      /* device -> host bytes copied by this context */
     uint32_t error_word;     /* RC_GUARD_* bits raised by kernels */
-    uint32_t reserved;
+    uint32_t bvh_depth;      /* levels below the root of the uploaded BVH (0: a
+                                leaf root or no scene); past 28 the shadow walk,
+                                past 60 every walk keeps the reference's own
+                                stack policy (its stacks can overflow there) */
 } rc_counters;
 
 /* Kernel kinds for rc_get_kernel_times. */
@@ -350,7 +353,10 @@ int rc_total_samples(const rc_ctx* ctx);
  * SPPM (scene/SPPMManager.java, scene/PhotonMap.java)
  * ------------------------------------------------------------------------- */
 
-/* SPPMManager.reset: radius = r0, iteration = 0. */
+/* SPPMManager.reset: radius = r0, iteration = 0.  The gathers of one SPPM
+ * sequence share their pixel-centre rays (same camera, scene and settings:
+ * traced by the first gather, reused by the next); a reset starts a new
+ * sequence whose first gather traces them again. */
 int rc_sppm_reset(rc_ctx* ctx, float initial_radius);
 /* SPPMManager.tracePhotons: clears the hash (PhotonMap.clear) and traces
  * photon_count photons with seed iteration*7919+6271 at the current radius. */
@@ -379,13 +385,15 @@ int rc_denoise_atrous(rc_ctx* ctx, const rc_atrous_params* params, float* out_rg
  * allocation can cause mid-frame.  Same p00 + à-trous chain as
  * rc_denoise_atrous, but every image is a caller-owned DEVICE pointer (accum
  * RGBA32F, gbuffer/albedo RGBA16F, variance R32F, out RGBA32F; out must not
- * alias accum) and the one intermediate image lives in a static device array
- * of RC_NOALLOC_MAX_PIXELS RGBA32F pixels (16 MiB) that every GPU loading this
- * library holds until the process exits.  Larger images return
- * RC_ERR_CAPACITY.  The first call on a device resolves that array's device
- * address (make it before any stream capture); errors are read with
- * rc_last_error(NULL, ...).  All calls on a device share the array, so calls
- * that overlap on the GPU race.  cuda_stream may be NULL (legacy stream). */
+ * share a byte with any input, else RC_ERR_INVALID_ARG) and the one
+ * intermediate image lives in a static device array of RC_NOALLOC_MAX_PIXELS
+ * RGBA32F pixels (16 MiB) that every GPU loading this library holds until the
+ * process exits.  Larger images return RC_ERR_CAPACITY.  Every call looks up
+ * that array's address in the caller's current CUDA context; the first call
+ * on a device also loads the module there, so make it before any stream
+ * capture.  Errors are read with rc_last_error(NULL, ...).  All calls on a
+ * device share the array, so calls that overlap on the GPU race.
+ * cuda_stream may be NULL (legacy stream). */
 #define RC_NOALLOC_MAX_PIXELS 1048576
 int rc_denoise_atrous_noalloc(const float* accum_rgba, const uint16_t* gbuffer_rgba16f,
                               const uint16_t* albedo_rgba16f, const float* variance,

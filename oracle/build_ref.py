@@ -34,7 +34,16 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
-DEFAULT_REF = "/root/reference"
+
+
+def default_ref_root() -> str:
+    """Where the reference checkout is looked for: $RETROCAM_REFERENCE, else a
+    directory named `reference` beside this repository's root."""
+    env = os.environ.get("RETROCAM_REFERENCE")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(REPO), "reference")
+
 SHADER_DIR = os.path.join("src", "main", "resources", "shaders")
 SHADERS = [
     ("pt", "pathtrace.comp"),
@@ -49,6 +58,8 @@ SHADERS = [
     "p14_tracking", "p15_edge_enhance", "p16_interlace")]
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_LIB = os.path.join(OUT_DIR, "libretrocam_ref.so")
+# timing variant: sin/cos/exp/log/pow from the host C library (not for parity)
+OUT_LIB_LIBM = os.path.join(OUT_DIR, "libretrocam_ref_libm.so")
 
 
 def _match_paren(s: str, open_idx: int) -> int:
@@ -124,26 +135,28 @@ def translation_unit(ref_root: str) -> str:
     return "\n".join(parts)
 
 
-def build(ref_root: str = DEFAULT_REF, quiet: bool = False) -> str | None:
+def build(ref_root: str | None = None, quiet: bool = False) -> str | None:
     """Compile the reference shaders; returns the library path, or None when
     no reference checkout is present (the prebuilt library is then used)."""
+    ref_root = ref_root or default_ref_root()
     if not os.path.isdir(os.path.join(ref_root, SHADER_DIR)):
         return OUT_LIB if os.path.exists(OUT_LIB) else None
     os.makedirs(OUT_DIR, exist_ok=True)
     tu = translation_unit(ref_root)
-    cmd = ["g++", "-std=c++20", "-O2", "-fopenmp", "-fwrapv", "-ffp-contract=off",
-           "-fno-fast-math", "-fPIC", "-shared", "-w",
-           "-I", HERE, "-I", os.path.join(REPO, "include"),
-           "-x", "c++", "-", "-o", OUT_LIB + ".tmp"]
-    proc = subprocess.run(cmd, input=tu.encode(), capture_output=True)
-    if proc.returncode != 0:
-        sys.stderr.write(proc.stderr.decode(errors="replace"))
-        raise RuntimeError("building oracle/_ref failed")
-    os.replace(OUT_LIB + ".tmp", OUT_LIB)
-    if not quiet:
-        print(f"built {OUT_LIB}")
+    for out, defs in ((OUT_LIB, []), (OUT_LIB_LIBM, ["-DRC_REF_HOST_LIBM"])):
+        cmd = ["g++", "-std=c++20", "-O2", "-fopenmp", "-fwrapv", "-ffp-contract=off",
+               "-fno-fast-math", "-fPIC", "-shared", "-w"] + defs + [
+               "-I", HERE, "-I", os.path.join(REPO, "include"),
+               "-x", "c++", "-", "-o", out + ".tmp"]
+        proc = subprocess.run(cmd, input=tu.encode(), capture_output=True)
+        if proc.returncode != 0:
+            sys.stderr.write(proc.stderr.decode(errors="replace"))
+            raise RuntimeError("building oracle/_ref failed")
+        os.replace(out + ".tmp", out)
+        if not quiet:
+            print(f"built {out}")
     return OUT_LIB
 
 
 if __name__ == "__main__":
-    build(sys.argv[1] if len(sys.argv) > 1 else DEFAULT_REF)
+    build(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -128,11 +128,22 @@ inline vec3 operator*(const mat3& m, const vec3& v) { return m.c0 * v.x + m.c1 *
 inline float abs(float x) { return rcx_bitsf(rcx_fbits(x) & 0x7fffffffu); }
 inline float sqrt(float x) { return __builtin_sqrtf(x); }
 inline float floor(float x) { return __builtin_floorf(x); }
+#ifdef RC_REF_HOST_LIBM
+/* timing variant of the compiled reference (oracle/_ref/libretrocam_ref_libm.so):
+ * the host C library's single-precision functions, as a GL driver's compiler
+ * would use its own fast ones; not used for parity */
+inline float sin(float x) { return __builtin_sinf(x); }
+inline float cos(float x) { return __builtin_cosf(x); }
+inline float exp(float x) { return __builtin_expf(x); }
+inline float log(float x) { return __builtin_logf(x); }
+inline float pow(float x, float y) { return __builtin_powf(x, y); }
+#else
 inline float sin(float x) { return rcx_sinf(x); }
 inline float cos(float x) { return rcx_cosf(x); }
 inline float exp(float x) { return rcx_expf(x); }
 inline float log(float x) { return rcx_logf(x); }
 inline float pow(float x, float y) { return rcx_powf(x, y); }
+#endif
 inline float min(float x, float y) { return (y < x) ? y : x; }
 inline float max(float x, float y) { return (x < y) ? y : x; }
 inline int min(int x, int y) { return (y < x) ? y : x; }

@@ -18,6 +18,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libretrocam_ref.so")
+# the same shaders with the host C library's sin/cos/exp/log/pow: a timing
+# variant of the CPU baseline, not a parity reference
+REF_LIB_LIBM = os.path.join(HERE, "_ref", "libretrocam_ref_libm.so")
 
 F3 = ("<f4", 3)
 TRI = np.dtype([("v0",) + F3, ("pad0", "<f4"), ("v1",) + F3, ("pad1", "<f4"), ("v2",) + F3, ("pad2", "<f4"),
@@ -301,3 +304,8 @@ def load(build: bool = True):
             sys.path.pop(0)
     ref = Reference() if os.path.exists(REF_LIB) else None
     return Oracle(), ref
+
+
+def load_reference_libm():
+    """The timing variant of the compiled reference, or None."""
+    return Reference(REF_LIB_LIBM) if os.path.exists(REF_LIB_LIBM) else None

@@ -133,7 +133,7 @@ class rc_counters(C.Structure):
                 ("node_tests", C.c_uint64), ("tri_tests", C.c_uint64), ("surface_hits", C.c_uint64),
                 ("light_samples", C.c_uint64), ("photon_node_tests", C.c_uint64),
                 ("photon_tri_tests", C.c_uint64), ("kernel_launches", C.c_uint64), ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64),
-                ("error_word", C.c_uint32), ("reserved", C.c_uint32)]
+                ("error_word", C.c_uint32), ("bvh_depth", C.c_uint32)]
 
 
 KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <mutex>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -535,9 +536,18 @@ struct BinnedBuilder {
         BinnedBuilder right(tb, cen, idx);
         right.nodes.reserve(2 * (size_t)(end - mid));
         right.nodes.emplace_back();
-        std::thread job([&] { right.build(0, mid, end, spawn - 1); });
+        // no exception may leave the C ABI: without a thread to be had, the
+        // right subtree is built here after the left one (disjoint ranges)
+        std::thread job;
+        try {
+            job = std::thread([&] { right.build(0, mid, end, spawn - 1); });
+        } catch (const std::system_error&) {
+        }
         build(l, begin, mid, spawn - 1);
-        job.join();
+        if (job.joinable())
+            job.join();
+        else
+            right.build(0, mid, end, spawn - 1);
         // the right subtree's root takes slot l + 1, its other nodes follow
         const int base = (int)nodes.size() - 1;
         auto place = [&](int j) { return j == 0 ? l + 1 : base + j; };
@@ -798,7 +808,14 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     SubsetBvh sb, db;
     bool built = false;
     JoinOnExit split_job;
-    if (want_split) split_job.t = std::thread([&] { built = build_split(tris, tri_count, mats, sb, db); });
+    bool split_inline = false;  // no helper thread could be started: build at the join
+    if (want_split) {
+        try {
+            split_job.t = std::thread([&] { built = build_split(tris, tri_count, mats, sb, db); });
+        } catch (const std::system_error&) {
+            split_inline = true;
+        }
+    }
     // ---- convert to the kernels' layout ----
     std::vector<NodeRec> recs(node_count);
     memset(recs.data(), 0, recs.size() * sizeof(NodeRec));
@@ -877,7 +894,10 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     //      the specular (metal or glass) triangles and over the others ----
     ctx->photon_split = false;
     if (want_split) {
-        split_job.t.join();
+        if (split_inline)
+            built = build_split(tris, tri_count, mats, sb, db);
+        else
+            split_job.t.join();
         if (built) {
             CK(ensure(ctx->sp_nodes, sb.recs.size() * sizeof(NodeRec)));
             CK(ensure(ctx->sp_isect, sb.isect.size() * sizeof(float4)));
@@ -1149,6 +1169,9 @@ int rc_sppm_reset(rc_ctx* ctx, float initial_radius) {
     if (!(initial_radius > 0.0f)) return fail(ctx, RC_ERR_INVALID_ARG, "rc_sppm_reset: radius must be > 0");
     ctx->sppm_radius = initial_radius;
     ctx->sppm_iteration = 0;
+    // a new SPPM sequence (a new export frame) traces its gather rays again:
+    // the per-pixel gather hits are reused only within one sequence
+    ctx->gcache_valid = false;
     return RC_OK;
 }
 
@@ -1230,7 +1253,10 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     A.hash_size = p->hash_size;
     A.radius = ctx->sppm_radius;
     A.seed = ctx->sppm_iteration * 7919 + 6271;
-    A.split = (ctx->math_mode == RC_MATH_FAST && ctx->photon_split && !ctx->photon_full_first) ? 1 : 0;
+    // the split walks other BVHs; past 60 levels the photon walk keeps the
+    // reference's own order over its BVH (its 64-entry stack can overflow)
+    A.split = (ctx->math_mode == RC_MATH_FAST && ctx->photon_split && !ctx->photon_full_first &&
+               ctx->scene.depth <= 60) ? 1 : 0;
     A.spec = ctx->spec_view;
     A.diff = ctx->diff_view;
     A.spec_orig = (const int*)ctx->sp_orig.ptr;
@@ -1566,7 +1592,7 @@ int rc_get_counters(rc_ctx* ctx, rc_counters* out) {
     out->h2d_bytes = ctx->h2d;
     out->d2h_bytes = ctx->d2h;
     out->error_word = d.error_word;
-    out->reserved = 0;
+    out->bvh_depth = ctx->has_scene ? (uint32_t)ctx->scene.depth : 0u;
     return RC_OK;
 }
 

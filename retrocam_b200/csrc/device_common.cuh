@@ -626,11 +626,21 @@ DI bool traverse4(const DeviceScene& S, const Ray& r, float max_t, Guard& g, Hit
 
 // Closest hit and visibility as used by the kernels: the reference's
 // traversal order in the exact build; in the fast build the 4-wide
-// traversal when the scene has 4-wide nodes, else the binary one.
+// traversal when the scene has 4-wide nodes, else the binary one -- except
+// on BVHs deep enough that the reference's stacks can overflow (closest hit
+// and photon walks past 60 levels, shadow walks past 28): there the
+// reference drops pushes, which ones depends on its own visiting order, and
+// the fast build keeps that order so that it drops the same ones.
+// kShallow: the caller runs only on BVHs of at most 60 levels (the
+// shallow-tree instantiations of its kernel: 28 levels for the path tracer's,
+// 60 for the photon passes'), where the reference's closest-hit stack cannot
+// overflow, so the deep-tree branch is compiled out.
+template <bool kShallow>
 DI Hit closest_hit(const DeviceScene& S, const Ray& r, Guard& g) {
 #if RC_EXACT
     return trace_closest(S, r, g);
 #else
+    if (!kShallow && S.depth > 60) return trace_closest(S, r, g);
     Hit h;
     if (S.nodes4)
         traverse4<false>(S, r, 1e30f, g, h);
@@ -645,6 +655,7 @@ DI bool unoccluded(const DeviceScene& S, const Ray& r, float max_dist, Guard& g)
 #if RC_EXACT
     return trace_shadow<kTestAtParent>(S, r, max_dist, g);
 #else
+    if (!kTestAtParent) return trace_shadow<false>(S, r, max_dist, g);
     Hit h;
     if (S.nodes4) return !traverse4<true>(S, r, max_dist, g, h);
     return !traverse_ww<true>(S, r, max_dist, g, h);
@@ -658,7 +669,8 @@ DI Hit photon_hit(const DeviceScene& S, const Ray& r, Guard& g) {
 #if RC_EXACT
     return trace_unordered<kTestAtParent>(S, r, g);
 #else
-    return closest_hit(S, r, g);
+    if (!kTestAtParent) return trace_unordered<false>(S, r, g);
+    return closest_hit<true>(S, r, g);
 #endif
 }
 
@@ -834,7 +846,7 @@ DI float3 trace_radiance(const DeviceScene& S, Ray ray, uint32_t& seed, int nee,
     cn.paths++;
     for (int bounce = 0; bounce < 6; ++bounce) {
         cn.closest++;
-        const Hit hit = closest_hit(S, ray, g);
+        const Hit hit = closest_hit<kShadowAtParent>(S, ray, g);
         if (hit.prim < 0) break;
         cn.hits++;
         const Surf sf = surface(S, ray, hit);

@@ -21,6 +21,8 @@
 // Every traversal loop is bounded: a traversal that pops more stack
 // entries than the scene has nodes (impossible for a validated tree) sets
 // RC_GUARD_TRAVERSAL_CAP in the context's error word and stops.
+#include <atomic>
+
 #include "device_common.cuh"
 #include "dyn_trace.cuh"
 
@@ -79,7 +81,7 @@ __global__ void __launch_bounds__(128) render_kernel(RenderArgs A) {
                 uint32_t gs = init_seed(px, py, 99991);
                 const Ray gr = generate_ray(cam, W, H, px, py, gs, 0.0f);
                 cn.closest++;
-                const Hit h = closest_hit(S, gr, g);
+                const Hit h = closest_hit<kShadowAtParent>(S, gr, g);
                 float4 gv = make_float4(0.0f, 1.0f, 0.0f, 1e4f);
                 if (h.prim >= 0) {
                     cn.hits++;
@@ -922,6 +924,27 @@ cudaError_t launch_render(const RenderArgs& A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+#if !RC_EXACT
+// One persistent grid of photon_emit_dyn per device: every SM times the
+// blocks that fit it, computed once per device.
+static int emit_grid() {
+    constexpr int kDevs = 64;
+    static std::atomic<int> cache[kDevs];
+    int dev = 0, sms = 148, pe = 1;
+    cudaGetDevice(&dev);
+    const bool cached = dev >= 0 && dev < kDevs;
+    if (cached) {
+        const int g = cache[dev].load(std::memory_order_relaxed);
+        if (g > 0) return g;
+    }
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, photon_emit_dyn, 128, 0);
+    const int g = sms * (pe > 0 ? pe : 1);
+    if (cached) cache[dev].store(g, std::memory_order_relaxed);
+    return g;
+}
+#endif
+
 cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) {
     const int b = block <= 64 ? 64 : (block <= 128 ? 128 : 256);
     const int blocks = (A.photon_count + b - 1) / b;
@@ -934,15 +957,7 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) 
         cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
         if (e != cudaSuccess) return e;
-        static int grid_emit = 0;
-        if (!grid_emit) {
-            int dev = 0, sms = 148, pe = 1;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, photon_emit_dyn, 128, 0);
-            grid_emit = sms * (pe > 0 ? pe : 1);
-        }
-        photon_emit_dyn<<<grid_emit, 128, 0, s>>>(A);
+        photon_emit_dyn<<<emit_grid(), 128, 0, s>>>(A);
         if (A.scene.depth <= 60)
             photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
         else

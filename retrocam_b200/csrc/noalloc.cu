@@ -17,7 +17,7 @@
 // the GPU (different streams, or different host threads) race on the array.
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <cstdint>
 
 #include "device_scene.h"
 #include "host_checks.h"
@@ -38,29 +38,25 @@ static __device__ __align__(256) float4 g_atrous_scratch[RC_NOALLOC_MAX_PIXELS];
 
 namespace {
 
-const int kMaxDevices = 64;
-std::mutex g_mutex;
-float4* g_scratch_addr[kMaxDevices] = {};  // device address of g_atrous_scratch, per device
-
-// The address of g_atrous_scratch on the current device.  Host code cannot
-// use the symbol's name as a pointer (it is a host-side stand-in), so the
-// first call on each device asks the runtime for the real address, with that
-// device current, and keeps it.
-cudaError_t scratch_for_current_device(float4** out, int* dev_out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
+// The address of g_atrous_scratch in the current CUDA context.  Host code
+// cannot use the symbol's name as a pointer (it is a host-side stand-in), so
+// every call asks the runtime for the real address, with the caller's device
+// current.  The address belongs to the context that loaded this module: a
+// cached copy would outlive a cudaDeviceReset or point into another context
+// on the same device, so it is looked up again each time (cheap once the
+// module is loaded; the first call on a device loads it).
+cudaError_t scratch_for_current_device(float4** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_atrous_scratch);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lk(g_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_atrous_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = (float4*)p;
-    }
-    *out = g_scratch_addr[dev];
-    *dev_out = dev;
+    *out = (float4*)p;
     return cudaSuccess;
+}
+
+// [a, a+na) and [b, b+nb) share a byte.
+bool overlaps(const void* a, size_t na, const void* b, size_t nb) {
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+    return x < y + nb && y < x + na;
 }
 
 }  // namespace
@@ -83,15 +79,18 @@ extern "C" int rc_denoise_atrous_noalloc(const float* accum, const uint16_t* gbu
     if (!aligned_to(accum, 16) || !aligned_to(out, 16) || !aligned_to(gbuffer, 8) || !aligned_to(albedo, 8) ||
         !aligned_to(variance, 4))
         return rc_noalloc_fail(RC_ERR_INVALID_ARG, "rc_denoise_atrous_noalloc: misaligned buffer");
-    if ((const void*)out == (const void*)accum)
-        return rc_noalloc_fail(RC_ERR_INVALID_ARG, "rc_denoise_atrous_noalloc: out must not alias accum");
     if ((long long)width * height > RC_NOALLOC_MAX_PIXELS)
         return rc_noalloc_fail(RC_ERR_CAPACITY,
                                "rc_denoise_atrous_noalloc: width*height exceeds RC_NOALLOC_MAX_PIXELS "
                                "(1048576); use rc_denoise_atrous");
+    // every pass reads its neighbours' pixels from the inputs while others
+    // write the output, so the output may share no byte with any input
+    const size_t npx = (size_t)width * height;
+    if (overlaps(out, npx * 16, accum, npx * 16) || overlaps(out, npx * 16, gbuffer, npx * 8) ||
+        overlaps(out, npx * 16, albedo, npx * 8) || overlaps(out, npx * 16, variance, npx * 4))
+        return rc_noalloc_fail(RC_ERR_INVALID_ARG, "rc_denoise_atrous_noalloc: out overlaps an input image");
     float4* scratch = nullptr;
-    int dev = -1;
-    cudaError_t e = scratch_for_current_device(&scratch, &dev);
+    cudaError_t e = scratch_for_current_device(&scratch);
     if (e != cudaSuccess)
         return rc_noalloc_fail(RC_ERR_CUDA, "rc_denoise_atrous_noalloc: cannot resolve the scratch array");
     cudaStream_t s = (cudaStream_t)cuda_stream;

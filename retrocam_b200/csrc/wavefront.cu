@@ -21,6 +21,8 @@
 // accumulation adds samples in frame order, so exact-math results stay
 // bit-identical to the oracle.  Kernels are grid-stride loops over device-side
 // queue lengths, launched with a grid that fills the GPU once.
+#include <mutex>
+
 #include "device_common.cuh"
 #include "dyn_trace.cuh"
 
@@ -155,7 +157,7 @@ __global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
         if (i < nr) {
             const int p = B.rq[cur][i];
             const Ray r = make_ray(xyz(B.o[p]), xyz(B.d[p]));
-            const Hit h = closest_hit(A.scene, r, g);
+            const Hit h = closest_hit<kShadowAtParent>(A.scene, r, g);
             B.hit[p] = make_float4(h.t, h.u, h.v, __int_as_float(h.prim));
             ++closest;
         } else {
@@ -439,7 +441,7 @@ __global__ void __launch_bounds__(128) wf_accumulate(WaveArgs A) {
                 uint32_t gs = init_seed(px, py, 99991);
                 const Ray gr = generate_ray(sg.cam, W, H, px, py, gs, 0.0f);
                 ++closest;
-                const Hit h = closest_hit(A.scene, gr, g);
+                const Hit h = closest_hit<false>(A.scene, gr, g);
                 float4 gv = make_float4(0.0f, 1.0f, 0.0f, 1e4f);
                 if (h.prim >= 0) {
                     ++ghits;
@@ -598,23 +600,37 @@ struct WfGrids {
     int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, dyn[3] = {}, dyn4[3] = {};
 };
 static int block_class(int block) { return block <= 64 ? 0 : (block <= 128 ? 1 : 2); }
-static WfGrids& grids() {
-    static WfGrids g;
-    if (!g.gen) {
-        g.gen = grid_for((const void*)wf_generate, 256);
-        g.acc = grid_for((const void*)wf_accumulate, 128);
-        for (int c = 0; c < 3; ++c) {
-            const int b = 64 << c;
-            g.trace0[c] = grid_for((const void*)wf_trace<false>, b);
-            g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
-            g.shade[c] = grid_for((const void*)wf_shade, b);
+static void fill_grids(WfGrids& g) {
+    g.gen = grid_for((const void*)wf_generate, 256);
+    g.acc = grid_for((const void*)wf_accumulate, 128);
+    for (int c = 0; c < 3; ++c) {
+        const int b = 64 << c;
+        g.trace0[c] = grid_for((const void*)wf_trace<false>, b);
+        g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
+        g.shade[c] = grid_for((const void*)wf_shade, b);
 #if !RC_EXACT
-            g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
-            g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
+        g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
+        g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
 #endif
-        }
     }
-    return g;
+}
+
+// The grids of the current device (SM counts and occupancy differ between
+// devices), filled once per device; a process may drive several devices
+// from several threads.
+static WfGrids& grids() {
+    constexpr int kDevs = 64;
+    static WfGrids g[kDevs];
+    static std::once_flag once[kDevs];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kDevs) {
+        thread_local WfGrids t;
+        fill_grids(t);
+        return t;
+    }
+    std::call_once(once[dev], [&] { fill_grids(g[dev]); });
+    return g[dev];
 }
 
 cudaError_t launch_wf_generate(const WaveArgs& A, cudaStream_t s) {
@@ -631,7 +647,10 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
     // chunks below refill_min_paths hold about one wave of rays per launch,
     // where the refill bookkeeping costs more than it recovers (854x480 at
     // 1 spp: trace 0.264 ms grid-stride vs 0.306 ms refill; they tie at 2 spp)
-    if (A.dynamic_fetch && A.paths >= A.refill_min_paths && A.scene.max_leaf < 0x10000) {
+    // BVHs deeper than 28 levels keep the reference's shadow walk (its
+    // 32-entry stack can overflow), which the refill walk does not follow
+    if (A.dynamic_fetch && A.paths >= A.refill_min_paths && A.scene.max_leaf < 0x10000 &&
+        A.scene.depth <= 28) {
         if (A.scene.nodes4)
             wf_trace_dyn4<<<grids().dyn4[c], b, 0, s>>>(A);
         else

@@ -259,19 +259,32 @@ def _timed(ctx, fn) -> float:
     return (time.perf_counter() - t0) * 1e3
 
 
+def box5(img: np.ndarray) -> np.ndarray:
+    """5x5 box average with edge clamping (the control filter: equal weights
+    over the learned filter's footprint, no features)."""
+    p = np.pad(img.astype(np.float64), ((2, 2), (2, 2), (0, 0)), mode="edge")
+    c = np.cumsum(np.cumsum(p, axis=0), axis=1)
+    c = np.pad(c, ((1, 0), (1, 0), (0, 0)))
+    H, W = img.shape[:2]
+    s = c[5:5 + H, 5:5 + W] - c[0:H, 5:5 + W] - c[5:5 + H, 0:W] + c[0:H, 0:W]
+    return (s / 25.0).astype(np.float32)
+
+
 def evaluate(params: np.ndarray, seeds, spps=(1, 2, 4, 8, 16, 32, 64, 128, 256), ref_spp=4096, width=854,
              height=480, threshold=1e-2, log=print) -> dict:
     """relMSE against an independent `ref_spp` render, for the path tracer
-    plus à-trous (5 passes, sigma_n 128, sigma_d 1, sigma_c 1) and plus the
-    learned denoiser at equal spp; wall time of render + denoise per frame.
-    `time_to_threshold` is, per method, the time at the smallest spp whose
-    mean relMSE over the variants is <= threshold (None if none is)."""
+    plus à-trous (5 passes, sigma_n 128, sigma_d 1, sigma_c 1), plus the
+    learned denoiser, and plus a plain 5x5 box average (a control: what the
+    learned filter's footprint gives with equal weights) at equal spp; wall
+    time of render + denoise per frame.  `time_to_threshold` is, per
+    method, the time at the smallest spp of `spps` whose mean relMSE over
+    the variants is <= threshold (None if none is)."""
     atrous = api.atrous_params(scenes.AtrousDesc(max_spp=0))
     res = {"spp": list(spps), "ref_spp": ref_spp, "variants": list(seeds), "width": width, "height": height,
-           "relmse": {"noisy": [], "atrous": [], "learned": []},
+           "relmse": {"noisy": [], "atrous": [], "learned": [], "box5": []},
            "ms": {"render": [], "atrous": [], "learned": []}}
-    per = {k: np.zeros((len(seeds), len(spps))) for k in ("noisy", "atrous", "learned", "render", "t_atrous",
-                                                           "t_learned")}
+    per = {k: np.zeros((len(seeds), len(spps))) for k in ("noisy", "atrous", "learned", "box5", "render",
+                                                           "t_atrous", "t_learned")}
     with api.Context(width, height, 0, api.RC_MATH_FAST) as ctx:
         for vi, seed in enumerate(seeds):
             w = scenes.cornell_variant(seed, width, height)
@@ -289,7 +302,9 @@ def evaluate(params: np.ndarray, seeds, spps=(1, 2, 4, 8, 16, 32, 64, 128, 256),
                 ctx.reset()
                 per["render"][vi, si] = _timed(ctx, lambda: ctx.render(cam, st, 0, k))
                 acc = ctx.read_buffers()[0]
-                per["noisy"][vi, si] = relmse(acc[..., :3] / np.maximum(acc[..., 3:4], 1), ref)
+                noisy = acc[..., :3] / np.maximum(acc[..., 3:4], 1)
+                per["noisy"][vi, si] = relmse(noisy, ref)
+                per["box5"][vi, si] = relmse(box5(noisy), ref)
                 per["t_atrous"][vi, si] = _timed(ctx, lambda: ctx.denoise(atrous, read=False))
                 per["atrous"][vi, si] = relmse(ctx.read_output(), ref)
                 per["t_learned"][vi, si] = _timed(ctx, lambda: ctx.denoise_learned(params, read=False))
@@ -299,7 +314,7 @@ def evaluate(params: np.ndarray, seeds, spps=(1, 2, 4, 8, 16, 32, 64, 128, 256),
             if log:
                 log(f"variant {seed}: atrous {np.round(per['atrous'][vi], 4).tolist()} "
                     f"learned {np.round(per['learned'][vi], 4).tolist()}")
-    for k in ("noisy", "atrous", "learned"):
+    for k in ("noisy", "atrous", "learned", "box5"):
         res["relmse"][k] = per[k].mean(axis=0).tolist()
     res["ms"]["render"] = per["render"].mean(axis=0).tolist()
     res["ms"]["atrous"] = per["t_atrous"].mean(axis=0).tolist()

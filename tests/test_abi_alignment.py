@@ -54,3 +54,22 @@ def test_noalloc_alignment(product):
                                                  C.c_void_p((1 << 20) + 4096), 4, 4, 1, C.byref(a),
                                                  product.RC_MATH_FAST, None)
     assert rc == product.RC_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("which", [0, 1, 2, 3])
+def test_noalloc_rejects_output_overlapping_an_input(product, which):
+    """The output image may share no byte with any of the four inputs: a pass
+    reads neighbouring pixels of its inputs while other threads write the
+    output.  Each input in turn is placed so that it ends inside the output's
+    first bytes (16x16 pixels: 4 KiB of output)."""
+    a = product.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)
+    base = 1 << 24
+    out = C.c_void_p(base)
+    sizes = [16 * 256, 8 * 256, 8 * 256, 4 * 256]
+    args = [C.c_void_p(base + (1 << 20) * (k + 1)) for k in range(4)]
+    args[which] = C.c_void_p(base - sizes[which] + 16)
+    rc = product.lib().rc_denoise_atrous_noalloc(*args, out, 16, 16, 1, C.byref(a), product.RC_MATH_FAST, None)
+    assert rc == product.RC_ERR_INVALID_ARG
+    buf = C.create_string_buffer(256)
+    product.lib().rc_last_error(None, buf, len(buf))
+    assert b"overlaps" in buf.value

@@ -117,3 +117,55 @@ def test_display_bit_identical(orc, ref, total, exposure):
     assert (a[..., 3] == 255).all()
     # rows top first: flipping the buffer flips the image
     assert np.array_equal(a[::-1], orc.display(np.ascontiguousarray(c[::-1]), W, H, total, exposure))
+
+
+@pytest.fixture(scope="module")
+def deep_scene(orc):
+    """The export frame's triangles under the chained 87-level tree of
+    tests/deep_bvh.py, where the shaders' stacks overflow."""
+    import deep_bvh
+    import pyoracle as po
+    from retrocam_b200 import scenes
+    w = scenes.export_frame()
+    sc = deep_bvh.chain_scene(w.scene, orc, po.MAT, groups=80)
+    assert deep_bvh.bvh_depth(sc["nodes"]) > 60
+    return w, sc, scenes.camera(w.orbit, w.lens, orc)
+
+
+@pytest.mark.parametrize("lca,settings", [(True, (1, 1.0)), (False, (0, 1.0)), (False, (1, 20.0))])
+def test_render_bit_identical_deep_tree(orc, ref, deep_scene, scenes_built, lca, settings):
+    """Closest-hit (top < 62) and shadow (top < 30) stack overflow as the
+    shaders have it.  With NEE on, the deep tree must change the image
+    against the builder's tree (shadow rays lose subtrees), or no overflow
+    happened; with NEE off only the few closest-hit rays travelling against
+    the chain's order overflow."""
+    w, sc, cam = deep_scene
+    cam = dict(cam)
+    cam["lca_delta"] = (-0.009, 0.0, 0.009) if lca else (0.0, 0.0, 0.0)
+    W, H = 64, 36
+    mine, _ = orc.render(sc, cam, settings, W, H, 0, 2)
+    theirs = ref.render(sc, cam, settings, W, H, 0, 2)
+    for a, b in zip(mine, theirs):
+        assert _eq(a, b)
+    shallow, _ = orc.render(scenes_built["export_frame"][1], cam, settings, W, H, 0, 2)
+    changed = (np.abs(shallow[0] - mine[0]).max(axis=-1) > 1e-3).mean()
+    assert changed > (0.02 if settings[0] else 0.0), changed
+
+
+def test_photon_trace_and_gather_bit_identical_deep_tree(orc, ref, deep_scene, scenes_built):
+    w, sc, cam = deep_scene
+    N, r, hs = 100_000, 0.02, 1 << 18
+    ph, hd, nx, cnt, _ = orc.photon_trace(sc, N, r, 6271, hs)
+    ph2, hd2, nx2, cnt2 = ref.photon_trace(sc, N, r, 6271, hs, threads=1)
+    assert cnt == cnt2 > 1000
+    assert _eq(ph[:cnt].view(np.float32), ph2[:cnt].view(np.float32))
+    assert np.array_equal(hd, hd2) and np.array_equal(nx[:cnt], nx2[:cnt])
+    # the photon walk's 64-entry stack overflowed: fewer photons stored
+    _, _, _, cnt_shallow, _ = orc.photon_trace(scenes_built["export_frame"][1], N, r, 6271, hs)
+    assert cnt < 0.9 * cnt_shallow
+    W, H = 80, 48
+    a1 = np.ones((H, W, 4), np.float32)
+    a2 = a1.copy()
+    orc.photon_gather(sc, cam, W, H, r, hs, ph, hd, nx, a1)
+    ref.photon_gather(sc, cam, W, H, r, N, hs, 0, ph2, hd2, nx2, a2)
+    assert _eq(a1, a2) and (a1 != 1.0).any()

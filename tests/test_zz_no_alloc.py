@@ -7,12 +7,13 @@ allocation can bring.  It reads and writes only caller-owned device buffers
 plus one static device array inside the library.
 
 The test renders a frame through a context, copies the four renderer images
-into device buffers it owns, and makes two no-alloc calls in a row (exact
-math, then fast math with other settings, so the second call reuses the
-static array the first one left behind).  Each result must equal what
-rc_denoise_atrous produced for the same images: bit for bit in exact math,
-within the fast-math tolerance of the other denoiser tests otherwise.  This
-file is named to be collected last.
+into device buffers it owns, and makes no-alloc calls in a row (exact math
+with several settings -- five passes, the denoiser disabled, a sample count
+above max_spp, one pass, seven passes clamped to five -- then fast math with
+other settings, so each call reuses the static array the one before left
+behind).  Each result must equal what rc_denoise_atrous produced for the same
+images: bit for bit in exact math, within the fast-math tolerance of the
+other denoiser tests otherwise.  This file is named to be collected last.
 """
 import ctypes as C
 
@@ -29,6 +30,21 @@ def _bind(api):
     return fn
 
 
+def _device_images(torch, dev, acc, gb, ga, var):
+    return (torch.from_numpy(acc).to(dev), torch.from_numpy(gb.view(np.int16)).to(dev),
+            torch.from_numpy(ga.view(np.int16)).to(dev), torch.from_numpy(var).to(dev))
+
+
+# (math mode, spp, parameter cases).  Exact math: the full five passes, the
+# normalise-only branch (denoiser disabled; sample count above max_spp) and
+# pass counts the reference clamps (1 and 7 -> 5); fast math: other sigmas.
+CASES = [
+    (0, 3, [(1, 5, 1.0, 128.0, 1.0, 0, 1.0), (0, 5, 1.0, 128.0, 1.0, 0, 1.0), (1, 5, 1.0, 128.0, 1.0, 2, 1.0),
+            (1, 1, 1.0, 128.0, 1.0, 0, 1.0), (1, 7, 1.0, 128.0, 1.0, 0, 1.3)]),
+    (1, 5, [(1, 4, 1.0, 64.0, 0.15, 0, 1.5)]),
+]
+
+
 def test_noalloc_denoise_matches_context_denoise(product, cuda_ok):
     import torch
     from retrocam_b200 import scenes
@@ -39,29 +55,27 @@ def test_noalloc_denoise_matches_context_denoise(product, cuda_ok):
     cam = api.workload_camera(w)
     W, H = 200, 120
     dev = torch.device("cuda", 0)
-    calls = [(api.RC_MATH_EXACT, 3, api.rc_atrous_params(1, 5, 1.0, 128.0, 1.0, 0, 1.0)),
-             (api.RC_MATH_FAST, 5, api.rc_atrous_params(1, 4, 1.0, 64.0, 0.15, 0, 1.5))]
-    for mode, spp, params in calls:
+    for fast, spp, plist in CASES:
+        mode = api.RC_MATH_FAST if fast else api.RC_MATH_EXACT
         with api.Context(W, H, 0, mode) as ctx:
             ctx.upload(sc)
             ctx.render(cam, (1, 1.0), 0, spp)
             acc, gb, ga, var = ctx.read_buffers()
-            want = ctx.denoise(params)
-        d_acc = torch.from_numpy(acc).to(dev)
-        d_gb = torch.from_numpy(gb.view(np.int16)).to(dev)
-        d_ga = torch.from_numpy(ga.view(np.int16)).to(dev)
-        d_var = torch.from_numpy(var).to(dev)
-        d_out = torch.full((H, W, 4), float("nan"), dtype=torch.float32, device=dev)
-        torch.cuda.synchronize()
-        rc = fn(d_acc.data_ptr(), d_gb.data_ptr(), d_ga.data_ptr(), d_var.data_ptr(), d_out.data_ptr(), W, H,
-                spp, C.byref(params), mode, None)
-        assert rc == api.RC_OK
-        torch.cuda.synchronize()
-        got = d_out.cpu().numpy()
-        if mode == api.RC_MATH_EXACT:
-            assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
-        else:
-            np.testing.assert_allclose(got, want, rtol=2e-3, atol=2e-4)
+            wants = [ctx.denoise(api.rc_atrous_params(*pv)) for pv in plist]
+        d_acc, d_gb, d_ga, d_var = _device_images(torch, dev, acc, gb, ga, var)
+        for pv, want in zip(plist, wants):
+            params = api.rc_atrous_params(*pv)
+            d_out = torch.full((H, W, 4), float("nan"), dtype=torch.float32, device=dev)
+            torch.cuda.synchronize()
+            rc = fn(d_acc.data_ptr(), d_gb.data_ptr(), d_ga.data_ptr(), d_var.data_ptr(), d_out.data_ptr(), W, H,
+                    spp, C.byref(params), mode, None)
+            assert rc == api.RC_OK, pv
+            torch.cuda.synchronize()
+            got = d_out.cpu().numpy()
+            if mode == api.RC_MATH_EXACT:
+                assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), pv
+            else:
+                np.testing.assert_allclose(got, want, rtol=2e-3, atol=2e-4)
 
 
 def test_noalloc_rejects_images_over_its_limit(product, cuda_ok):
