@@ -415,6 +415,46 @@ int rc_render_frame(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settin
                     float* out_rgba);
 
 /* ---------------------------------------------------------------------------
+ * One export frame split across devices.  No counterpart in the reference
+ * (one GL context, one GPU); the split keeps RenderPipeline.accumulateFrame's
+ * work (export/RenderPipeline.java:209-239) and the shaders' seeds: frame
+ * index f seeds pixel paths (pathtrace.comp:94-98, Renderer.java:99) and
+ * iteration k seeds its photons (k*7919+6271, SPPMManager.java:88), so a
+ * part renders exactly the samples and photon maps the whole frame would.
+ * ------------------------------------------------------------------------- */
+
+/* The part-th of `parts` contiguous shares of a frame: SPPM iterations
+ * [k0, k1) with their sample blocks [s0, s1) (iteration k owns samples
+ * [k*spp/it, (k+1)*spp/it), as in rc_render_frame), or, without SPPM,
+ * samples [s0, s1) = [part*spp/parts, (part+1)*spp/parts) (k0 = k1 = 0).
+ * Host arithmetic only. */
+int rc_frame_part_range(int spp, int sppm_iterations, int part, int parts, int* k0, int* k1, int* s0,
+                        int* s1);
+/* Renders one part of rc_render_frame's work into this context's images:
+ * rc_reset, then (SPPM) the radius and iteration counter advanced to
+ * iteration k0 and, per iteration k < k1, trace -> render the block ->
+ * gather -> shrink the radius; no denoise.  The images then hold this
+ * part's sums (accum rgb and count, variance); the part holding sample 0
+ * also writes the G-buffer and albedo.  The sum of all parts' accum and
+ * variance images is the whole frame's, up to the order of the float
+ * additions; after adding the other parts' images into one context, set
+ * its sample count with rc_set_total_samples and denoise there.
+ * rc_total_samples reports this part's sample count. */
+int rc_render_frame_part(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, int spp,
+                         const rc_sppm_params* sppm, float sppm_initial_radius, int sppm_iterations, int part,
+                         int parts);
+/* The sample count rc_denoise_atrous and rc_denoise_learned divide by
+ * (Renderer.getTotalSamples), for images merged from parts. */
+int rc_set_total_samples(rc_ctx* ctx, int total_samples);
+/* Device addresses of the context's images (accum RGBA32F, G-buffer and
+ * albedo RGBA16F, variance R32F; W*H pixels each, row-major) and the
+ * cudaStream_t its work runs on, for a caller that reduces parts with a
+ * collective library in place.  Work queued on that stream must finish
+ * (or be waited for on the caller's stream) before another stream reads or
+ * writes the images. */
+int rc_get_images(rc_ctx* ctx, void** accum, void** gbuffer, void** albedo, void** variance, void** stream);
+
+/* ---------------------------------------------------------------------------
  * Batched export frames (export/RenderPipeline.java:149-239 per frame, the
  * video-export loop over keyframed cameras)
  * ------------------------------------------------------------------------- */

@@ -180,6 +180,10 @@ _SIGNATURES = {
     "rc_sppm_state": (_I, [_VP, C.POINTER(_F), C.POINTER(_I)]),
     "rc_denoise_atrous": (_I, [_VP, _VP, _VP]),
     "rc_render_frame": (_I, [_VP, _VP, _VP, _I, _VP, _F, _I, _VP, _VP]),
+    "rc_frame_part_range": (_I, [_I, _I, _I, _I] + [C.POINTER(_I)] * 4),
+    "rc_render_frame_part": (_I, [_VP, _VP, _VP, _I, _VP, _F, _I, _I, _I]),
+    "rc_set_total_samples": (_I, [_VP, _I]),
+    "rc_get_images": (_I, [_VP] + [C.POINTER(_VP)] * 5),
     "rc_read_buffers": (_I, [_VP, _VP, _VP, _VP, _VP]),
     "rc_read_output": (_I, [_VP, _VP]),
     "rc_display": (_I, [_VP, _I, _F, _VP]),
@@ -433,6 +437,22 @@ class Context:
                                          C.byref(atrous), _p(out)))
         return out
 
+    def render_frame_part(self, cam, settings, spp, sppm: rc_sppm_params | None, r0, sppm_iters, part, parts):
+        """rc_render_frame_part: this context's share of a frame split
+        `parts` ways (no denoise; images hold the part's sums)."""
+        self.check(lib().rc_render_frame_part(self.h, C.byref(camera_struct(cam)), C.byref(rc_settings(*settings)),
+                                              spp, C.byref(sppm) if sppm is not None else None, r0, sppm_iters,
+                                              part, parts))
+
+    def set_total_samples(self, n: int):
+        self.check(lib().rc_set_total_samples(self.h, int(n)))
+
+    def image_pointers(self) -> dict:
+        """Device addresses of the images and the context's stream handle."""
+        p = [C.c_void_p() for _ in range(5)]
+        self.check(lib().rc_get_images(self.h, *[C.byref(x) for x in p]))
+        return dict(zip(("accum", "gbuffer", "albedo", "variance", "stream"), (x.value or 0 for x in p)))
+
     def read_buffers(self):
         H, W = self.height, self.width
         acc = np.zeros((H, W, 4), np.float32)
@@ -591,6 +611,13 @@ class AtrousDenoiser:
 
     def denoise(self, params: rc_atrous_params, read=True):
         return self.ctx.denoise(params, read)
+
+
+def frame_part_range(spp: int, sppm_iterations: int, part: int, parts: int) -> tuple:
+    """rc_frame_part_range: (k0, k1, s0, s1) of one part of a split frame."""
+    v = [C.c_int() for _ in range(4)]
+    _check(lib().rc_frame_part_range(spp, sppm_iterations, part, parts, *[C.byref(x) for x in v]))
+    return tuple(x.value for x in v)
 
 
 def atrous_params(a: scenes.AtrousDesc) -> rc_atrous_params:

@@ -1475,6 +1475,75 @@ int rc_render_frame(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settin
     return rc_denoise_atrous(ctx, atrous, out_rgba);
 }
 
+int rc_frame_part_range(int spp, int sppm_iterations, int part, int parts, int* k0, int* k1, int* s0,
+                        int* s1) {
+    if (spp < 1 || sppm_iterations < 0 || sppm_iterations > spp || parts < 1 || part < 0 || part >= parts ||
+        !k0 || !k1 || !s0 || !s1)
+        return RC_ERR_INVALID_ARG;
+    if (sppm_iterations > 0) {
+        // whole SPPM iterations, each with rc_render_frame's sample block
+        *k0 = (int)((long)part * sppm_iterations / parts);
+        *k1 = (int)((long)(part + 1) * sppm_iterations / parts);
+        *s0 = (int)((long)*k0 * spp / sppm_iterations);
+        *s1 = (int)((long)*k1 * spp / sppm_iterations);
+    } else {
+        *k0 = *k1 = 0;
+        *s0 = (int)((long)part * spp / parts);
+        *s1 = (int)((long)(part + 1) * spp / parts);
+    }
+    return RC_OK;
+}
+
+int rc_render_frame_part(rc_ctx* ctx, const rc_camera* cam, const rc_settings* settings, int spp,
+                         const rc_sppm_params* sppm, float sppm_initial_radius, int sppm_iterations, int part,
+                         int parts) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    int k0, k1, s0, s1;
+    if (!cam || !settings || (sppm_iterations > 0 && !sppm) ||
+        rc_frame_part_range(spp, sppm_iterations, part, parts, &k0, &k1, &s0, &s1) != RC_OK)
+        return fail(ctx, RC_ERR_INVALID_ARG, "rc_render_frame_part: bad arguments");
+    if (!ctx->has_scene) return fail(ctx, RC_ERR_NO_SCENE, "rc_render_frame_part: no scene uploaded");
+    int r = rc_reset(ctx);
+    if (r != RC_OK) return r;
+    if (sppm_iterations > 0 && ctx->scene.light_count > 0) {
+        // the radius and iteration count iteration k0 starts from, as
+        // updateRadius leaves them after k0 iterations
+        if ((r = rc_sppm_reset(ctx, sppm_initial_radius)) != RC_OK) return r;
+        for (int k = 0; k < k0; ++k)
+            if ((r = rc_sppm_update_radius(ctx, sppm->alpha)) != RC_OK) return r;
+        for (int k = k0; k < k1; ++k) {
+            const int b0 = (int)((long)k * spp / sppm_iterations);
+            const int b1 = (int)((long)(k + 1) * spp / sppm_iterations);
+            if ((r = rc_sppm_trace(ctx, sppm)) != RC_OK) return r;
+            if ((r = rc_render(ctx, cam, settings, b0, b1 - b0)) != RC_OK) return r;
+            if ((r = rc_sppm_gather(ctx, cam, sppm, (float)(b1 - b0))) != RC_OK) return r;
+            if ((r = rc_sppm_update_radius(ctx, sppm->alpha)) != RC_OK) return r;
+        }
+    } else if (s1 > s0) {
+        if ((r = rc_render(ctx, cam, settings, s0, s1 - s0)) != RC_OK) return r;
+    }
+    // this part's samples only; rc_set_total_samples after the merge
+    ctx->total_samples = s1 - s0;
+    return RC_OK;
+}
+
+int rc_set_total_samples(rc_ctx* ctx, int total_samples) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (total_samples < 0) return fail(ctx, RC_ERR_INVALID_ARG, "rc_set_total_samples: negative count");
+    ctx->total_samples = total_samples;
+    return RC_OK;
+}
+
+int rc_get_images(rc_ctx* ctx, void** accum, void** gbuf, void** galb, void** var, void** stream) {
+    if (!ctx) return RC_ERR_INVALID_ARG;
+    if (accum) *accum = ctx->img.accum;
+    if (gbuf) *gbuf = ctx->img.gbuf;
+    if (galb) *galb = ctx->img.galb;
+    if (var) *var = ctx->img.var;
+    if (stream) *stream = ctx->stream;
+    return RC_OK;
+}
+
 int rc_read_buffers(rc_ctx* ctx, float* accum, uint16_t* gbuf, uint16_t* galb, float* var) {
     if (!ctx) return RC_ERR_INVALID_ARG;
     const size_t px = (size_t)ctx->width * ctx->height;

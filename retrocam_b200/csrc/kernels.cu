@@ -808,18 +808,58 @@ DI float3 color_at(const AtrousArgs& A, long i) {
     return xyz(c);
 }
 
-// post/atrous_denoise.frag:50-122, one thread per pixel.  Colour taps use
-// the framebuffer textures' CLAMP_TO_EDGE addressing; G-buffer, albedo and
-// variance taps use the renderer textures' default REPEAT addressing.
-__global__ void __launch_bounds__(128) atrous_kernel(AtrousArgs A) {
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * 4 + (threadIdx.x >> 5);
-    const int W = A.width, H = A.height;
+// post/atrous_denoise.frag:50-122 as a shared-memory-tiled stencil.
+//
+// The 25 taps of pixel p sit at p + step*(i, j): on the lattice of pixels
+// congruent to p modulo step.  A block takes a 32 x 8 tile of one of the
+// step^2 interleaved sub-images (blockIdx.z = the residue (ox, oy)) and
+// stages the (32+4) x (8+4) lattice points its taps read, once each: the
+// demodulated irradiance irr = col / max(alb, .01) (when luma(alb) > .02)
+// with log(luma(irr) + 1e-3), and the normal and depth.  These depend only on
+// the tap position q -- the colour at q clamped into the image
+// (CLAMP_TO_EDGE framebuffer texture), the G-buffer and albedo at q wrapped
+// around it (the renderer textures' default REPEAT) -- so a staged halo point
+// holds exactly what every tap at q computed, and the centre pixel's own
+// irradiance and log-luma are its lattice point's.  Each thread then runs
+// the 25 weights from shared memory.
+//
+// Exact build: every expression as the shader orders it (bit-identical to
+// the per-tap form).  Fast build: the three edge-stopping factors in one
+// exp2, pow(d, sn) * exp(a) * exp(b) = exp2(sn*log2(d) + (a + b)*log2(e)),
+// two SFU operations per tap instead of four.
+constexpr int kAtW = 32, kAtH = 8, kAtPW = kAtW + 4, kAtPH = kAtH + 4;
+
+__global__ void __launch_bounds__(kAtW * kAtH) atrous_kernel(AtrousArgs A) {
+    __shared__ float4 s_irr[kAtPH][kAtPW];   // irradiance xyz, log-luma
+    __shared__ float4 s_geo[kAtPH][kAtPW];   // normal xyz, depth
+    const int W = A.width, H = A.height, st = A.step;
+    const int ox = blockIdx.z % st, oy = blockIdx.z / st;
+    const int u0 = blockIdx.x * kAtW, v0 = blockIdx.y * kAtH;
+    // tiles past this residue's part of the image (the grid is sized for
+    // the largest residue class) have nothing to write
+    if (ox + u0 * st >= W || oy + v0 * st >= H) return;
+    for (int k = threadIdx.x; k < kAtPW * kAtPH; k += kAtW * kAtH) {
+        const int lu = k % kAtPW, lv = k / kAtPW;
+        const int qx = ox + (u0 + lu - 2) * st, qy = oy + (v0 + lv - 2) * st;
+        const long ri = (long)wrap_repeat(qy, H) * W + wrap_repeat(qx, W);
+        const long ki = (long)wrap_clamp(qy, H) * W + wrap_clamp(qx, W);
+        const ushort4 g = __ldg(A.gbuf + ri);
+        const float3 col = color_at(A, ki);
+        const float3 alb = half3(__ldg(A.galb + ri));
+        const float3 irr = (luma709(alb) > 0.02f) ? col / vmax(alb, f3(0.01f, 0.01f, 0.01f)) : col;
+        const float logl = logf_(luma709(irr) + 1e-3f);
+        const float3 n = half3(g);
+        s_irr[lv][lu] = make_float4(irr.x, irr.y, irr.z, logl);
+        s_geo[lv][lu] = make_float4(n.x, n.y, n.z, halfw(g));
+    }
+    __syncthreads();
+    const int tu = threadIdx.x % kAtW, tv = threadIdx.x / kAtW;
+    const int x = ox + (u0 + tu) * st, y = oy + (v0 + tv) * st;
     if (x >= W || y >= H) return;
     const long ci = (long)y * W + x;
-    const ushort4 cg = __ldg(A.gbuf + ci);
-    const float3 c_norm = half3(cg);
-    const float c_depth = halfw(cg);
+    const float4 cgeo = s_geo[tv + 2][tu + 2];
+    const float3 c_norm = xyz(cgeo);
+    const float c_depth = cgeo.w;
     const float3 c_col = color_at(A, ci);
     if (c_depth > 9000.0f) {
         A.out[ci] = make_float4(c_col.x, c_col.y, c_col.z, 1.0f);
@@ -827,37 +867,47 @@ __global__ void __launch_bounds__(128) atrous_kernel(AtrousArgs A) {
     }
     const float3 c_alb = half3(__ldg(A.galb + ci));
     const bool has_alb = luma709(c_alb) > 0.02f;
-    const float3 c_irr = has_alb ? c_col / vmax(c_alb, f3(0.01f, 0.01f, 0.01f)) : c_col;
+    const float4 cirr = s_irr[tv + 2][tu + 2];
+    const float3 c_irr = xyz(cirr);
     const float N = (float)A.sample_count;
     const float sum_l2 = __ldg(A.var + ci);
     const float mean_l = luma709(c_col / gmax(A.exposure, 1e-4f));
     const float variance = gmax(0.0f, sum_l2 / N - mean_l * mean_l);
     const float var_denom = A.sigma_color * A.sigma_color * variance + 1e-6f;
     const float depth_denom = A.sigma_depth * A.sigma_depth + 1e-6f;
-    const float c_logl = logf_(luma709(c_irr) + 1e-3f);
+    const float c_logl = cirr.w;
     const float hk[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
     float3 irr_sum = f3(0, 0, 0);
     float w_sum = 0.0f;
+#if !RC_EXACT
+    const float kLog2e = 1.4426950408889634f;
+    const float inv_dd = kLog2e / depth_denom, inv_vd = kLog2e / var_denom;
+    const float c_dinv = 1.0f / (c_depth + 0.001f);
+#endif
 #pragma unroll
     for (int j = -2; j <= 2; ++j) {
 #pragma unroll
         for (int i = -2; i <= 2; ++i) {
-            const int tx = x + i * A.step, ty = y + j * A.step;
-            const long ri = (long)wrap_repeat(ty, H) * W + wrap_repeat(tx, W);
-            const long ki = (long)wrap_clamp(ty, H) * W + wrap_clamp(tx, W);
-            const ushort4 g2 = __ldg(A.gbuf + ri);
-            const float3 n2 = half3(g2);
-            const float dep2 = halfw(g2);
-            const float3 col2 = color_at(A, ki);
-            const float3 alb2 = half3(__ldg(A.galb + ri));
-            const float3 irr2 = (luma709(alb2) > 0.02f) ? col2 / vmax(alb2, f3(0.01f, 0.01f, 0.01f)) : col2;
+            const float4 e = s_irr[tv + 2 + j][tu + 2 + i];
+            const float4 g2 = s_geo[tv + 2 + j][tu + 2 + i];
+            const float3 irr2 = xyz(e);
             const float hw = hk[i + 2] * hk[j + 2];
-            const float wn = powf_(gmax(0.0f, dot(c_norm, n2)), A.sigma_normal);
-            const float dd = (c_depth - dep2) / (c_depth + 0.001f);
+#if RC_EXACT
+            const float wn = powf_(gmax(0.0f, dot(c_norm, xyz(g2))), A.sigma_normal);
+            const float dd = (c_depth - g2.w) / (c_depth + 0.001f);
             const float wd = expf_(-(dd * dd) / depth_denom);
-            const float ld = c_logl - logf_(luma709(irr2) + 1e-3f);
+            const float ld = c_logl - e.w;
             const float wc = expf_(-(ld * ld) / var_denom);
             const float w = hw * wn * wd * wc;
+#else
+            const float d = gmax(0.0f, dot(c_norm, xyz(g2)));
+            const float dd = (c_depth - g2.w) * c_dinv;
+            const float ld = c_logl - e.w;
+            const float ex = -(dd * dd) * inv_dd - (ld * ld) * inv_vd;
+            // pow(0, sn) is 0 for sn > 0 and 1 for sn == 0 (powf_ above)
+            const float w = d > 0.0f ? hw * exp2f(A.sigma_normal * __log2f(d) + ex)
+                                     : (A.sigma_normal == 0.0f ? hw * exp2f(ex) : 0.0f);
+#endif
             irr_sum = irr_sum + irr2 * w;
             w_sum += w;
         }
@@ -1021,8 +1071,11 @@ cudaError_t launch_photon_gather(const GatherArgs& A, cudaStream_t s) {
 }
 
 cudaError_t launch_atrous(const AtrousArgs& A, cudaStream_t s) {
-    const dim3 grid((A.width + 31) / 32, (A.height + 3) / 4);
-    atrous_kernel<<<grid, 128, 0, s>>>(A);
+    // residue classes (step^2) x tiles of the largest class's lattice
+    const int st = A.step < 1 ? 1 : A.step;
+    const int lw = (A.width + st - 1) / st, lh = (A.height + st - 1) / st;
+    const dim3 grid((lw + kAtW - 1) / kAtW, (lh + kAtH - 1) / kAtH, st * st);
+    atrous_kernel<<<grid, kAtW * kAtH, 0, s>>>(A);
     return cudaGetLastError();
 }
 
