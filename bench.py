@@ -73,7 +73,8 @@ BYTES_SAMPLE_RMW = 20     # accum RGBA32F (16) + variance R32F (4) per pixel sam
 
 KERNEL_SYMBOL = {"render": "render_kernel", "wf_trace": "wf_trace", "wf_shade": "wf_shade",
                  "photon_trace": "photon_trace_kernel", "photon_gather": "photon_gather_kernel",
-                 "atrous": "atrous_kernel", "wf_generate": "wf_generate", "wf_accumulate": "wf_accumulate"}
+                 "atrous": "atrous_kernel", "wf_generate": "wf_generate", "wf_accumulate": "wf_accumulate",
+                 "wf_sort": "wf_sort"}
 
 
 def algorithmic_bytes(kernel: str, ctr: dict, samples: int) -> float:
@@ -573,6 +574,29 @@ def exact_math_line(args, w, sc, cam, sppm, atrous, fast_ctx, stream, device) ->
                                                                 a_ex[..., :3].mean())}}
 
 
+def converged_line(w, sc, cam, device, width=427, height=240) -> dict:
+    """The path tracer's converged image (the export scene and lens, path
+    tracing alone, half resolution): relMSE of the fast build at 1024 spp
+    and of the exact build at the same samples, against an exact 4096-spp
+    render on independent frame indices (2^20 on)."""
+    from retrocam_b200 import api, kpcnn
+    settings = (w.nee_enabled, w.nee_firefly_clamp)
+
+    def mean_image(mode, first, spp):
+        with api.Context(width, height, device.index, mode) as c:
+            c.upload(sc)
+            c.reset()
+            c.render(cam, settings, first, spp)
+            acc = c.read_buffers()[0]
+        return acc[..., :3] / acc[..., 3:4]
+
+    ref = mean_image(api.RC_MATH_EXACT, 1 << 20, 4096)
+    fast = kpcnn.relmse(mean_image(api.RC_MATH_FAST, 0, 1024), ref)
+    exact = kpcnn.relmse(mean_image(api.RC_MATH_EXACT, 0, 1024), ref)
+    return {"relmse_fast_1024spp": fast, "relmse_exact_1024spp": exact, "bound": 1e-3,
+            "reference": f"exact build, 4096 spp, independent seeds, {width}x{height}, path tracer alone"}
+
+
 def small_cornell_line(args, stream, device) -> dict:
     """The small Cornell box (256x256, 16 spp, no SPPM, no denoiser) on the
     B200, device-resident, autotuned shape; the reference arm times the
@@ -741,6 +765,8 @@ def run_b200(args):
         line["exact_math"] = exact_math_line(args, w, sc, cam, sppm, atrous, ctx, stream, device)
     if world == 1 and args.workload != "cornell_small":
         line["cornell_small"] = small_cornell_line(args, stream, device)
+    if world == 1 and not args.no_exact:
+        line["converged"] = converged_line(w, sc, cam, device)
     if rank == 0 and world == 1 and not args.no_quality:
         line["time_to_relmse"] = time_to_relmse(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -171,7 +171,8 @@ typedef struct rc_counters {
 #define RC_KERNEL_KPCNN 10         /* learned denoiser: features, 4 convolutions, filter */
 #define RC_KERNEL_DISPLAY 11       /* ACES + sRGB to RGBA8 (rc_display) */
 #define RC_KERNEL_VHS 12           /* the VHS chain's passes (rc_post_vhs) */
-#define RC_KERNEL_KINDS 13
+#define RC_KERNEL_WF_SORT 13       /* wavefront: misses finished, hits into material queues */
+#define RC_KERNEL_KINDS 14
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */

@@ -137,7 +137,7 @@ class rc_counters(C.Structure):
 
 
 KERNEL_KINDS = ("render", "photon_trace", "photon_gather", "atrous", "normalize", "wf_generate", "wf_trace",
-                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn", "display", "vhs")
+                "wf_shade", "wf_accumulate", "photon_layout", "kpcnn", "display", "vhs", "wf_sort")
 RC_ENGINE_MEGAKERNEL = 0
 RC_ENGINE_WAVEFRONT = 1
 RC_ENGINE_WAVEFRONT_STATIC = 2

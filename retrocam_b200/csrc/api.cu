@@ -34,6 +34,7 @@ cudaError_t launch_display(const DisplayArgs&, cudaStream_t);
 cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
 cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
+cudaError_t launch_wf_sort(const WaveArgs&, cudaStream_t);
 cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace exact
 namespace fast {
@@ -47,6 +48,7 @@ cudaError_t launch_display(const DisplayArgs&, cudaStream_t);
 cudaError_t launch_wf_generate(const WaveArgs&, cudaStream_t);
 cudaError_t launch_wf_trace(const WaveArgs&, cudaStream_t, int block);
 cudaError_t launch_wf_shade(const WaveArgs&, cudaStream_t, int block);
+cudaError_t launch_wf_sort(const WaveArgs&, cudaStream_t);
 cudaError_t launch_wf_accumulate(const WaveArgs&, cudaStream_t);
 }  // namespace fast
 namespace vhs {
@@ -114,7 +116,7 @@ struct rc_ctx {
     int refill_lanes = 16, leaf_quarters = 2;
     int refill_min_paths = 1 << 20;
     DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
-        wf_qlen;
+        wf_qlen, wf_mq;
     int wf_capacity = 0;
     // batched frames (rc_render_frames) and their captured graph
     DevBuf frames;
@@ -311,7 +313,8 @@ int rc_ctx_destroy(rc_ctx* ctx) {
                       &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw, &ctx->seg_powyz,
                       &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
                       &ctx->wf_rad, &ctx->wf_hit, &ctx->wf_res, &ctx->wf_seed, &ctx->wf_rq0, &ctx->wf_rq1,
-                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->frames,
+                      &ctx->wf_sq0, &ctx->wf_sq1, &ctx->wf_srec0, &ctx->wf_srec1, &ctx->wf_qlen, &ctx->wf_mq,
+                      &ctx->frames,
                       &ctx->kp_feat, &ctx->kp_act0, &ctx->kp_act1, &ctx->kp_logits, &ctx->kp_color,
                       &ctx->kp_params, &ctx->kp_packed, &ctx->batch_img, &ctx->batch_segs, &ctx->sp_nodes,
                       &ctx->sp_isect, &ctx->sp_orig, &ctx->df_nodes, &ctx->df_isect, &ctx->ph_queue,
@@ -1023,6 +1026,7 @@ static int wavefront_reserve(rc_ctx* ctx, long cap) {
         CK(ensure(ctx->wf_sq1, n * 4));
         CK(ensure(ctx->wf_srec0, n * 64));
         CK(ensure(ctx->wf_srec1, n * 64));
+        CK(ensure(ctx->wf_mq, n * 4));
         CK(ensure(ctx->wf_qlen, 8 * sizeof(unsigned int)));
         ctx->wf_capacity = (int)cap;
     }
@@ -1054,6 +1058,7 @@ static WaveArgs wave_args(rc_ctx* ctx, const DeviceScene& scene, int nee_enabled
     B.srec[0] = (float4*)ctx->wf_srec0.ptr;
     B.srec[1] = (float4*)ctx->wf_srec1.ptr;
     B.qlen = (unsigned int*)ctx->wf_qlen.ptr;
+    B.mq = (int*)ctx->wf_mq.ptr;
     B.capacity = ctx->wf_capacity;
     A.nee_enabled = nee_enabled;
     A.firefly_clamp = firefly_clamp;
@@ -1084,6 +1089,10 @@ static int wavefront_chunk(rc_ctx* ctx, WaveArgs& A) {
         });
         if (e != cudaSuccess) return launch_err(ctx, e, "wavefront trace");
         if (b == 6) break;
+        e = timed_launch(ctx, RC_KERNEL_WF_SORT, [&] {
+            return ex ? exact::launch_wf_sort(A, ctx->stream) : fast::launch_wf_sort(A, ctx->stream);
+        });
+        if (e != cudaSuccess) return launch_err(ctx, e, "wavefront sort");
         e = timed_launch(ctx, RC_KERNEL_WF_SHADE, [&] {
             return ex ? exact::launch_wf_shade(A, ctx->stream, ctx->shade_block)
                       : fast::launch_wf_shade(A, ctx->stream, ctx->shade_block);

@@ -227,6 +227,9 @@ struct WaveBuffers {
     int* rq[2];       // ray queues (ping-pong by bounce)
     int* sq[2];       // shadow queues
     float4* srec[2];  // shadow records, 4 float4 per queue slot
+    int* mq;          // material queues of the bounce's hits: diffuse paths
+                      // from the front (count qlen[5]), metal and glass
+                      // paths from the back (count qlen[6])
     unsigned int* qlen;
     int capacity;     // paths per chunk
 };

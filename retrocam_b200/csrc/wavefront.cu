@@ -8,8 +8,11 @@
 //     wf_trace     closest hit for the ray queue AND the visibility test of
 //                  the shadow rays the previous shade produced (one launch,
 //                  two queues: a warp only ever holds one kind of ray)
+//     wf_sort      misses finish their path; hits go to material queues
+//                  (diffuse / metal or glass) by warp ballot and block append
 //     wf_shade     emission, Russian roulette, BSDF, NEE light sample
-//                  (pathtrace.comp:454-585); survivors -> next ray queue,
+//                  (pathtrace.comp:454-585) over the material queues, so a
+//                  warp runs one BSDF branch; survivors -> next ray queue,
 //                  NEE rays -> shadow queue
 //   wf_trace       the last bounce's shadow rays
 //   wf_accumulate  per pixel, the samples in frame order, LCA channel
@@ -149,6 +152,8 @@ __global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         B.qlen[prev] = 0u;      // the ray queue shade(bounce) fills
         B.qlen[2 + cur] = 0u;   // the shadow queue shade(bounce) fills
+        B.qlen[5] = 0u;         // the material queues sort(bounce) fills
+        B.qlen[6] = 0u;
     }
     Guard g = {0u, 0u, 0u};
     uint32_t closest = 0, shadow = 0;
@@ -189,8 +194,62 @@ __global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
     }
 }
 
-// One bounce of pathtrace.comp's traceRadiance for every path in ray queue
-// rq[bounce&1] whose closest hit wf_trace has stored.
+// The bounce-0 albedo image is written by the G channel's path (or the only
+// one) of frame 0.
+DI bool albedo_path(const WaveArgs& A, int p, PathId& id, ushort4*& galb) {
+    const FrameSeg& sg = seg_at(A, seg_index(A, p));
+    id = decode(A, sg, p);
+    galb = sg.img.galb;
+    return sg.first_frame + id.sample == 0 && id.channel == (sg.channels == 3 ? 1 : 0);
+}
+
+// Between trace and shade: a path whose ray missed ends here (its radiance
+// so far is final; on bounce 0 the albedo image gets (1,1,1) --
+// pathtrace.comp:476-479 with the first-hit albedo preset); a hit joins the
+// material queue of its surface -- diffuse from the front of mq, metal or
+// glass (pathtrace.comp:504-566) from the back -- so wf_shade's warps each
+// run one BSDF branch.  Appends are block-aggregated (block_append).
+__global__ void __launch_bounds__(256) wf_sort(WaveArgs A) {
+    const WaveBuffers& B = A.wb;
+    const DeviceScene& S = A.scene;
+    const int cur = A.bounce & 1;
+    const int b = A.bounce;
+    const unsigned int n = B.qlen[cur];
+    __shared__ BlockAppend sh;
+    if (threadIdx.x == 0) sh.cnt[0] = sh.cnt[1] = 0u;
+    __syncthreads();
+    // block-uniform trip count: the appends synchronise the block
+    for (unsigned int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const unsigned int i = i0 + threadIdx.x;
+        bool diffuse = false, specular = false;
+        int p = 0;
+        if (i < n) {
+            p = B.rq[cur][i];
+            const int prim = __float_as_int(B.hit[p].w);
+            if (prim < 0) {
+                PathId id;
+                ushort4* galb;
+                if (b == 0 && albedo_path(A, p, id, galb))
+                    galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
+                B.res[p] = b == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : B.rad[p];
+            } else {
+                const int m = __float_as_int(__ldg(S.tri_shade + 3 * prim).w);
+                // wf_shade's branch tests: transmission > 0.5 glass, metallic > 0.5 metal
+                const float metallic = __ldg(S.materials + 4 * m + 0).w;
+                const float transmission = __ldg(S.materials + 4 * m + 2).z;
+                specular = metallic > 0.5f || transmission > 0.5f;
+                diffuse = !specular;
+            }
+        }
+        unsigned int slot_d, slot_s;
+        block_append(sh, diffuse, specular, B.qlen + 5, B.qlen + 6, slot_d, slot_s);
+        if (diffuse) B.mq[slot_d] = p;
+        if (specular) B.mq[B.capacity - 1 - (int)slot_s] = p;
+    }
+}
+
+// One bounce of pathtrace.comp's traceRadiance for every path in the
+// material queues wf_sort filled from ray queue rq[bounce&1] (hits only).
 // Registers capped at 72 (105 uncapped, no spills at 72; 64 spills): the
 // kernel streams path state and waits on memory, so resident warps matter
 // more than registers (7 blocks of 128 threads per SM instead of 4).
@@ -201,7 +260,8 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
     const int nxt = cur ^ 1;
     const int b = A.bounce;
     const bool last = b == 5;
-    const unsigned int n = B.qlen[cur];
+    const unsigned int nd = B.qlen[5];
+    const unsigned int n = nd + B.qlen[6];
     if (blockIdx.x == 0 && threadIdx.x == 0) B.qlen[4] = 0u;  // work counter of the next trace
     __shared__ BlockAppend sh;
     if (threadIdx.x == 0) sh.cnt[0] = sh.cnt[1] = 0u;
@@ -214,7 +274,7 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
         float4 rec0, rec1, rec2, rec3;
         int p = 0;
         if (i < n) {
-            p = B.rq[cur][i];
+            p = i < nd ? B.mq[i] : B.mq[B.capacity - 1 - (int)(i - nd)];
             const float4 hv = B.hit[p];
             const int prim = __float_as_int(hv.w);
             float3 rad = b == 0 ? f3(0.0f, 0.0f, 0.0f) : xyz(B.rad[p]);
@@ -222,16 +282,8 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
             bool alb_path = false;
             PathId id;
             ushort4* galb = nullptr;
-            if (b == 0) {
-                const FrameSeg& sg = seg_at(A, seg_index(A, p));
-                id = decode(A, sg, p);
-                alb_path = sg.first_frame + id.sample == 0 && id.channel == (sg.channels == 3 ? 1 : 0);
-                galb = sg.img.galb;
-            }
-            if (prim < 0) {
-                if (alb_path) galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
-                B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
-            } else {
+            if (b == 0) alb_path = albedo_path(A, p, id, galb);
+            {
                 ++hits;
                 const Ray ray = make_ray(xyz(B.o[p]), xyz(B.d[p]));
                 Hit h;
@@ -503,6 +555,8 @@ DI void trace_dyn(const WaveArgs& A) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         B.qlen[prev] = 0u;
         B.qlen[2 + cur] = 0u;
+        B.qlen[5] = 0u;
+        B.qlen[6] = 0u;
     }
     const unsigned int FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -596,13 +650,14 @@ __global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<tru
 // sized to fill every SM (grid-stride and persistent kernels), once per
 // kernel and block size (64, 128 or 256 threads).
 struct WfGrids {
-    int gen = 0, acc = 0;
+    int gen = 0, acc = 0, sort = 0;
     int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, dyn[3] = {}, dyn4[3] = {};
 };
 static int block_class(int block) { return block <= 64 ? 0 : (block <= 128 ? 1 : 2); }
 static void fill_grids(WfGrids& g) {
     g.gen = grid_for((const void*)wf_generate, 256);
     g.acc = grid_for((const void*)wf_accumulate, 128);
+    g.sort = grid_for((const void*)wf_sort, 256);
     for (int c = 0; c < 3; ++c) {
         const int b = 64 << c;
         g.trace0[c] = grid_for((const void*)wf_trace<false>, b);
@@ -668,6 +723,11 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
 cudaError_t launch_wf_shade(const WaveArgs& A, cudaStream_t s, int block) {
     const int c = block_class(block);
     wf_shade<<<grids().shade[c], 64 << c, 0, s>>>(A);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_sort(const WaveArgs& A, cudaStream_t s) {
+    wf_sort<<<grids().sort, 256, 0, s>>>(A);
     return cudaGetLastError();
 }
 
