@@ -214,6 +214,12 @@ typedef struct rc_tuning {
     int32_t refill_min_paths; /* RC_ENGINE_WAVEFRONT, fast math: chunks of fewer paths are
                                  traced with the grid-stride loop, where a launch holds
                                  about one wave of rays (0 = 1048576; 1 = always refill) */
+    int32_t material_queues;  /* wavefront engines: 1 sorts each bounce's hits into
+                                 material queues (diffuse / metal or glass) before the
+                                 shade, so a warp runs one BSDF branch; 0 shades the ray
+                                 queue as it stands (default: the shade waits on path-state
+                                 memory, not on divergence, and the sort costs more than
+                                 the fuller warps save on the export frame) */
 } rc_tuning;
 
 /* error_word bits. */

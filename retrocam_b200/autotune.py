@@ -39,6 +39,7 @@ KNOBS: dict[str, tuple[int, ...]] = {
     "photon_full_first": (0, 1),
     "refill_lanes": (12, 16, 20, 24, 28),
     "leaf_quarters": (1, 2, 3, 4),
+    "material_queues": (0, 1),
 }
 
 

@@ -203,9 +203,20 @@ DI bool albedo_path(const WaveArgs& A, int p, PathId& id, ushort4*& galb) {
     return sg.first_frame + id.sample == 0 && id.channel == (sg.channels == 3 ? 1 : 0);
 }
 
-// Between trace and shade: a path whose ray missed ends here (its radiance
-// so far is final; on bounce 0 the albedo image gets (1,1,1) --
-// pathtrace.comp:476-479 with the first-hit albedo preset); a hit joins the
+// A path whose ray missed ends: its radiance so far is final; on bounce 0
+// the albedo image gets (1,1,1) (pathtrace.comp:476-479, the first-hit
+// albedo preset).
+DI void finish_miss(const WaveArgs& A, int p, int b) {
+    const WaveBuffers& B = A.wb;
+    PathId id;
+    ushort4* galb;
+    if (b == 0 && albedo_path(A, p, id, galb))
+        galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
+    B.res[p] = b == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : B.rad[p];
+}
+
+// Material queues (rc_tuning.material_queues): between trace and shade, a
+// path whose ray missed ends here (finish_miss) and a hit joins the
 // material queue of its surface -- diffuse from the front of mq, metal or
 // glass (pathtrace.comp:504-566) from the back -- so wf_shade's warps each
 // run one BSDF branch.  Appends are block-aggregated (block_append).
@@ -227,11 +238,7 @@ __global__ void __launch_bounds__(256) wf_sort(WaveArgs A) {
             p = B.rq[cur][i];
             const int prim = __float_as_int(B.hit[p].w);
             if (prim < 0) {
-                PathId id;
-                ushort4* galb;
-                if (b == 0 && albedo_path(A, p, id, galb))
-                    galb[(long)id.py * A.width + id.px] = to_half4(1.0f, 1.0f, 1.0f, 1.0f);
-                B.res[p] = b == 0 ? make_float4(0.0f, 0.0f, 0.0f, 0.0f) : B.rad[p];
+                finish_miss(A, p, b);
             } else {
                 const int m = __float_as_int(__ldg(S.tri_shade + 3 * prim).w);
                 // wf_shade's branch tests: transmission > 0.5 glass, metallic > 0.5 metal
@@ -248,11 +255,13 @@ __global__ void __launch_bounds__(256) wf_sort(WaveArgs A) {
     }
 }
 
-// One bounce of pathtrace.comp's traceRadiance for every path in the
-// material queues wf_sort filled from ray queue rq[bounce&1] (hits only).
+// One bounce of pathtrace.comp's traceRadiance for every path in ray queue
+// rq[bounce&1] whose closest hit wf_trace has stored (misses end here), or,
+// with material queues (kMQ), for the hits wf_sort queued from it.
 // Registers capped at 72 (105 uncapped, no spills at 72; 64 spills): the
 // kernel streams path state and waits on memory, so resident warps matter
 // more than registers (7 blocks of 128 threads per SM instead of 4).
+template <bool kMQ>
 __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
@@ -260,8 +269,8 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
     const int nxt = cur ^ 1;
     const int b = A.bounce;
     const bool last = b == 5;
-    const unsigned int nd = B.qlen[5];
-    const unsigned int n = nd + B.qlen[6];
+    const unsigned int nd = kMQ ? B.qlen[5] : B.qlen[cur];
+    const unsigned int n = kMQ ? nd + B.qlen[6] : nd;
     if (blockIdx.x == 0 && threadIdx.x == 0) B.qlen[4] = 0u;  // work counter of the next trace
     __shared__ BlockAppend sh;
     if (threadIdx.x == 0) sh.cnt[0] = sh.cnt[1] = 0u;
@@ -274,7 +283,7 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
         float4 rec0, rec1, rec2, rec3;
         int p = 0;
         if (i < n) {
-            p = i < nd ? B.mq[i] : B.mq[B.capacity - 1 - (int)(i - nd)];
+            p = !kMQ ? B.rq[cur][i] : (i < nd ? B.mq[i] : B.mq[B.capacity - 1 - (int)(i - nd)]);
             const float4 hv = B.hit[p];
             const int prim = __float_as_int(hv.w);
             float3 rad = b == 0 ? f3(0.0f, 0.0f, 0.0f) : xyz(B.rad[p]);
@@ -283,7 +292,9 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
             PathId id;
             ushort4* galb = nullptr;
             if (b == 0) alb_path = albedo_path(A, p, id, galb);
-            {
+            if (!kMQ && prim < 0) {
+                finish_miss(A, p, b);
+            } else {
                 ++hits;
                 const Ray ray = make_ray(xyz(B.o[p]), xyz(B.d[p]));
                 Hit h;
@@ -651,7 +662,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<tru
 // kernel and block size (64, 128 or 256 threads).
 struct WfGrids {
     int gen = 0, acc = 0, sort = 0;
-    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, dyn[3] = {}, dyn4[3] = {};
+    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, shade_mq[3] = {}, dyn[3] = {}, dyn4[3] = {};
 };
 static int block_class(int block) { return block <= 64 ? 0 : (block <= 128 ? 1 : 2); }
 static void fill_grids(WfGrids& g) {
@@ -662,7 +673,8 @@ static void fill_grids(WfGrids& g) {
         const int b = 64 << c;
         g.trace0[c] = grid_for((const void*)wf_trace<false>, b);
         g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
-        g.shade[c] = grid_for((const void*)wf_shade, b);
+        g.shade[c] = grid_for((const void*)wf_shade<false>, b);
+        g.shade_mq[c] = grid_for((const void*)wf_shade<true>, b);
 #if !RC_EXACT
         g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
         g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
@@ -722,7 +734,10 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
 
 cudaError_t launch_wf_shade(const WaveArgs& A, cudaStream_t s, int block) {
     const int c = block_class(block);
-    wf_shade<<<grids().shade[c], 64 << c, 0, s>>>(A);
+    if (A.material_queues)
+        wf_shade<true><<<grids().shade_mq[c], 64 << c, 0, s>>>(A);
+    else
+        wf_shade<false><<<grids().shade[c], 64 << c, 0, s>>>(A);
     return cudaGetLastError();
 }
 

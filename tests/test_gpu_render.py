@@ -65,17 +65,45 @@ def test_tuning_roundtrip_and_validation(product):
         t = ctx.tuning()
         assert t == {"engine": product.RC_ENGINE_WAVEFRONT, "chunk_paths": 0, "wide_bvh": 0,
                      "trace_block": 128, "shade_block": 128, "photon_block": 128, "photon_full_first": 0,
-                     "refill_lanes": 16, "leaf_quarters": 2, "refill_min_paths": 1 << 20}
+                     "refill_lanes": 16, "leaf_quarters": 2, "refill_min_paths": 1 << 20, "material_queues": 0}
         ctx.set_tuning(engine=product.RC_ENGINE_WAVEFRONT_STATIC, wide_bvh=3, trace_block=256, shade_block=64)
         t = ctx.tuning()
         assert (t["engine"], t["wide_bvh"], t["trace_block"], t["shade_block"]) == (2, 3, 256, 64)
         for bad in ({"engine": 7}, {"chunk_paths": -1}, {"wide_bvh": 4}, {"trace_block": 96},
                     {"photon_block": 512}, {"photon_full_first": 2},
-                    {"refill_lanes": 33}, {"leaf_quarters": 5}, {"refill_min_paths": -1}):
+                    {"refill_lanes": 33}, {"leaf_quarters": 5}, {"refill_min_paths": -1},
+                    {"material_queues": 2}):
             with pytest.raises(product.RetroCamError) as e:
                 ctx.set_tuning(**bad)
             assert e.value.code == product.RC_ERR_INVALID_ARG
         assert ctx.tuning() == t   # a rejected call changes nothing
+
+
+@pytest.mark.parametrize("mode", ["exact", "fast"])
+@pytest.mark.parametrize("engine", ("wavefront", "wavefront_static"))
+def test_material_queues_change_nothing(product, orc, c1, mode, engine):
+    """Shading each bounce's hits from material queues (misses finished by
+    the sort kernel) only reorders independent paths: bit-identical images
+    in both builds, and in exact math the oracle's."""
+    w, sc, cam = c1
+    cam = dict(cam)
+    W, H, spp = 96, 64, 3
+    m = product.RC_MATH_EXACT if mode == "exact" else product.RC_MATH_FAST
+    out = []
+    for mq in (0, 1):
+        with _ctx(product, W, H, m, engine) as ctx:
+            ctx.set_tuning(material_queues=mq)
+            ctx.set_kernel_timing(True)
+            ctx.upload(sc)
+            ctx.render(cam, (1, 1.0), 0, spp)
+            out.append(ctx.read_buffers())
+            sorted_launches = ctx.kernel_times()["wf_sort"][1]
+            assert (sorted_launches > 0) == (mq == 1)
+            assert ctx.counters()["error_word"] == 0
+    _same_images(out[1], out[0])
+    if mode == "exact":
+        cpu, _ = orc.render(sc, cam, (1, 1.0), W, H, 0, spp)
+        _same_images(out[1], cpu)
 
 
 def test_exact_results_independent_of_tuning(product, orc, c1):
