@@ -23,6 +23,8 @@ of export/RenderPipeline.java:209-239, issued through rc_render_frame.
   exact_math  the same frame in the bit-exact build, and how many pixels of
          the fast build agree with it within 1e-4 at 1 spp
   cornell_small  the small Cornell box (256x256 x 16 spp) on the B200
+  bvh_stress  the 1M-triangle scene (854x480 x 32 spp), device-resident
+  keyframes  the 64-frame keyframed batch under one CUDA graph
   time_to_relmse  the metric's second half (64 held-out Cornell variants,
          every integer spp to 16, a 5x5 box filter as control); one GPU only
   cpu_baseline  the reference's own shaders compiled for the host
@@ -149,6 +151,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-quality", action="store_true", help="skip the time-to-relMSE comparison")
     ap.add_argument("--quality-variants", type=int, default=64, help="held-out Cornell variants for time-to-relMSE")
     ap.add_argument("--no-exact", action="store_true", help="skip the exact-math line")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the 1M-triangle and keyframed-batch lines")
     ap.add_argument("--spp", type=int, default=0, help="override spp (profiling of a small case)")
     ap.add_argument("--sppm-iterations", type=int, default=-1, help="override SPPM iterations")
     return ap.parse_args(argv)
@@ -620,6 +624,66 @@ def small_cornell_line(args, stream, device) -> dict:
             "config": "256x256, 16 spp, 6 bounces, 35 mm f/16, 36 triangles"}
 
 
+def stress_line(args, stream, device) -> dict:
+    """The 1M-triangle scene (854x480, 32 spp, no SPPM, no denoiser; about
+    160 MB of BVH and triangles, larger than L2), device-resident frames,
+    autotuned shape (warm-up 3, then the timed frames)."""
+    import torch
+    from retrocam_b200 import api, autotune, scenes
+    w = scenes.bvh_stress()
+    t0 = time.perf_counter()
+    sc = api.build_scene(w.scene)
+    build_s = time.perf_counter() - t0
+    cam = api.workload_camera(w)
+    settings = (w.nee_enabled, w.nee_firefly_clamp)
+    atrous = api.atrous_params(scenes.AtrousDesc(enabled=0))
+    with api.Context(w.width, w.height, device.index, api.RC_MATH_FAST) as c:
+        c.set_stream(stream.cuda_stream)
+        c.upload(sc)
+        key = autotune.cache_key(torch.cuda.get_device_name(device), w.width, w.height, api.RC_MATH_FAST,
+                                 autotune.scene_signature(sc))
+        t = autotune.TuningCache().get(key)
+        if t:
+            c.set_tuning(**t)
+        ms = device_timed(lambda: c.render_frame(cam, settings, w.spp, None, 0.05, 0, atrous, read=False),
+                          max(1, min(args.steps, 5)), 3, stream)
+        ctr = c.counters()
+    return {"value": w.width * w.height * w.spp / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_frame": ms,
+            "triangles": len(sc["tris"]), "nodes": len(sc["nodes"]), "bvh_depth": int(ctr["bvh_depth"]),
+            "host_bvh_build_s": build_s, "config": "854x480, 32 spp, 6 bounces, no SPPM, no denoiser"}
+
+
+def keyframes_line(args, stream, device) -> dict:
+    """The 64-frame keyframed batch (spp U{8..128}, SPPM iterations U{4..16})
+    as one rc_render_frames call under a CUDA graph: samples of all frames
+    over the device time of the batch (one warm-up batch, which also
+    captures the graph, then two timed)."""
+    from retrocam_b200 import api, autotune, scenes
+    import torch
+    w = scenes.export_frame()
+    sc = api.build_scene(w.scene)
+    frames = scenes.keyframe_batch(api.HOST, 64, 1)
+    sppm = api.rc_sppm_params(w.sppm.photons, w.sppm.hash_size, w.sppm.alpha)
+    atrous = api.atrous_params(w.atrous)
+    settings = (w.nee_enabled, w.nee_firefly_clamp)
+    with api.Context(w.width, w.height, device.index, api.RC_MATH_FAST) as c:
+        c.set_stream(stream.cuda_stream)
+        c.upload(sc)
+        key = autotune.cache_key(torch.cuda.get_device_name(device), w.width, w.height, api.RC_MATH_FAST,
+                                 autotune.scene_signature(sc))
+        t = autotune.TuningCache().get(key)
+        if t:
+            c.set_tuning(**t)
+        ms = device_timed(lambda: c.render_frames(frames, settings, sppm, w.sppm.r0, atrous, use_graph=True,
+                                                  read=False), 2, 1, stream)
+        if c.counters()["error_word"]:
+            raise RuntimeError("kernel guard raised in the keyframed batch")
+    samples = sum(s for _, s, _ in frames) * w.width * w.height
+    return {"value": samples / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_batch": ms, "frames": len(frames),
+            "spp_total": sum(s for _, s, _ in frames), "sppm_iterations_total": sum(i for _, _, i in frames),
+            "config": "64 keyframed export frames, one rc_render_frames call under a CUDA graph"}
+
+
 def run_b200(args):
     import torch
     from retrocam_b200 import api, build
@@ -767,6 +831,9 @@ def run_b200(args):
         line["cornell_small"] = small_cornell_line(args, stream, device)
     if world == 1 and not args.no_exact:
         line["converged"] = converged_line(w, sc, cam, device)
+    if world == 1 and args.workload == "export_frame" and not args.no_configs:
+        line["bvh_stress"] = stress_line(args, stream, device)
+        line["keyframes"] = keyframes_line(args, stream, device)
     if rank == 0 and world == 1 and not args.no_quality:
         line["time_to_relmse"] = time_to_relmse(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
