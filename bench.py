@@ -147,6 +147,8 @@ def parse_args(argv=None):
                     help="auto: the autotuner's launch shape for this GPU and workload (cached)")
     ap.add_argument("--retune", action="store_true", help="with --engine auto: tune again, ignore the cache")
     ap.add_argument("--chunk-paths", type=int, default=0, help="wavefront paths in flight (0: default)")
+    ap.add_argument("--material-queues", action="store_true",
+                    help="shade each bounce's hits from material queues (rc_tuning.material_queues)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the time-to-relMSE comparison")
     ap.add_argument("--quality-variants", type=int, default=64, help="held-out Cornell variants for time-to-relMSE")
@@ -713,6 +715,8 @@ def run_b200(args):
     else:
         ctx.set_engine({"wavefront": api.RC_ENGINE_WAVEFRONT, "wavefront_static": api.RC_ENGINE_WAVEFRONT_STATIC,
                         "megakernel": api.RC_ENGINE_MEGAKERNEL}[args.engine], args.chunk_paths)
+    if args.material_queues:
+        ctx.set_tuning(material_queues=1)
     tuning = ctx.tuning()
 
     if world > 1:
