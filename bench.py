@@ -149,6 +149,8 @@ def parse_args(argv=None):
     ap.add_argument("--chunk-paths", type=int, default=0, help="wavefront paths in flight (0: default)")
     ap.add_argument("--material-queues", action="store_true",
                     help="shade each bounce's hits from material queues (rc_tuning.material_queues)")
+    ap.add_argument("--tune", action="append", default=[], metavar="KNOB=VALUE",
+                    help="set an rc_tuning knob after the autotuned shape (repeatable)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-quality", action="store_true", help="skip the time-to-relMSE comparison")
     ap.add_argument("--quality-variants", type=int, default=64, help="held-out Cornell variants for time-to-relMSE")
@@ -717,6 +719,9 @@ def run_b200(args):
                         "megakernel": api.RC_ENGINE_MEGAKERNEL}[args.engine], args.chunk_paths)
     if args.material_queues:
         ctx.set_tuning(material_queues=1)
+    for kv in args.tune:
+        k, _, v = kv.partition("=")
+        ctx.set_tuning(**{k: int(v)})
     tuning = ctx.tuning()
 
     if world > 1:

@@ -121,7 +121,8 @@ class rc_tuning(C.Structure):
     _fields_ = [("engine", C.c_int32), ("chunk_paths", C.c_int32), ("wide_bvh", C.c_int32),
                 ("trace_block", C.c_int32), ("shade_block", C.c_int32), ("photon_block", C.c_int32),
                 ("photon_full_first", C.c_int32), ("refill_lanes", C.c_int32), ("leaf_quarters", C.c_int32),
-                ("refill_min_paths", C.c_int32), ("material_queues", C.c_int32)]
+                ("refill_min_paths", C.c_int32), ("material_queues", C.c_int32),
+                ("interior_steps", C.c_int32)]
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

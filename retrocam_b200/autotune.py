@@ -40,6 +40,7 @@ KNOBS: dict[str, tuple[int, ...]] = {
     "refill_lanes": (12, 16, 20, 24, 28),
     "leaf_quarters": (1, 2, 3, 4),
     "material_queues": (0, 1),
+    "interior_steps": (2, 4, 6, 8),
 }
 
 

@@ -116,6 +116,7 @@ struct rc_ctx {
     int refill_lanes = 16, leaf_quarters = 2;
     int refill_min_paths = 1 << 20;
     int material_queues = 0;
+    int interior_steps = 6;
     DevBuf wf_o, wf_d, wf_thr, wf_rad, wf_hit, wf_res, wf_seed, wf_rq0, wf_rq1, wf_sq0, wf_sq1, wf_srec0, wf_srec1,
         wf_qlen, wf_mq;
     int wf_capacity = 0;
@@ -950,13 +951,13 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
         !valid_block(t->shade_block) || !valid_block(t->photon_block) ||
         (t->photon_full_first != 0 && t->photon_full_first != 1) || t->refill_lanes < 0 || t->refill_lanes > 32 ||
         t->leaf_quarters < 0 || t->leaf_quarters > 4 || t->refill_min_paths < 0 ||
-        (t->material_queues != 0 && t->material_queues != 1))
+        (t->material_queues != 0 && t->material_queues != 1) || t->interior_steps < 0 || t->interior_steps > 8)
         return fail(ctx, RC_ERR_INVALID_ARG,
                     "rc_set_tuning: engine %d chunk %d wide %d blocks %d/%d/%d first %d refill %d leaf %d "
-                    "refill_min %d material_queues %d",
+                    "refill_min %d material_queues %d interior_steps %d",
                     t->engine, t->chunk_paths, t->wide_bvh, t->trace_block, t->shade_block, t->photon_block,
                     t->photon_full_first, t->refill_lanes, t->leaf_quarters, t->refill_min_paths,
-                    t->material_queues);
+                    t->material_queues, t->interior_steps);
     ctx->engine = t->engine;
     ctx->chunk_paths = t->chunk_paths;
     ctx->wide_bvh = t->wide_bvh;
@@ -968,6 +969,7 @@ int rc_set_tuning(rc_ctx* ctx, const rc_tuning* t) {
     ctx->leaf_quarters = t->leaf_quarters ? t->leaf_quarters : 2;
     ctx->refill_min_paths = t->refill_min_paths ? t->refill_min_paths : (1 << 20);
     ctx->material_queues = t->material_queues;
+    ctx->interior_steps = t->interior_steps ? t->interior_steps : 6;
     return RC_OK;
 }
 
@@ -985,6 +987,7 @@ int rc_get_tuning(rc_ctx* ctx, rc_tuning* out) {
     out->leaf_quarters = ctx->leaf_quarters;
     out->refill_min_paths = ctx->refill_min_paths;
     out->material_queues = ctx->material_queues;
+    out->interior_steps = ctx->interior_steps;
     return RC_OK;
 }
 
@@ -1075,6 +1078,7 @@ static WaveArgs wave_args(rc_ctx* ctx, const DeviceScene& scene, int nee_enabled
     A.refill_lanes = ctx->refill_lanes;
     A.leaf_quarters = ctx->leaf_quarters;
     A.material_queues = ctx->material_queues;
+    A.interior_steps = ctx->interior_steps;
     A.bounce = 0;
     return A;
 }
@@ -1939,10 +1943,10 @@ int rc_render_frames(rc_ctx* ctx, const rc_frame_desc* frames, int n_frames, con
                                 &ctx->seg_powyz, &ctx->ph_queue, &ctx->ph_queue_len, &ctx->gcache,
                                 &ctx->batch_gcache, &ctx->gheavy})
             key = fnv1a(key, &b->ptr, sizeof(void*));
-        const int shape[11] = {ctx->chunk_paths,  ctx->wide_bvh,       ctx->trace_block,
+        const int shape[12] = {ctx->chunk_paths,  ctx->wide_bvh,       ctx->trace_block,
                                ctx->shade_block,  ctx->photon_block,   ctx->width,
                                ctx->photon_full_first, ctx->refill_lanes, ctx->leaf_quarters,
-                               ctx->refill_min_paths, ctx->material_queues};
+                               ctx->refill_min_paths, ctx->material_queues, ctx->interior_steps};
         key = fnv1a(key, shape, sizeof(shape));
         if (!ctx->graph_exec || ctx->graph_key != key) {
             if (ctx->graph_exec) {

@@ -267,6 +267,7 @@ struct WaveArgs {
     int refill_lanes;  // refill when fewer lanes than this are busy (1..32)
     int leaf_quarters; // leaf phase once this many quarters of the busy lanes are blocked (1..4)
     int material_queues; // wf_sort ran: wf_shade walks the material queues (hits only)
+    int interior_steps;  // refill trace: tree moves per lane per scheduling round (1..8)
     DevCounters* counters;
 };
 

@@ -89,22 +89,26 @@ DI void dyn_start(const Scn& S, LaneRay& L, float tmax, bool any, Guard& g) {
                   !(tmin > L.h.t);
 }
 
-// The warp's choice for this iteration; every lane of the warp calls it.
-// Returns whether this lane steps, and the phase.
-DI bool dyn_schedule(const LaneRay& L, bool busy, int leaf_quarters, bool& leaf_phase) {
+// The warp's choice for this iteration; every lane of the warp calls it with
+// the warp's busy mask `act` (the caller's ballot of `busy`).  Returns
+// whether this lane steps, and the phase.
+DI bool dyn_schedule(const LaneRay& L, bool busy, unsigned int act, int leaf_quarters, bool& leaf_phase) {
     const unsigned int FULL = 0xffffffffu;
     const bool blocked = busy && L.leaf.cnt > 0 && (!L.have_node || L.node.cnt > 0);
-    const unsigned int act = __ballot_sync(FULL, busy);
     const unsigned int parked = __ballot_sync(FULL, busy && L.leaf.cnt > 0);
     const unsigned int blk = __ballot_sync(FULL, blocked);
     leaf_phase = parked == act || 4 * __popc(blk) >= leaf_quarters * __popc(act);
     return busy && (leaf_phase ? L.leaf.cnt > 0 : !blocked);
 }
 
-// One step of L (kWide: interior nodes from S.nodes4).  Returns true when
-// the ray is finished: its walk ended, an any-hit ray hit, or the step cap.
+// One step of L (kWide: interior nodes from S.nodes4): in the leaf phase the
+// parked leaf's triangles; otherwise up to `interior_steps` moves through
+// the tree -- interior nodes, or parking a reached leaf -- while the lane is
+// not blocked (a leaf parked and the next node a leaf too, or none), so the
+// warp's scheduling work is shared by several moves.  Returns true when the
+// ray is finished: its walk ended, an any-hit ray hit, or the step cap.
 template <bool kWide, class Scn>
-DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g) {
+DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
     bool done = false;
     if (leaf_phase) {
         for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
@@ -121,79 +125,83 @@ DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g)
             }
         }
         L.leaf.cnt = 0;
-    } else if (L.have_node) {
-        if (L.node.cnt > 0) {
-            L.leaf = L.node;
-            L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
-        } else if (kWide) {
-            // 4-wide node: hit children ordered by entry distance, the
-            // nearest entered, the others pushed far to near
-            const Node4* n4 = S.nodes4 + L.node.ref;
-            const float4 lx = __ldg(&n4->lox), hx = __ldg(&n4->hix), ly = __ldg(&n4->loy);
-            const float4 hy = __ldg(&n4->hiy), lz = __ldg(&n4->loz), hz = __ldg(&n4->hiz);
-            const int4 cr = __ldg(&n4->ref), cc = __ldg(&n4->cnt);
-            const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
-            const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
-            const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
-            const int CR[4] = {cr.x, cr.y, cr.z, cr.w}, CC[4] = {cc.x, cc.y, cc.z, cc.w};
-            float t4[4];
-            unsigned int key[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const bool hit = CC[k] >= 0 && tslab(g, L.r, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k], t4[k]) &&
-                                 !(t4[k] > L.h.t);
-                key[k] = hit ? ((__float_as_uint(fmaxf(t4[k], 0.0f)) & ~3u) | (unsigned int)k) : 0xffffffffu;
-            }
-            cswap(key[0], key[1]);
-            cswap(key[2], key[3]);
-            cswap(key[0], key[2]);
-            cswap(key[1], key[3]);
-            cswap(key[1], key[2]);
-            if (key[0] == 0xffffffffu) {
+    } else {
+        for (int m = 0; m < interior_steps && L.have_node; ++m) {
+            if (L.node.cnt > 0) {
+                if (L.leaf.cnt > 0) break;   // blocked: a leaf is parked already
+                L.leaf = L.node;
                 L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
-            } else {
-#pragma unroll
-                for (int k = 3; k >= 1; --k) {
-                    if (key[k] != 0xffffffffu) {
-                        if (L.top < kDynStack) {
-                            const int s = key[k] & 3u;
-                            stk[L.top++] =
-                                make_int2(CR[s], (CC[s] & 0xffff) | (__float_as_int(t4[s]) & (int)0xffff0000));
-                        } else {
-                            g.flags |= RC_GUARD_TRAVERSAL_CAP;
+            } else if (kWide) {
+                // 4-wide node: hit children ordered by entry distance, the
+                // nearest entered, the others pushed far to near
+                const Node4* n4 = S.nodes4 + L.node.ref;
+                const float4 lx = __ldg(&n4->lox), hx = __ldg(&n4->hix), ly = __ldg(&n4->loy);
+                const float4 hy = __ldg(&n4->hiy), lz = __ldg(&n4->loz), hz = __ldg(&n4->hiz);
+                const int4 cr = __ldg(&n4->ref), cc = __ldg(&n4->cnt);
+                const float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
+                const float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
+                const float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+                const int CR[4] = {cr.x, cr.y, cr.z, cr.w}, CC[4] = {cc.x, cc.y, cc.z, cc.w};
+                float t4[4];
+                unsigned int key[4];
+    #pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const bool hit = CC[k] >= 0 && tslab(g, L.r, LX[k], LY[k], LZ[k], HX[k], HY[k], HZ[k], t4[k]) &&
+                                     !(t4[k] > L.h.t);
+                    key[k] = hit ? ((__float_as_uint(fmaxf(t4[k], 0.0f)) & ~3u) | (unsigned int)k) : 0xffffffffu;
+                }
+                cswap(key[0], key[1]);
+                cswap(key[2], key[3]);
+                cswap(key[0], key[2]);
+                cswap(key[1], key[3]);
+                cswap(key[1], key[2]);
+                if (key[0] == 0xffffffffu) {
+                    L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                } else {
+    #pragma unroll
+                    for (int k = 3; k >= 1; --k) {
+                        if (key[k] != 0xffffffffu) {
+                            if (L.top < kDynStack) {
+                                const int s = key[k] & 3u;
+                                stk[L.top++] =
+                                    make_int2(CR[s], (CC[s] & 0xffff) | (__float_as_int(t4[s]) & (int)0xffff0000));
+                            } else {
+                                g.flags |= RC_GUARD_TRAVERSAL_CAP;
+                            }
                         }
                     }
+                    const int s0 = key[0] & 3u;
+                    L.node.ref = CR[s0];
+                    L.node.cnt = CC[s0];
                 }
-                const int s0 = key[0] & 3u;
-                L.node.ref = CR[s0];
-                L.node.cnt = CC[s0];
-            }
-        } else {
-            const NodeRec* nrec = S.nodes + L.node.ref;
-            const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
-            const int4 d = __ldg(&nrec->d);
-            float tl, tr;
-            const bool hl = tslab(g, L.r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > L.h.t);
-            const bool hr = tslab(g, L.r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > L.h.t);
-            if (hl && hr) {
-                const bool left_first = tl < tr;
-                if (L.top < 62) {
-                    const float tf = left_first ? tr : tl;
-                    const int cf = left_first ? d.w : d.y;
-                    stk[L.top++] =
-                        make_int2(left_first ? d.z : d.x, (cf & 0xffff) | (__float_as_int(tf) & (int)0xffff0000));
-                }
-                L.node.ref = left_first ? d.x : d.z;
-                L.node.cnt = left_first ? d.y : d.w;
-            } else if (hl) {
-                L.node.ref = d.x;
-                L.node.cnt = d.y;
-            } else if (hr) {
-                L.node.ref = d.z;
-                L.node.cnt = d.w;
             } else {
-                L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                const NodeRec* nrec = S.nodes + L.node.ref;
+                const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
+                const int4 d = __ldg(&nrec->d);
+                float tl, tr;
+                const bool hl = tslab(g, L.r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > L.h.t);
+                const bool hr = tslab(g, L.r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > L.h.t);
+                if (hl && hr) {
+                    const bool left_first = tl < tr;
+                    if (L.top < 62) {
+                        const float tf = left_first ? tr : tl;
+                        const int cf = left_first ? d.w : d.y;
+                        stk[L.top++] =
+                            make_int2(left_first ? d.z : d.x, (cf & 0xffff) | (__float_as_int(tf) & (int)0xffff0000));
+                    }
+                    L.node.ref = left_first ? d.x : d.z;
+                    L.node.cnt = left_first ? d.y : d.w;
+                } else if (hl) {
+                    L.node.ref = d.x;
+                    L.node.cnt = d.y;
+                } else if (hr) {
+                    L.node.ref = d.z;
+                    L.node.cnt = d.w;
+                } else {
+                    L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                }
             }
+            if (m + 1 < interior_steps && ++L.steps > 4 * S.node_count + 64) break;
         }
     }
     if (!L.have_node && L.leaf.cnt == 0) done = true;

@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(128) photon_emit_dyn(PhotonArgs A) {
             bool busy = L.item >= 0;
             bool push = false;
             bool leaf_phase;
-            if (dyn_schedule(L, busy, A.leaf_quarters, leaf_phase) &&
+            if (dyn_schedule(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
                 dyn_step<false>(step_scene(second, A.spec, A.diff), L, stk, leaf_phase, g)) {
                 if (!second && L.h.prim >= 0) {
                     hs = L.h;

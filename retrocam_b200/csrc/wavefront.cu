@@ -608,11 +608,11 @@ DI void trace_dyn(const WaveArgs& A) {
             }
         }
         if (__all_sync(FULL, L.item == -2)) break;
-        // ---- advance the rays ----
         while (true) {
             bool busy = L.item >= 0;
             bool leaf_phase;
-            if (dyn_schedule(L, busy, A.leaf_quarters, leaf_phase) && dyn_step<kWide>(S, L, stk, leaf_phase, g)) {
+            if (dyn_schedule(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
+                dyn_step<kWide>(S, L, stk, leaf_phase, g, A.interior_steps)) {
                 const int item = L.item;
                 if ((unsigned int)item < nr) {
                     const int p = B.rq[cur][item];
@@ -630,8 +630,7 @@ DI void trace_dyn(const WaveArgs& A) {
                 L.item = -1;
                 busy = false;
             }
-            const unsigned int still = __ballot_sync(FULL, busy);
-            if (__popc(still) < A.refill_lanes) break;
+            if (__popc(__ballot_sync(FULL, busy)) < A.refill_lanes) break;
         }
     }
     const unsigned int c = __reduce_add_sync(FULL, closest);

@@ -9,7 +9,7 @@ class FakeCtx:
     def __init__(self, cost):
         self.t = {"engine": 1, "chunk_paths": 0, "wide_bvh": 0, "trace_block": 128, "shade_block": 128,
                   "photon_block": 128, "photon_full_first": 0, "refill_lanes": 20, "leaf_quarters": 2,
-                  "material_queues": 0}
+                  "material_queues": 0, "interior_steps": 1}
         self.cost = cost
         self.calls = 0
 
@@ -26,7 +26,7 @@ class FakeCtx:
 def test_coordinate_descent_finds_separable_optimum():
     want = {"engine": 2, "chunk_paths": 32 << 20, "wide_bvh": 3, "trace_block": 64, "shade_block": 256,
             "photon_block": 64, "photon_full_first": 1, "refill_lanes": 28, "leaf_quarters": 3,
-            "material_queues": 1}
+            "material_queues": 1, "interior_steps": 4}
 
     def cost(t):
         return 100.0 + sum(10.0 for k in want if t[k] != want[k])

@@ -60,19 +60,36 @@ def test_fast_dynamic_fetch_matches_static_schedule(product, c1):
     assert same > 0.995, same
 
 
+def test_refill_interior_steps_change_nothing(product, c1):
+    """The refill trace's per-round budget of tree moves changes only when a
+    lane moves, not where: every budget gives the same hits, bit for bit."""
+    w, sc, cam = c1
+    out = []
+    for steps in (1, 2, 6, 8):
+        with _ctx(product, 160, 90, product.RC_MATH_FAST, "wavefront") as ctx:
+            ctx.set_tuning(interior_steps=steps)
+            ctx.upload(sc)
+            ctx.render(cam, (1, 1.0), 0, 4)
+            out.append(ctx.read_buffers())
+            assert ctx.counters()["error_word"] == 0
+    for o in out[1:]:
+        _same_images(o, out[0])
+
+
 def test_tuning_roundtrip_and_validation(product):
     with product.Context(64, 64, 0, product.RC_MATH_FAST) as ctx:
         t = ctx.tuning()
         assert t == {"engine": product.RC_ENGINE_WAVEFRONT, "chunk_paths": 0, "wide_bvh": 0,
                      "trace_block": 128, "shade_block": 128, "photon_block": 128, "photon_full_first": 0,
-                     "refill_lanes": 16, "leaf_quarters": 2, "refill_min_paths": 1 << 20, "material_queues": 0}
+                     "refill_lanes": 16, "leaf_quarters": 2, "refill_min_paths": 1 << 20, "material_queues": 0,
+                     "interior_steps": 6}
         ctx.set_tuning(engine=product.RC_ENGINE_WAVEFRONT_STATIC, wide_bvh=3, trace_block=256, shade_block=64)
         t = ctx.tuning()
         assert (t["engine"], t["wide_bvh"], t["trace_block"], t["shade_block"]) == (2, 3, 256, 64)
         for bad in ({"engine": 7}, {"chunk_paths": -1}, {"wide_bvh": 4}, {"trace_block": 96},
                     {"photon_block": 512}, {"photon_full_first": 2},
                     {"refill_lanes": 33}, {"leaf_quarters": 5}, {"refill_min_paths": -1},
-                    {"material_queues": 2}):
+                    {"material_queues": 2}, {"interior_steps": 9}):
             with pytest.raises(product.RetroCamError) as e:
                 ctx.set_tuning(**bad)
             assert e.value.code == product.RC_ERR_INVALID_ARG
