@@ -555,9 +555,16 @@ def exact_math_line(args, w, sc, cam, sppm, atrous, fast_ctx, stream, device) ->
     settings = (w.nee_enabled, w.nee_firefly_clamp)
     iters = w.sppm.iterations if w.sppm is not None else 0
     r0 = w.sppm.r0 if w.sppm is not None else 0.05
+    import torch
+    from retrocam_b200 import autotune
     with api.Context(w.width, w.height, device.index, api.RC_MATH_EXACT) as ex:
         ex.set_stream(stream.cuda_stream)
         ex.upload(sc)
+        # the autotuned shape for exact math when the table has one
+        t = autotune.TuningCache().get(autotune.cache_key(torch.cuda.get_device_name(device), w.width, w.height,
+                                                          api.RC_MATH_EXACT, autotune.scene_signature(sc)))
+        if t:
+            ex.set_tuning(**t)
         steps = max(1, min(args.steps, 5))
         ms = device_timed(lambda: ex.render_frame(cam, settings, w.spp, sppm, r0, iters, atrous, read=False),
                           steps, max(3, min(args.warmup, 3)), stream)
@@ -573,7 +580,7 @@ def exact_math_line(args, w, sc, cam, sppm, atrous, fast_ctx, stream, device) ->
     rel = np.abs(a_fa[..., :3] - a_ex[..., :3]) / np.maximum(np.abs(a_ex[..., :3]), 1e-3)
     within = np.all(rel <= 1e-4, axis=-1)
     return {"value": w.width * w.height * w.spp / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms,
-            "steps": steps, "engine": tuning["engine"],
+            "steps": steps, "tuning": tuning,
             "fast_vs_exact_1spp": {"pixels_within_1e-4_rel": float(within.mean()),
                                    "pixels_bit_identical": float(np.all(a_fa[..., :3].view(np.uint32) ==
                                                                         a_ex[..., :3].view(np.uint32),

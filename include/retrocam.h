@@ -176,11 +176,12 @@ typedef struct rc_counters {
 
 /* Path-tracer engines (rc_set_engine). */
 #define RC_ENGINE_MEGAKERNEL 0  /* one thread per pixel runs whole paths */
-#define RC_ENGINE_WAVEFRONT 1   /* per-bounce kernels over compacted path queues;
-                                   fast math traces with a persistent kernel
-                                   that refills idle lanes with new rays
-                                   (chunks of rc_tuning.refill_min_paths
-                                   paths or more; smaller ones grid-stride) */
+#define RC_ENGINE_WAVEFRONT 1   /* per-bounce kernels over compacted path queues,
+                                   traced with a persistent kernel that refills
+                                   idle lanes with new rays (chunks of
+                                   rc_tuning.refill_min_paths paths or more;
+                                   smaller ones grid-stride); in exact math a
+                                   ray keeps the reference's visiting order */
 #define RC_ENGINE_WAVEFRONT_STATIC 2 /* as above, traced with a grid-stride loop */
 
 /* rc_tuning.wide_bvh bits: which rays traverse the 4-wide copy of the BVH
@@ -211,15 +212,17 @@ typedef struct rc_tuning {
     int32_t leaf_quarters; /* RC_ENGINE_WAVEFRONT trace: a warp tests its parked leaves
                               once this many quarters of its busy lanes cannot step on
                               (or all have a leaf parked), 1..4 (0 = 2) */
-    int32_t refill_min_paths; /* RC_ENGINE_WAVEFRONT, fast math: chunks of fewer paths are
+    int32_t refill_min_paths; /* RC_ENGINE_WAVEFRONT: chunks of fewer paths are
                                  traced with the grid-stride loop, where a launch holds
                                  about one wave of rays (0 = 1048576; 1 = always refill) */
     int32_t material_queues;  /* wavefront engines: 1 sorts each bounce's hits into
                                  material queues (diffuse / metal or glass) before the
                                  shade, so a warp runs one BSDF branch; 0 shades the ray
-                                 queue as it stands (default: the shade waits on path-state
-                                 memory, not on divergence, and the sort costs more than
-                                 the fuller warps save on the export frame) */
+                                 queue as it stands (default: in fast math the shade waits
+                                 on path-state memory, not on divergence, and the sort costs
+                                 more than the fuller warps save on the export frame; the
+                                 exact build's heavier shade gains, and its tuned shape on
+                                 the B200 sets it) */
     int32_t interior_steps;   /* RC_ENGINE_WAVEFRONT trace: moves through the tree a lane
                                  makes per scheduling round of its warp, 1..8 (0 = 6: the
                                  warp's ballots and phase choice are shared by up to six

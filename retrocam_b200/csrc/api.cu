@@ -366,9 +366,11 @@ int rc_synchronize(rc_ctx* ctx) {
 static void node_record(const rc_bvh_node* nodes, const rc_bvh_node& n, NodeRec& r) {
     const rc_bvh_node& L = nodes[n.left_child];
     const rc_bvh_node& R = nodes[n.right_child];
-    r.a = make_float4(L.aabb_min[0], L.aabb_min[1], L.aabb_min[2], L.aabb_max[0]);
-    r.b = make_float4(L.aabb_max[1], L.aabb_max[2], R.aabb_min[0], R.aabb_min[1]);
-    r.c = make_float4(R.aabb_min[2], R.aabb_max[0], R.aabb_max[1], R.aabb_max[2]);
+    // x and y bounds of each box side by side (one register pair each for
+    // the paired FMA of the fast build's slab test), the z bounds together
+    r.a = make_float4(L.aabb_min[0], L.aabb_min[1], L.aabb_max[0], L.aabb_max[1]);
+    r.b = make_float4(R.aabb_min[0], R.aabb_min[1], R.aabb_max[0], R.aabb_max[1]);
+    r.c = make_float4(L.aabb_min[2], L.aabb_max[2], R.aabb_min[2], R.aabb_max[2]);
     r.d = make_int4(L.prim_count > 0 ? L.prim_start : n.left_child, L.prim_count,
                     R.prim_count > 0 ? R.prim_start : n.right_child, R.prim_count);
 }
@@ -1286,6 +1288,7 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
     A.work = (unsigned int*)ctx->ph_queue_len.ptr + 1;
     A.refill_lanes = ctx->refill_lanes;
     A.leaf_quarters = ctx->leaf_quarters;
+    A.interior_steps = ctx->interior_steps;
     A.counters = ctx->counters;
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
     cudaError_t e = timed_launch(

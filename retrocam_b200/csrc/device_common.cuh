@@ -121,9 +121,14 @@ DI int cell_hash(int cx, int cy, int cz, int hash_size) {
 // intersection (pathtrace.comp:102-130)
 // ---------------------------------------------------------------------------
 struct Ray {
-    float3 o, d, inv;
-#if !RC_EXACT
-    float3 oinv;   // o * inv, for the FMA form of the slab test
+    float3 o, d;
+#if RC_EXACT
+    float3 inv;
+#else
+    // 1/d and -o/d for the FMA form of the slab test, x and y side by side
+    // so that one paired FMA (__ffma2_rn) covers both axes
+    float2 ixy, nxy;
+    float iz, nz;
 #endif
 };
 
@@ -131,11 +136,24 @@ DI Ray make_ray(float3 o, float3 d) {
     Ray r;
     r.o = o;
     r.d = d;
+#if RC_EXACT
     r.inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-#if !RC_EXACT
-    r.oinv = o * r.inv;
+#else
+    r.ixy = make_float2(1.0f / d.x, 1.0f / d.y);
+    r.iz = 1.0f / d.z;
+    r.nxy = make_float2(-(o.x * r.ixy.x), -(o.y * r.ixy.y));
+    r.nz = -(o.z * r.iz);
 #endif
     return r;
+}
+
+// The slab test from the six plane distances (pathtrace.comp:102-110).
+DI bool slab_from(float t0x, float t0y, float t0z, float t1x, float t1y, float t1z, float& tmin) {
+    const float lox = gmin(t0x, t1x), loy = gmin(t0y, t1y), loz = gmin(t0z, t1z);
+    const float hix = gmax(t0x, t1x), hiy = gmax(t0y, t1y), hiz = gmax(t0z, t1z);
+    tmin = gmax(gmax(lox, loy), loz);
+    const float tmax = gmin(gmin(hix, hiy), hiz);
+    return tmax >= gmax(tmin, 0.0f);
 }
 
 DI bool slab(const Ray& r, float nx, float ny, float nz, float xx, float xy, float xz, float& tmin) {
@@ -143,14 +161,23 @@ DI bool slab(const Ray& r, float nx, float ny, float nz, float xx, float xy, flo
     const float t0x = (nx - r.o.x) * r.inv.x, t0y = (ny - r.o.y) * r.inv.y, t0z = (nz - r.o.z) * r.inv.z;
     const float t1x = (xx - r.o.x) * r.inv.x, t1y = (xy - r.o.y) * r.inv.y, t1z = (xz - r.o.z) * r.inv.z;
 #else
-    const float t0x = fmaf(nx, r.inv.x, -r.oinv.x), t0y = fmaf(ny, r.inv.y, -r.oinv.y), t0z = fmaf(nz, r.inv.z, -r.oinv.z);
-    const float t1x = fmaf(xx, r.inv.x, -r.oinv.x), t1y = fmaf(xy, r.inv.y, -r.oinv.y), t1z = fmaf(xz, r.inv.z, -r.oinv.z);
+    const float t0x = fmaf(nx, r.ixy.x, r.nxy.x), t0y = fmaf(ny, r.ixy.y, r.nxy.y), t0z = fmaf(nz, r.iz, r.nz);
+    const float t1x = fmaf(xx, r.ixy.x, r.nxy.x), t1y = fmaf(xy, r.ixy.y, r.nxy.y), t1z = fmaf(xz, r.iz, r.nz);
 #endif
-    const float lox = gmin(t0x, t1x), loy = gmin(t0y, t1y), loz = gmin(t0z, t1z);
-    const float hix = gmax(t0x, t1x), hiy = gmax(t0y, t1y), hiz = gmax(t0z, t1z);
-    tmin = gmax(gmax(lox, loy), loz);
-    const float tmax = gmin(gmin(hix, hiy), hiz);
-    return tmax >= gmax(tmin, 0.0f);
+    return slab_from(t0x, t0y, t0z, t1x, t1y, t1z, tmin);
+}
+
+// A box given as (min x, min y), min z, (max x, max y), max z.  The fast
+// build forms the x and y plane distances with one paired FMA per corner
+// (each lane rounded as fmaf rounds it: the same distances as slab()).
+DI bool slab_xy(const Ray& r, float2 lo, float loz, float2 hi, float hiz, float& tmin) {
+#if RC_EXACT
+    return slab(r, lo.x, lo.y, loz, hi.x, hi.y, hiz, tmin);
+#else
+    const float2 t0 = __ffma2_rn(lo, r.ixy, r.nxy);
+    const float2 t1 = __ffma2_rn(hi, r.ixy, r.nxy);
+    return slab_from(t0.x, t0.y, fmaf(loz, r.iz, r.nz), t1.x, t1.y, fmaf(hiz, r.iz, r.nz), tmin);
+#endif
 }
 
 DI bool hit_triangle(const Ray& r, const float4* __restrict__ tri_isect, int i, float& t, float& u, float& v) {
@@ -213,6 +240,18 @@ DI bool tslab(Guard& g, const Ray& r, float nx, float ny, float nz, float xx, fl
     return slab(r, nx, ny, nz, xx, xy, xz, tmin);
 }
 
+// The two child boxes of a node record (NodeRec: a = left (min x, min y,
+// max x, max y), b = the same for the right child, c = (left min z, left
+// max z, right min z, right max z)).
+DI bool tslab_left(Guard& g, const Ray& r, const float4& a, const float4& b, const float4& c, float& tmin) {
+    ++g.nodes;
+    return slab_xy(r, make_float2(a.x, a.y), c.x, make_float2(a.z, a.w), c.y, tmin);
+}
+DI bool tslab_right(Guard& g, const Ray& r, const float4& a, const float4& b, const float4& c, float& tmin) {
+    ++g.nodes;
+    return slab_xy(r, make_float2(b.x, b.y), c.z, make_float2(b.z, b.w), c.w, tmin);
+}
+
 // The root box test; a scene without triangles has no root to enter.
 DI bool enter_root(const DeviceScene& S, Guard& g, const Ray& r, float& tmin) {
     return S.tri_count > 0 &&
@@ -223,6 +262,12 @@ DI bool thit(Guard& g, const Ray& r, const float4* __restrict__ tri_isect, int i
     ++g.tris;
     return hit_triangle(r, tri_isect, i, t, u, v);
 }
+
+// A node to visit: cnt > 0 a leaf with primitives [ref, ref+cnt), else the
+// interior node `ref`.
+struct TravNode {
+    int ref, cnt;
+};
 
 // Closest hit, near child first (pathtrace.comp:142-203).  A stack entry
 // holds the child's (ref, count) and the entry distance the parent computed;
@@ -258,8 +303,8 @@ DI Hit trace_closest(const DeviceScene& S, const Ray& r, Guard& g) {
             const float4 a = __ldg(&nr->a), b = __ldg(&nr->b), c = __ldg(&nr->c);
             const int4 d = __ldg(&nr->d);
             float tl, tr;
-            const bool hl = tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tl);
-            const bool hr = tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tr);
+            const bool hl = tslab_left(g, r, a, b, c, tl);
+            const bool hr = tslab_right(g, r, a, b, c, tr);
             if (hl && hr) {
                 if (tl < tr) {
                     stk[top] = make_int2(d.z, d.w); stt[top++] = tr;
@@ -328,8 +373,8 @@ DI Hit trace_unordered(const DeviceScene& S, const Ray& r, Guard& g) {
                 const float4 a = __ldg(&nr->a), b = __ldg(&nr->b), c = __ldg(&nr->c);
                 const int4 d = __ldg(&nr->d);
                 float tl, tr;
-                const bool hl = tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tl);
-                const bool hr = tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tr);
+                const bool hl = tslab_left(g, r, a, b, c, tl);
+                const bool hr = tslab_right(g, r, a, b, c, tr);
                 if (hr) { stk[top] = make_int2(d.z, d.w); stt[top++] = tr; }
                 if (hl) { stk[top] = make_int2(d.x, d.y); stt[top++] = tl; }
             } else {
@@ -351,8 +396,8 @@ DI Hit trace_unordered(const DeviceScene& S, const Ray& r, Guard& g) {
                 const int4 d = __ldg(&nr->d);
                 float tc;
                 const bool right = stk[top].y != 0;
-                const bool hit = right ? tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tc)
-                                       : tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tc);
+                const bool hit = right ? tslab_right(g, r, a, b, c, tc)
+                                       : tslab_left(g, r, a, b, c, tc);
                 if (!hit || tc > h.t) continue;
                 ref = right ? d.z : d.x;
                 cnt = right ? d.w : d.y;
@@ -392,8 +437,8 @@ DI bool trace_shadow(const DeviceScene& S, const Ray& r, float max_dist, Guard& 
                 const float4 a = __ldg(&nr->a), b = __ldg(&nr->b), c = __ldg(&nr->c);
                 const int4 d = __ldg(&nr->d);
                 float tl, tr;
-                const bool hl = tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > max_dist);
-                const bool hr = tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > max_dist);
+                const bool hl = tslab_left(g, r, a, b, c, tl) && !(tl > max_dist);
+                const bool hr = tslab_right(g, r, a, b, c, tr) && !(tr > max_dist);
                 if (hr) stk[top++] = make_int2(d.z, d.w);
                 if (hl) stk[top++] = make_int2(d.x, d.y);
             } else {
@@ -413,8 +458,8 @@ DI bool trace_shadow(const DeviceScene& S, const Ray& r, float max_dist, Guard& 
                 const int4 d = __ldg(&nr->d);
                 float tc;
                 const bool right = stk[top].y != 0;
-                const bool hit = right ? tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tc)
-                                       : tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tc);
+                const bool hit = right ? tslab_right(g, r, a, b, c, tc)
+                                       : tslab_left(g, r, a, b, c, tc);
                 if (!hit || tc > max_dist) continue;
                 ref = right ? d.z : d.x;
                 cnt = right ? d.w : d.y;
@@ -436,9 +481,6 @@ DI bool trace_shadow(const DeviceScene& S, const Ray& r, float max_dist, Guard& 
 // lane.  The nearer hit child is entered directly and only the farther one is
 // pushed.  The closest hit equals trace_closest's except where two triangles
 // tie exactly; the shadow answer is the same yes/no.
-struct TravNode {
-    int ref, cnt;   // cnt > 0: leaf with primitives [ref, ref+cnt)
-};
 
 DI bool pop_entry(const int2* stk, const float* stt, int& top, float cull, TravNode& n) {
     while (top > 0) {
@@ -478,8 +520,8 @@ DI bool traverse_ww(const DeviceScene& S, const Ray& r, float max_t, Guard& g, H
                 const float4 a = __ldg(&nr->a), b = __ldg(&nr->b), c = __ldg(&nr->c);
                 const int4 d = __ldg(&nr->d);
                 float tl, tr;
-                const bool hl = tslab(g, r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > h.t);
-                const bool hr = tslab(g, r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > h.t);
+                const bool hl = tslab_left(g, r, a, b, c, tl) && !(tl > h.t);
+                const bool hr = tslab_right(g, r, a, b, c, tr) && !(tr > h.t);
                 if (hl && hr) {
                     const bool left_first = tl < tr;
                     if (top < 62) {

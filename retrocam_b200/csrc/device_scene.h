@@ -30,8 +30,10 @@
 namespace rc {
 
 struct NodeRec {
-    float4 a, b, c;
-    int4 d;
+    float4 a;   // left child:  min x, min y, max x, max y
+    float4 b;   // right child: min x, min y, max x, max y
+    float4 c;   // left min z, left max z, right min z, right max z
+    int4 d;     // left (ref, count), right (ref, count)
 };
 
 // 4-wide node of the fast build's traversal (128 B, two cache lines): the
@@ -138,6 +140,7 @@ struct PhotonArgs {
     unsigned int* work;
     int refill_lanes;
     int leaf_quarters;
+    int interior_steps;   // tree moves per lane per scheduling round of the refill emission
     float4* photons;        // 3 float4 per photon (std430 record)
     int* heads;
     int* next;

@@ -1,37 +1,47 @@
-// dyn_trace.cuh -- the per-lane traversal state machine of the fast build's
-// refill kernels (camera / shadow rays in wavefront.cu, photon segments in
-// kernels.cu).
+// dyn_trace.cuh -- the per-lane traversal state machine of the refill
+// kernels (camera / shadow rays in wavefront.cu, both builds; photon
+// segments in kernels.cu, fast build).
 //
-// A lane owns one ray at a time and advances it one step per loop iteration
-// of its warp: an interior node, parking a reached leaf, or the triangles of
-// a parked leaf.  Leaf tests and interior steps never share an iteration:
-// the warp tests leaves (every lane with one parked, together) once all busy
-// lanes have one parked or `leaf_quarters` quarters of them are blocked (a
-// leaf parked and no interior node to go on with); otherwise the unblocked
-// lanes take interior steps.  A kernel refills lanes whose ray finished from
-// its own work list when fewer than `refill_lanes` lanes are busy, so a warp
-// is not held by its slowest ray.  The rays, the visit order of each ray and
-// the hits are the plain traversal's; only the schedule differs.
+// A lane owns one ray at a time and advances it per loop iteration of its
+// warp: interior nodes, parking a reached leaf, or the triangles of a parked
+// leaf.  Leaf tests and interior steps never share an iteration: the warp
+// tests leaves (every lane with one parked, together) once all busy lanes
+// have one parked or `leaf_quarters` quarters of them are blocked (a leaf
+// parked and no interior node to go on with); otherwise the unblocked lanes
+// take up to `interior_steps` interior moves each.  A kernel refills lanes
+// whose ray finished from its own work list when fewer than `refill_lanes`
+// lanes are busy, so a warp is not held by its slowest ray.
+//
+// Fast build: a lane walks on past a parked leaf (its triangles are tested
+// later, with the warp); the hits are the plain traversal's, ties aside.
+// Exact build: a closest-hit lane stops at a reached leaf until the warp
+// tests it, and pops the next stack entry only then, with the entry distance
+// kept exactly -- trace_closest's visits in trace_closest's order, so the
+// same hit bit for bit; shadow lanes walk on as in the fast build (a yes/no
+// that does not depend on the order).
 #ifndef RC_DYN_TRACE_CUH
 #define RC_DYN_TRACE_CUH
 
 #include "device_common.cuh"
 
-#if !RC_EXACT
 namespace rc {
 namespace RC_NS {
 
+#if !RC_EXACT
 // Stack entries: the binary walk pushes at most one per level (guarded at
-// 62, as the reference), the 4-wide walk up to three.
+// 62, as the reference), the 4-wide walk up to three.  An entry is 8 bytes:
+// (ref, count | entry distance truncated to its top 16 bits); truncation
+// rounds a positive distance down, so the cull `t > hit` never drops a
+// needed entry.
 constexpr int kDynStack = 96;
+struct DynStack {
+    int2 e[kDynStack];
+};
 
-// Pops the next stack entry not culled by the current hit distance.  An
-// entry is 8 bytes: (ref, count | entry distance truncated to its top 16
-// bits); truncation rounds a positive distance down, so the cull `t > hit`
-// never drops a needed entry.
-DI bool pop_packed(const int2* stk, int& top, float cull, TravNode& n) {
+// Pops the next stack entry not culled by the current hit distance.
+DI bool pop_entry(DynStack& stk, int& top, float cull, TravNode& n) {
     while (top > 0) {
-        const int2 e = stk[--top];
+        const int2 e = stk.e[--top];
         if (__int_as_float(e.y & (int)0xffff0000) > cull) continue;
         n.ref = e.x;
         n.cnt = e.y & 0xffff;
@@ -39,6 +49,27 @@ DI bool pop_packed(const int2* stk, int& top, float cull, TravNode& n) {
     }
     return false;
 }
+#else
+// Exact build: (ref, count) and the exact entry distance the parent
+// computed (what the reference's re-test on pop returns); at most 61
+// entries on trees of up to 60 levels, the only ones this walk serves.
+constexpr int kDynStack = 64;
+struct DynStack {
+    int2 e[kDynStack];
+    float t[kDynStack];
+};
+
+DI bool pop_entry(DynStack& stk, int& top, float cull, TravNode& n) {
+    while (top > 0) {
+        --top;
+        if (stk.t[top] > cull) continue;
+        n.ref = stk.e[top].x;
+        n.cnt = stk.e[top].y;
+        return true;
+    }
+    return false;
+}
+#endif
 
 // The members of a DeviceScene that dyn_step reads, for walks whose scene
 // is chosen per lane (a select of four values instead of a whole scene).
@@ -101,6 +132,7 @@ DI bool dyn_schedule(const LaneRay& L, bool busy, unsigned int act, int leaf_qua
     return busy && (leaf_phase ? L.leaf.cnt > 0 : !blocked);
 }
 
+#if !RC_EXACT
 // One step of L (kWide: interior nodes from S.nodes4): in the leaf phase the
 // parked leaf's triangles; otherwise up to `interior_steps` moves through
 // the tree -- interior nodes, or parking a reached leaf -- while the lane is
@@ -108,7 +140,7 @@ DI bool dyn_schedule(const LaneRay& L, bool busy, unsigned int act, int leaf_qua
 // warp's scheduling work is shared by several moves.  Returns true when the
 // ray is finished: its walk ended, an any-hit ray hit, or the step cap.
 template <bool kWide, class Scn>
-DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
+DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
     bool done = false;
     if (leaf_phase) {
         for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
@@ -130,7 +162,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g,
             if (L.node.cnt > 0) {
                 if (L.leaf.cnt > 0) break;   // blocked: a leaf is parked already
                 L.leaf = L.node;
-                L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
             } else if (kWide) {
                 // 4-wide node: hit children ordered by entry distance, the
                 // nearest entered, the others pushed far to near
@@ -156,14 +188,14 @@ DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g,
                 cswap(key[1], key[3]);
                 cswap(key[1], key[2]);
                 if (key[0] == 0xffffffffu) {
-                    L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                    L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
                 } else {
     #pragma unroll
                     for (int k = 3; k >= 1; --k) {
                         if (key[k] != 0xffffffffu) {
                             if (L.top < kDynStack) {
                                 const int s = key[k] & 3u;
-                                stk[L.top++] =
+                                stk.e[L.top++] =
                                     make_int2(CR[s], (CC[s] & 0xffff) | (__float_as_int(t4[s]) & (int)0xffff0000));
                             } else {
                                 g.flags |= RC_GUARD_TRAVERSAL_CAP;
@@ -179,14 +211,14 @@ DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g,
                 const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
                 const int4 d = __ldg(&nrec->d);
                 float tl, tr;
-                const bool hl = tslab(g, L.r, a.x, a.y, a.z, a.w, b.x, b.y, tl) && !(tl > L.h.t);
-                const bool hr = tslab(g, L.r, b.z, b.w, c.x, c.y, c.z, c.w, tr) && !(tr > L.h.t);
+                const bool hl = tslab_left(g, L.r, a, b, c, tl) && !(tl > L.h.t);
+                const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
                 if (hl && hr) {
                     const bool left_first = tl < tr;
                     if (L.top < 62) {
                         const float tf = left_first ? tr : tl;
                         const int cf = left_first ? d.w : d.y;
-                        stk[L.top++] =
+                        stk.e[L.top++] =
                             make_int2(left_first ? d.z : d.x, (cf & 0xffff) | (__float_as_int(tf) & (int)0xffff0000));
                     }
                     L.node.ref = left_first ? d.x : d.z;
@@ -198,7 +230,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g,
                     L.node.ref = d.z;
                     L.node.cnt = d.w;
                 } else {
-                    L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                    L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
                 }
             }
             if (m + 1 < interior_steps && ++L.steps > 4 * S.node_count + 64) break;
@@ -212,8 +244,85 @@ DI bool dyn_step(const Scn& S, LaneRay& L, int2* stk, bool leaf_phase, Guard& g,
     return done;
 }
 
+#else
+// Exact build: one step of L with trace_closest's order for closest-hit
+// lanes (see the file comment); shadow lanes park and walk on.
+template <bool kWide, class Scn>
+DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
+    bool done = false;
+    if (leaf_phase) {
+        for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
+            float t, u, v;
+            if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
+                L.h.t = t;
+                L.h.u = u;
+                L.h.v = v;
+                L.h.prim = i;
+                if (L.any) {
+                    done = true;
+                    break;
+                }
+            }
+        }
+        L.leaf.cnt = 0;
+    } else {
+        for (int m = 0; m < interior_steps; ++m) {
+            if (!L.have_node) {
+                // a closest-hit lane pops only after its parked leaf was
+                // tested, against the distance that leaf may have lowered
+                if (L.leaf.cnt > 0 || L.top == 0) break;
+                L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
+                if (!L.have_node) break;
+            }
+            if (L.node.cnt > 0) {
+                if (L.leaf.cnt > 0) break;   // blocked: a leaf is parked already
+                L.leaf = L.node;
+                if (L.any) {
+                    L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
+                } else {
+                    L.have_node = false;
+                    break;
+                }
+            } else {
+                const NodeRec* nrec = S.nodes + L.node.ref;
+                const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
+                const int4 d = __ldg(&nrec->d);
+                float tl, tr;
+                // a child whose entry lies past the current hit is the one
+                // trace_closest would push and then drop when popping it
+                const bool hl = tslab_left(g, L.r, a, b, c, tl) && !(tl > L.h.t);
+                const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
+                if (hl && hr) {
+                    const bool left_first = tl < tr;
+                    if (L.top < 62) {
+                        stk.e[L.top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
+                        stk.t[L.top++] = left_first ? tr : tl;
+                    }
+                    L.node.ref = left_first ? d.x : d.z;
+                    L.node.cnt = left_first ? d.y : d.w;
+                } else if (hl) {
+                    L.node.ref = d.x;
+                    L.node.cnt = d.y;
+                } else if (hr) {
+                    L.node.ref = d.z;
+                    L.node.cnt = d.w;
+                } else {
+                    L.have_node = false;
+                }
+            }
+            if (m + 1 < interior_steps && ++L.steps > 4 * S.node_count + 64) break;
+        }
+    }
+    if (!L.have_node && L.leaf.cnt == 0 && L.top == 0) done = true;
+    if (++L.steps > 4 * S.node_count + 64) {
+        g.flags |= RC_GUARD_TRAVERSAL_CAP;
+        done = true;
+    }
+    return done;
+}
+#endif
+
 }  // namespace RC_NS
 }  // namespace rc
-#endif  // !RC_EXACT
 
 #endif

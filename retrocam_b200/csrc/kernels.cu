@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(128) photon_emit_dyn(PhotonArgs A) {
     const unsigned int total = S.light_count != 0 ? (unsigned int)A.photon_count : 0u;
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0;
-    int2 stk[kDynStack];
+    DynStack stk;
     LaneRay L;
     L.item = -1;
     L.top = 0;
@@ -424,7 +424,7 @@ __global__ void __launch_bounds__(128) photon_emit_dyn(PhotonArgs A) {
             bool push = false;
             bool leaf_phase;
             if (dyn_schedule(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
-                dyn_step<false>(step_scene(second, A.spec, A.diff), L, stk, leaf_phase, g)) {
+                dyn_step<false>(step_scene(second, A.spec, A.diff), L, stk, leaf_phase, g, A.interior_steps)) {
                 if (!second && L.h.prim >= 0) {
                     hs = L.h;
                     hs.prim = __ldg(A.spec_orig + hs.prim);

@@ -547,11 +547,10 @@ static int grid_for(const void* fn, int block) {
     return sms * (per > 0 ? per : 1);
 }
 
-#if !RC_EXACT
-// Persistent trace with dynamic ray fetch (fast build): the refill state
-// machine of dyn_trace.cuh over the ray queue followed by the shadow queue
-// (one atomicAdd per warp on the work counter per refill).  Same rays and
-// results as wf_trace; only the schedule differs.
+// Persistent trace with dynamic ray fetch: the refill state machine of
+// dyn_trace.cuh over the ray queue followed by the shadow queue (one
+// atomicAdd per warp on the work counter per refill).  Same rays and results
+// as wf_trace (bit for bit in the exact build); only the schedule differs.
 // kWide: interior steps over the 4-wide nodes (scene.nodes4) instead of the
 // binary records.
 template <bool kWide>
@@ -573,7 +572,7 @@ DI void trace_dyn(const WaveArgs& A) {
     const int lane = threadIdx.x & 31;
     Guard g = {0u, 0u, 0u};
     uint32_t closest = 0, shadow = 0;
-    int2 stk[kDynStack];
+    DynStack stk;
     LaneRay L;
     L.item = -1;
     L.top = 0;
@@ -651,6 +650,7 @@ DI void trace_dyn(const WaveArgs& A) {
 // so 9 blocks of 128 threads fit an SM instead of 8; the kernel waits on L1
 // latency and the extra warps pay (65.0 vs 67.4 ms per export frame).
 __global__ void __maxnreg__(56) wf_trace_dyn(WaveArgs A) { trace_dyn<false>(A); }
+#if !RC_EXACT
 // 4-wide walk: uncapped (77 registers; 56 spills)
 __global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<true>(A); }
 #endif
@@ -674,8 +674,8 @@ static void fill_grids(WfGrids& g) {
         g.trace1[c] = grid_for((const void*)wf_trace<true>, b);
         g.shade[c] = grid_for((const void*)wf_shade<false>, b);
         g.shade_mq[c] = grid_for((const void*)wf_shade<true>, b);
-#if !RC_EXACT
         g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
+#if !RC_EXACT
         g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
 #endif
     }
@@ -708,8 +708,7 @@ cudaError_t launch_wf_generate(const WaveArgs& A, cudaStream_t s) {
 
 cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
     const int c = block_class(block), b = 64 << c;
-#if !RC_EXACT
-    // the refill trace packs leaf counts into 16 bits of a stack entry
+    // the fast refill trace packs leaf counts into 16 bits of a stack entry
     // chunks below refill_min_paths hold about one wave of rays per launch,
     // where the refill bookkeeping costs more than it recovers (854x480 at
     // 1 spp: trace 0.264 ms grid-stride vs 0.306 ms refill; they tie at 2 spp)
@@ -717,13 +716,15 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
     // 32-entry stack can overflow), which the refill walk does not follow
     if (A.dynamic_fetch && A.paths >= A.refill_min_paths && A.scene.max_leaf < 0x10000 &&
         A.scene.depth <= 28) {
-        if (A.scene.nodes4)
+#if !RC_EXACT
+        if (A.scene.nodes4) {
             wf_trace_dyn4<<<grids().dyn4[c], b, 0, s>>>(A);
-        else
-            wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
+            return cudaGetLastError();
+        }
+#endif
+        wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
         return cudaGetLastError();
     }
-#endif
     if (A.scene.depth <= 28)
         wf_trace<true><<<grids().trace1[c], b, 0, s>>>(A);
     else
