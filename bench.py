@@ -102,10 +102,10 @@ def algorithmic_bytes(kernel: str, ctr: dict, samples: int) -> float:
 
 def state_bytes(kernel: str, ctr: dict) -> float:
     """Path state the wavefront trace reads and writes per ray (origin and
-    direction in, hit record out: 48 B per closest ray; shadow record in,
-    radiance read-modify-write: 96 B per shadow ray)."""
+    direction in, hit record out: 48 B per closest ray; the 48-B shadow
+    record in, radiance read-modify-write: 80 B per shadow ray)."""
     if kernel == "wf_trace":
-        return 48 * ctr["closest_rays"] + 96 * ctr["shadow_rays"]
+        return 48 * ctr["closest_rays"] + 80 * ctr["shadow_rays"]
     return 0.0
 
 

@@ -1034,8 +1034,8 @@ static int wavefront_reserve(rc_ctx* ctx, long cap) {
         CK(ensure(ctx->wf_rq1, n * 4));
         CK(ensure(ctx->wf_sq0, n * 4));
         CK(ensure(ctx->wf_sq1, n * 4));
-        CK(ensure(ctx->wf_srec0, n * 64));
-        CK(ensure(ctx->wf_srec1, n * 64));
+        CK(ensure(ctx->wf_srec0, n * 48));
+        CK(ensure(ctx->wf_srec1, n * 48));
         CK(ensure(ctx->wf_mq, n * 4));
         CK(ensure(ctx->wf_qlen, 8 * sizeof(unsigned int)));
         ctx->wf_capacity = (int)cap;

@@ -229,7 +229,7 @@ struct WaveBuffers {
     uint32_t* seed;   // PCG state
     int* rq[2];       // ray queues (ping-pong by bounce)
     int* sq[2];       // shadow queues
-    float4* srec[2];  // shadow records, 4 float4 per queue slot
+    float4* srec[2];  // shadow records, 3 float4 per queue slot (wavefront.cu)
     int* mq;          // material queues of the bounce's hits: diffuse paths
                       // from the front (count qlen[5]), metal and glass
                       // paths from the back (count qlen[6])

@@ -140,6 +140,27 @@ __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(&A.counters->camera_paths, (unsigned long long)n);
 }
 
+// Shadow records (3 float4 per queue slot): origin and tmax, direction and
+// path index, and (throughput * light term, flags).  The flags hold the
+// path's last-bounce bit and, per throughput channel, what throughput * 0
+// is (0: +0, 1: -0, 2: NaN), so the occluded case adds what the reference's
+// `radiance += throughput * 0` adds.
+DI int zero_code(float x) { return bad(x) ? 2 : (__float_as_int(x) < 0 ? 1 : 0); }
+DI float zero_of(int code) {
+    return code == 2 ? __int_as_float(0x7fffffff) : (code == 1 ? -0.0f : 0.0f);
+}
+
+// radiance += throughput * sampleDirectLight(...), the light term 0 when
+// occluded (pathtrace.comp:341-395 as traceRadiance adds it); the path's
+// final radiance when this was its last bounce.
+DI void shadow_add(const WaveBuffers& B, int p, bool vis, const float4 sq) {
+    const int fl = __float_as_int(sq.w);
+    const float3 add = vis ? xyz(sq) : f3(zero_of((fl >> 1) & 3), zero_of((fl >> 3) & 3), zero_of((fl >> 5) & 3));
+    const float3 r = xyz(B.rad[p]) + add;
+    B.rad[p] = make_float4(r.x, r.y, r.z, 0.0f);
+    if (fl & 1) B.res[p] = make_float4(r.x, r.y, r.z, 0.0f);
+}
+
 // Closest-hit traversal of ray queue rq[bounce&1] followed (same index
 // space) by the visibility tests of shadow queue sq[(bounce+1)&1].
 template <bool kShadowAtParent>
@@ -167,16 +188,12 @@ __global__ void __launch_bounds__(256) wf_trace(WaveArgs A) {
             ++closest;
         } else {
             const int k = (int)(i - nr);
-            const float4* rec = B.srec[prev] + 4 * k;
-            const float4 so = rec[0], sd = rec[1], st = rec[2], sl = rec[3];
+            const float4* rec = B.srec[prev] + 3 * k;
+            const float4 so = rec[0], sd = rec[1], sq = rec[2];
             const int p = __float_as_int(sd.w);
             const bool vis = unoccluded<kShadowAtParent>(A.scene, make_ray(xyz(so), xyz(sd)), so.w, g);
             ++shadow;
-            // radiance += throughput * sampleDirectLight(...), 0 when occluded
-            const float3 L = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
-            const float3 r = xyz(B.rad[p]) + xyz(st) * L;
-            B.rad[p] = make_float4(r.x, r.y, r.z, 0.0f);
-            if (__float_as_int(st.w) != 0) B.res[p] = make_float4(r.x, r.y, r.z, 0.0f);
+            shadow_add(B, p, vis, sq);
         }
     }
     const unsigned int active = __activemask();
@@ -279,14 +296,30 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
     // block-uniform trip count: the appends at the bottom synchronise the block
     for (unsigned int i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
         const unsigned int i = i0 + threadIdx.x;
+        {
+            // the next item's path state, fetched into L2 while this one runs
+            const unsigned int inext = i + gridDim.x * blockDim.x;
+            if (inext < n) {
+                const int pn = !kMQ ? B.rq[cur][inext]
+                                    : (inext < nd ? B.mq[inext] : B.mq[B.capacity - 1 - (int)(inext - nd)]);
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(B.hit + pn));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(B.o + pn));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(B.d + pn));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(B.seed + pn));
+                if (b > 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(B.thr + pn));
+            }
+        }
         bool cont = false, shadow_rec = false;
-        float4 rec0, rec1, rec2, rec3;
+        float4 rec0, rec1, rec2;
         int p = 0;
         if (i < n) {
             p = !kMQ ? B.rq[cur][i] : (i < nd ? B.mq[i] : B.mq[B.capacity - 1 - (int)(i - nd)]);
             const float4 hv = B.hit[p];
             const int prim = __float_as_int(hv.w);
-            float3 rad = b == 0 ? f3(0.0f, 0.0f, 0.0f) : xyz(B.rad[p]);
+            // radiance so far: implied 0 on bounce 0, else read when first
+            // needed (an add that can change it, or the path's end)
+            float3 rad = f3(0.0f, 0.0f, 0.0f);
+            bool rad_known = b == 0, rad_dirty = b == 0;
             // frame-0 albedo image: first hit of the G channel (or the only one)
             bool alb_path = false;
             PathId id;
@@ -314,7 +347,15 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
                     const float3 a = (m.transmission > 0.5f) ? f3(1.0f, 1.0f, 1.0f) : m.albedo;
                     galb[(long)id.py * A.width + id.px] = to_half4(a.x, a.y, a.z, 1.0f);
                 }
-                if (!last_diffuse) rad = rad + (thr * m.emission) * m.strength;
+                if (!last_diffuse) {
+                    const float3 e = (thr * m.emission) * m.strength;
+                    // rad + (+-0) is rad (rad is never -0); NaN != 0 too
+                    if (e.x != 0.0f || e.y != 0.0f || e.z != 0.0f) {
+                        if (!rad_known) rad = xyz(B.rad[p]);
+                        rad = rad + e;
+                        rad_known = rad_dirty = true;
+                    }
+                }
                 bool alive = true;
                 if (b >= 2) {
                     float survive = gmax(m.albedo.x, gmax(m.albedo.y, m.albedo.z));
@@ -412,15 +453,26 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
                                             const float3 so = sf.pos + nrm * 2e-3f;
                                             rec0 = make_float4(so.x, so.y, so.z, dist - 4e-3f);
                                             rec1 = make_float4(sd.x, sd.y, sd.z, __int_as_float(p));
-                                            rec2 = make_float4(thr.x, thr.y, thr.z, __int_as_float(last ? 1 : 0));
-                                            rec3 = make_float4(contrib.x, contrib.y, contrib.z, 0.0f);
+                                            // the visible light's term, and what throughput * 0 is
+                                            // per channel for the occluded case
+                                            const float3 q = thr * contrib;
+                                            rec2 = make_float4(q.x, q.y, q.z,
+                                                               __int_as_float((last ? 1 : 0) | (zero_code(thr.x) << 1) |
+                                                                              (zero_code(thr.y) << 3) |
+                                                                              (zero_code(thr.z) << 5)));
                                             shadow_rec = true;
                                             early = false;
                                         }
                                     }
                                 }
                             }
-                            if (early) rad = rad + thr * f3(0.0f, 0.0f, 0.0f);
+                            // rad + throughput * 0 changes rad only where a throughput
+                            // channel is not finite (NaN)
+                            if (early && (bad(thr.x) || bad(thr.y) || bad(thr.z))) {
+                                if (!rad_known) rad = xyz(B.rad[p]);
+                                rad = rad + thr * f3(0.0f, 0.0f, 0.0f);
+                                rad_known = rad_dirty = true;
+                            }
                         }
                         const float u1 = rnd(seed);
                         const float u2 = rnd(seed);
@@ -431,13 +483,14 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
                     }
                     cont = !last;
                 }
-                B.rad[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
+                if (rad_dirty) B.rad[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
                 if (cont) {
                     B.o[p] = make_float4(no.x, no.y, no.z, 0.0f);
                     B.d[p] = make_float4(nd.x, nd.y, nd.z, 0.0f);
                     B.thr[p] = make_float4(thr.x, thr.y, thr.z, nd_diffuse ? 1.0f : 0.0f);
                     B.seed[p] = seed;
                 } else if (!shadow_rec) {
+                    if (!rad_known) rad = xyz(B.rad[p]);
                     B.res[p] = make_float4(rad.x, rad.y, rad.z, 0.0f);
                 }
             }
@@ -447,11 +500,10 @@ __global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
         block_append(sh, cont, shadow_rec, B.qlen + nxt, B.qlen + 2 + cur, slot_r, slot_s);
         if (cont) B.rq[nxt][slot_r] = p;
         if (shadow_rec) {
-            float4* r = B.srec[cur] + 4 * slot_s;
+            float4* r = B.srec[cur] + 3 * slot_s;
             r[0] = rec0;
             r[1] = rec1;
             r[2] = rec2;
-            r[3] = rec3;
         }
     }
     const unsigned int active = __activemask();
@@ -597,7 +649,7 @@ DI void trace_dyn(const WaveArgs& A) {
                         dyn_start(S, L, 1e30f, false, g);
                         ++closest;
                     } else {
-                        const float4* rec = B.srec[prev] + 4 * (L.item - (int)nr);
+                        const float4* rec = B.srec[prev] + 3 * (L.item - (int)nr);
                         const float4 so = rec[0], sd = rec[1];
                         L.r = make_ray(xyz(so), xyz(sd));
                         dyn_start(S, L, so.w, true, g);
@@ -617,14 +669,8 @@ DI void trace_dyn(const WaveArgs& A) {
                     const int p = B.rq[cur][item];
                     B.hit[p] = make_float4(L.h.t, L.h.u, L.h.v, __int_as_float(L.h.prim));
                 } else {
-                    const float4* rec = B.srec[prev] + 4 * (item - (int)nr);
-                    const float4 sd = rec[1], st = rec[2], sl = rec[3];
-                    const int p = __float_as_int(sd.w);
-                    const bool vis = L.h.prim < 0;
-                    const float3 Lc = vis ? xyz(sl) : f3(0.0f, 0.0f, 0.0f);
-                    const float3 rr = xyz(B.rad[p]) + xyz(st) * Lc;
-                    B.rad[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
-                    if (__float_as_int(st.w) != 0) B.res[p] = make_float4(rr.x, rr.y, rr.z, 0.0f);
+                    const float4* rec = B.srec[prev] + 3 * (item - (int)nr);
+                    shadow_add(B, __float_as_int(rec[1].w), L.h.prim < 0, rec[2]);
                 }
                 L.item = -1;
                 busy = false;

@@ -87,6 +87,6 @@ def test_algorithmic_bytes_units():
                           "shadow_rays", "photon_node_tests", "photon_tri_tests")}
     ctr.update(node_tests=10, tri_tests=2, closest_rays=3, shadow_rays=1)
     assert bench.algorithmic_bytes("wf_trace", ctr, 0) == 10 * 32 + 2 * 36
-    assert bench.state_bytes("wf_trace", ctr) == 3 * 48 + 96
+    assert bench.state_bytes("wf_trace", ctr) == 3 * 48 + 80
     ctr.update(surface_hits=4, light_samples=2)
     assert bench.algorithmic_bytes("render", ctr, 5) == 10 * 32 + 2 * 36 + 4 * 104 + 2 * 80 + 5 * 20
