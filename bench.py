@@ -74,7 +74,7 @@ BYTES_SAMPLE_RMW = 20     # accum RGBA32F (16) + variance R32F (4) per pixel sam
 
 
 KERNEL_SYMBOL = {"render": "render_kernel", "wf_trace": "wf_trace", "wf_shade": "wf_shade",
-                 "photon_trace": "photon_trace_kernel", "photon_gather": "photon_gather_kernel",
+                 "photon_trace": "photon_bounce_kernel", "photon_gather": "photon_gather_kernel",
                  "atrous": "atrous_kernel", "wf_generate": "wf_generate", "wf_accumulate": "wf_accumulate",
                  "wf_sort": "wf_sort"}
 
@@ -570,6 +570,13 @@ def exact_math_line(args, w, sc, cam, sppm, atrous, fast_ctx, stream, device) ->
                           steps, max(3, min(args.warmup, 3)), stream)
         if ex.counters()["error_word"]:
             raise RuntimeError("kernel guard raised in the exact build")
+        # one more frame with per-kernel CUDA events: where the exact frame's time goes
+        ex.set_kernel_timing(True)
+        ex.kernel_times()
+        ex.render_frame(cam, settings, w.spp, sppm, r0, iters, atrous, read=False)
+        ex.synchronize()
+        kt = {k: v[0] for k, v in ex.kernel_times().items() if v[1]}
+        ex.set_kernel_timing(False)
         ex.reset()
         ex.render(cam, settings, 0, 1)
         a_ex = ex.read_buffers()[0]
@@ -580,7 +587,7 @@ def exact_math_line(args, w, sc, cam, sppm, atrous, fast_ctx, stream, device) ->
     rel = np.abs(a_fa[..., :3] - a_ex[..., :3]) / np.maximum(np.abs(a_ex[..., :3]), 1e-3)
     within = np.all(rel <= 1e-4, axis=-1)
     return {"value": w.width * w.height * w.spp / (ms / 1e3) / 1e6, "unit": UNIT, "ms_per_step": ms,
-            "steps": steps, "tuning": tuning,
+            "steps": steps, "tuning": tuning, "kernel_ms": kt,
             "fast_vs_exact_1spp": {"pixels_within_1e-4_rel": float(within.mean()),
                                    "pixels_bit_identical": float(np.all(a_fa[..., :3].view(np.uint32) ==
                                                                         a_ex[..., :3].view(np.uint32),

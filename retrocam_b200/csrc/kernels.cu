@@ -11,7 +11,11 @@
 //
 // Kernels (reference shader each replaces):
 //   render_kernel         pathtrace.comp main()   (Renderer.render x n_spp)
-//   photon_trace_kernel   photon_trace.comp main()
+//   photon_emit_full_kernel + photon_bounce_kernel
+//                         photon_trace.comp main(), split after the first
+//                         segment (fast build with the specular/other
+//                         BVH split: photon_emit_dyn or photon_emit_kernel
+//                         for the first phase)
 //   photon_gather_kernel  photon_gather.comp main()
 //   atrous_kernel         post/atrous_denoise.frag (p00_normalize fused
 //                         into the first pass)
@@ -278,31 +282,6 @@ DI bool first_specular(const PhotonArgs& A, const Ray& ray, Guard& g, Hit& hit) 
 }
 #endif
 
-// photon_trace.comp:168-252: one thread per photon, all its segments.
-template <bool kAtParent>
-__global__ void __launch_bounds__(256) photon_trace_kernel(PhotonArgs A) {
-    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
-    const DeviceScene& S = A.scene;
-    Guard g = {0u, 0u, 0u};
-    uint32_t rays = 0;
-    PhotonStore out;
-    out.store = false;
-    if (gid < A.photon_count && S.light_count != 0) {
-        const PhotonState st = emit_photon(A, S, gid);
-        Hit none;
-        none.prim = -1;
-#if !RC_EXACT
-        if (A.split) {
-            ++rays;
-            Hit h;
-            if (first_specular(A, st.ray, g, h)) out = photon_walk<kAtParent>(A, S, st, true, h, g, rays);
-        } else
-#endif
-            out = photon_walk<kAtParent>(A, S, st, false, none, g, rays);
-    }
-    store_photons(A, out, rays, g);
-}
-
 #if !RC_EXACT
 // Two-phase trace (fast build with the split): every photon's emission and
 // first segment, and only the photons whose first hit is specular -- the
@@ -322,6 +301,52 @@ __global__ void __launch_bounds__(256) photon_emit_kernel(PhotonArgs A) {
         st = emit_photon(A, S, gid);
         ++rays;
         want = first_specular(A, st.ray, g, h);
+    }
+    const unsigned int mask = __ballot_sync(0xffffffffu, want);
+    const int lane = threadIdx.x & 31;
+    if (mask != 0u) {
+        const int leader = __ffs(mask) - 1;
+        unsigned int base = 0;
+        if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (want) {
+            float4* q = A.queue + 4 * (size_t)(base + __popc(mask & ((1u << lane) - 1u)));
+            q[0] = make_float4(st.ray.o.x, st.ray.o.y, st.ray.o.z, __uint_as_float(st.seed));
+            q[1] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, st.power.x);
+            q[2] = make_float4(st.power.y, st.power.z, h.t, h.u);
+            q[3] = make_float4(h.v, __int_as_float(h.prim), 0.0f, 0.0f);
+        }
+    }
+    PhotonStore none;
+    none.store = false;
+    store_photons(A, none, rays, g);
+}
+#endif
+
+// Two-phase trace over the full scene (exact math, and fast math without
+// the split): every photon's emission and first segment; photons whose
+// first hit is glass or metal (photon_interact's branches) -- the only
+// ones that can be stored -- are queued for photon_bounce_kernel as
+// photon_emit_kernel queues them.  Same segments, hits and random numbers
+// as one walk of all the segments (photon_trace.comp:168-252), split after
+// the first segment.
+template <bool kAtParent>
+__global__ void __launch_bounds__(256) photon_emit_full_kernel(PhotonArgs A) {
+    const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+    const DeviceScene& S = A.scene;
+    Guard g = {0u, 0u, 0u};
+    uint32_t rays = 0;
+    bool want = false;
+    PhotonState st;
+    Hit h;
+    if (gid < A.photon_count && S.light_count != 0) {
+        st = emit_photon(A, S, gid);
+        ++rays;
+        h = photon_hit<kAtParent>(S, st.ray, g);
+        if (h.prim >= 0) {
+            const int m = __float_as_int(__ldg(S.tri_shade + 3 * h.prim).w);
+            want = __ldg(S.materials + 4 * m + 2).z > 0.5f || __ldg(S.materials + 4 * m + 0).w > 0.5f;
+        }
     }
     const unsigned int mask = __ballot_sync(0xffffffffu, want);
     const int lane = threadIdx.x & 31;
@@ -368,6 +393,7 @@ __global__ void __launch_bounds__(256) photon_bounce_kernel(PhotonArgs A) {
     store_photons(A, out, rays, g);
 }
 
+#if !RC_EXACT
 // The first phase as a refill kernel (dyn_trace.cuh): a lane emits the next
 // photon (work counter A.work) when its photon is done, walks the specular
 // triangles' tree for the nearest hit, then on a hit the other triangles'
@@ -1025,10 +1051,18 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) 
         return cudaGetLastError();
     }
 #endif
-    if (A.scene.depth <= 60)
-        photon_trace_kernel<true><<<blocks, b, 0, s>>>(A);
-    else
-        photon_trace_kernel<false><<<blocks, b, 0, s>>>(A);
+    // without the split (exact math, or scenes too large for the split
+    // BVHs): the emission and first segment over the full scene, then the
+    // queued walks (photon_trace.comp:168-252 in two launches)
+    cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    if (A.scene.depth <= 60) {
+        photon_emit_full_kernel<true><<<blocks, b, 0, s>>>(A);
+        photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
+    } else {
+        photon_emit_full_kernel<false><<<blocks, b, 0, s>>>(A);
+        photon_bounce_kernel<false><<<blocks, b, 0, s>>>(A);
+    }
     return cudaGetLastError();
 }
 
