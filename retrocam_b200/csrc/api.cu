@@ -1297,7 +1297,7 @@ int rc_sppm_trace(rc_ctx* ctx, const rc_sppm_params* p) {
             return ex ? exact::launch_photon_trace(A, ctx->stream, ctx->photon_block)
                       : fast::launch_photon_trace(A, ctx->stream, ctx->photon_block);
         },
-        A.split ? 2 : 1);
+        2);   // emission and first segments, then the queued walks
     if (e != cudaSuccess) return launch_err(ctx, e, "photon trace");
     e = timed_launch(ctx, RC_KERNEL_PHOTON_LAYOUT, [&] {
         return ex ? exact::launch_photon_layout(A, ctx->stream) : fast::launch_photon_layout(A, ctx->stream);
@@ -1343,17 +1343,13 @@ int rc_sppm_gather(rc_ctx* ctx, const rc_camera* cam, const rc_sppm_params* p, f
         ctx->gcache_valid = true;
     }
     const bool ex = ctx->math_mode == RC_MATH_EXACT;
-    A.heavy = nullptr;
-    A.heavy_len = nullptr;
-    if (!ex) {
-        // a batch allocated the list before its capture
-        if (!ctx->gcache_force) CK(ensure(ctx->gheavy, ((size_t)ctx->width * ctx->height + 1) * sizeof(int)));
-        A.heavy_len = (unsigned int*)ctx->gheavy.ptr;
-        A.heavy = (int*)ctx->gheavy.ptr + 1;
-    }
+    // the dense pixels' list (a batch allocated it before its capture)
+    if (!ctx->gcache_force) CK(ensure(ctx->gheavy, ((size_t)ctx->width * ctx->height + 1) * sizeof(int)));
+    A.heavy_len = (unsigned int*)ctx->gheavy.ptr;
+    A.heavy = (int*)ctx->gheavy.ptr + 1;
     const cudaError_t e = timed_launch(ctx, RC_KERNEL_PHOTON_GATHER, [&] {
         return ex ? exact::launch_photon_gather(A, ctx->stream) : fast::launch_photon_gather(A, ctx->stream);
-    }, ex ? 1 : 2);
+    }, 2);
     return launch_err(ctx, e, "photon gather");
 }
 

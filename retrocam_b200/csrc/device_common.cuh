@@ -785,7 +785,26 @@ DI float3 cosine_hemisphere(float ux, float uy, float3 n) {
 }
 
 // pathtrace.comp:310-321
-DI float2 sample_ngon(uint32_t& seed, float radius, int N) {
+// The aperture polygon's corner directions: (sin, cos) of
+// 6.28318530718f * k / N for k = 0..N+1, each computed as sample_ngon
+// computes it, so a sample read from the table is the sample computed
+// directly, bit for bit.  A kernel whose paths share a blade count fills
+// one per block (kNgonTab entries at most) and skips four sin/cos
+// evaluations per camera ray -- the exact build's correctly rounded ones
+// cost most of its ray generation.
+constexpr int kNgonTab = 34;
+DI void fill_ngon_table(float2* tab, int N) {
+    if (N < 1 || N + 2 > kNgonTab) return;
+    for (int k = threadIdx.x; k <= N + 1; k += blockDim.x) {
+        float s, c;
+        sincos_(6.28318530718f * (float)k / (float)N, &s, &c);
+        tab[k] = make_float2(s, c);
+    }
+}
+DI bool ngon_table_ok(int N) { return N >= 1 && N + 2 <= kNgonTab; }
+
+// tab: fill_ngon_table(tab, N)'s table for this N, or null.
+DI float2 sample_ngon(uint32_t& seed, float radius, int N, const float2* tab = nullptr) {
     float r1 = rnd(seed);
     float r2 = rnd(seed);
     if (r1 + r2 > 1.0f) {
@@ -793,11 +812,19 @@ DI float2 sample_ngon(uint32_t& seed, float radius, int N) {
         r2 = 1.0f - r2;
     }
     const int sector = (int)(rnd(seed) * (float)N);
-    const float a0 = 6.28318530718f * (float)sector / (float)N;
-    const float a1 = 6.28318530718f * (float)(sector + 1) / (float)N;
     float s0, c0, s1, c1;
-    sincos_(a0, &s0, &c0);
-    sincos_(a1, &s1, &c1);
+    if (tab && sector >= 0 && sector <= N) {
+        const float2 e0 = tab[sector], e1 = tab[sector + 1];
+        s0 = e0.x;
+        c0 = e0.y;
+        s1 = e1.x;
+        c1 = e1.y;
+    } else {
+        const float a0 = 6.28318530718f * (float)sector / (float)N;
+        const float a1 = 6.28318530718f * (float)(sector + 1) / (float)N;
+        sincos_(a0, &s0, &c0);
+        sincos_(a1, &s1, &c1);
+    }
     return make_float2((r1 * c0 + r2 * c1) * radius, (r1 * s0 + r2 * s1) * radius);
 }
 
@@ -806,7 +833,9 @@ struct Counts {
 };
 
 // pathtrace.comp:401-439
-DI Ray generate_ray(const CamParams& cam, int W, int H, int px, int py, uint32_t& seed, float offset) {
+// ngon: the corner table for cam.blades (fill_ngon_table), or null.
+DI Ray generate_ray(const CamParams& cam, int W, int H, int px, int py, uint32_t& seed, float offset,
+                    const float2* ngon = nullptr) {
     const float aspect = (float)W / (float)H;
     const float jx = rnd(seed) - 0.5f;
     const float jy = rnd(seed) - 0.5f;
@@ -820,7 +849,7 @@ DI Ray generate_ray(const CamParams& cam, int W, int H, int px, int py, uint32_t
     const float3 P = f3(cam.pos[0], cam.pos[1], cam.pos[2]);
     const float3 pin = normalize(F + R * (sx * aspect * cam.tan_half) + U * (sy * cam.tan_half));
     float2 lens = make_float2(0.0f, 0.0f);
-    if (cam.lens_radius > 0.0f) lens = sample_ngon(seed, cam.lens_radius, cam.blades);
+    if (cam.lens_radius > 0.0f) lens = sample_ngon(seed, cam.lens_radius, cam.blades, ngon);
     const float nr2 = (cam.lens_radius > 1e-6f)
         ? gclamp((lens.x * lens.x + lens.y * lens.y) / (cam.lens_radius * cam.lens_radius), 0.0f, 1.0f)
         : 0.0f;

@@ -502,13 +502,11 @@ DI void add_caustic(const GatherArgs& A, long pix, int hm, float3 caustic, float
     *a = v;
 }
 
-#if !RC_EXACT
-// Fast build: a pixel whose 27 cells hold more than this many photons (as
-// walked, at most 512 a cell) is gathered by photon_gather_heavy, one warp
-// per pixel.  One thread walking 27 x 512 photons held a whole gather launch
-// (the rest of the GPU idle) for about 0.5 ms.
+// A pixel whose 27 cells hold more than this many photons (as walked, at
+// most 512 a cell) is gathered by photon_gather_heavy, one warp per pixel.
+// One thread walking 27 x 512 photons held a whole gather launch (the rest
+// of the GPU idle) for about 0.5 ms.
 constexpr unsigned int kGatherLight = 64;
-#endif
 
 // photon_gather.comp:128-222: pinhole ray to the first diffuse surface,
 // 3x3x3 hash-cell query, Epanechnikov kernel, added into the accumulation.
@@ -520,9 +518,7 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
     const int W = A.img.width, H = A.img.height;
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0, hits = 0;
-#if !RC_EXACT
     bool heavy = false;
-#endif
     if (px < W && py < H) {
         const DeviceScene& S = A.scene;
         const CamParams& cam = A.cam;
@@ -574,7 +570,6 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
         if (A.cache_mode == 1) A.hit_cache[pix] = make_float4(hp.x, hp.y, hp.z, __int_as_float(found ? hm : -1));
         const float r = A.radius, r2 = r * r;
         const int ccx = (int)floorf(hp.x / r), ccy = (int)floorf(hp.y / r), ccz = (int)floorf(hp.z / r);
-#if !RC_EXACT
         if (found && A.heavy && A.cache_mode != 0) {
             unsigned int total = 0;
             for (int dz = -1; dz <= 1; ++dz)
@@ -587,7 +582,6 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
             heavy = total > kGatherLight;
             found = found && !heavy;
         }
-#endif
         if (found) {
             float3 caustic = f3(0, 0, 0);
             for (int dz = -1; dz <= 1; ++dz)
@@ -634,7 +628,6 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
             add_caustic(A, pix, hm, caustic, r2);
         }
     }
-#if !RC_EXACT
     if (A.heavy) {
         const unsigned int m = __ballot_sync(0xffffffffu, heavy);
         if (m) {
@@ -645,18 +638,20 @@ __global__ void __launch_bounds__(128) photon_gather_kernel(GatherArgs A) {
             if (heavy) A.heavy[base + __popc(m & ((1u << lane) - 1u))] = py * W + px;
         }
     }
-#endif
     const unsigned int rsum = __reduce_add_sync(0xffffffffu, rays);
     if (lane == 0 && rsum) atomicAdd(&A.counters->gather_rays, (unsigned long long)rsum);
     flush_work(g, 0u, 0u, A.counters, true);
 }
 
-#if !RC_EXACT
 // The heavy pixels of photon_gather_kernel, one warp per pixel: lanes 0..26
-// look up the 27 cells, then the warp walks each cell's photons 32 (two
-// loads deep, 64) at a time and sums the caustic with a butterfly
-// reduction.  The photons summed are the reference's (the first 512 of
-// each cell's chain); only the order of the float additions differs.
+// look up the 27 cells, then the warp walks each cell's photons 32 at a
+// time.  The photons summed are the reference's (the first 512 of each
+// cell's chain).  Fast build: two loads deep (64 photons a round), lane
+// sums combined by a butterfly, so only the order of the float additions
+// differs from one thread's walk.  Exact build: each lane forms its
+// photon's term, and the terms of the photons inside the radius are added
+// in chain order (every lane keeps the same running sum from shuffles), so
+// the sum is one thread's walk bit for bit.
 __global__ void __launch_bounds__(256) photon_gather_heavy(GatherArgs A) {
     const unsigned int FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -678,6 +673,35 @@ __global__ void __launch_bounds__(256) photon_gather_heavy(GatherArgs A) {
             cnt = (s1 - s0) < 512u ? (s1 - s0) : 512u;
         }
         float3 caustic = f3(0, 0, 0);
+#if RC_EXACT
+        for (int k = 0; k < 27; ++k) {
+            const unsigned int b = __shfl_sync(FULL, s0, k);
+            const unsigned int m = __shfl_sync(FULL, cnt, k);
+            for (unsigned int q0 = 0; q0 < m; q0 += 32) {
+                const unsigned int q = q0 + lane;
+                float3 term = f3(0, 0, 0);
+                bool inside = false;
+                if (q < m) {
+                    const float4 p = __ldg(A.seg_posw + b + q);
+                    const float3 d = hp - xyz(p);
+                    const float d2 = dot(d, d);
+                    if (d2 <= r2) {
+                        const float w = 1.0f - d2 / r2;
+                        const float2 yz = __ldg(A.seg_powyz + b + q);
+                        term = f3(p.w, yz.x, yz.y) * w;
+                        inside = true;
+                    }
+                }
+                unsigned int in = __ballot_sync(FULL, inside);
+                while (in) {
+                    const int j = __ffs(in) - 1;
+                    in &= in - 1u;
+                    caustic = caustic + f3(__shfl_sync(FULL, term.x, j), __shfl_sync(FULL, term.y, j),
+                                           __shfl_sync(FULL, term.z, j));
+                }
+            }
+        }
+#else
         for (int k = 0; k < 27; ++k) {
             const unsigned int b = __shfl_sync(FULL, s0, k);
             const unsigned int m = __shfl_sync(FULL, cnt, k);
@@ -703,10 +727,10 @@ __global__ void __launch_bounds__(256) photon_gather_heavy(GatherArgs A) {
             caustic.y += __shfl_xor_sync(FULL, caustic.y, o);
             caustic.z += __shfl_xor_sync(FULL, caustic.z, o);
         }
+#endif
         if (lane == 0) add_caustic(A, pix, hm, caustic, r2);
     }
 }
-#endif
 
 // ---------------------------------------------------------------------------
 // photon map: cell-sorted layout
@@ -1083,24 +1107,20 @@ cudaError_t launch_photon_layout(const PhotonArgs& A, cudaStream_t s) {
 
 cudaError_t launch_photon_gather(const GatherArgs& A, cudaStream_t s) {
     const dim3 grid((A.img.width + 15) / 16, (A.img.height + 7) / 8);
-#if !RC_EXACT
     if (A.heavy) {
         const cudaError_t e = cudaMemsetAsync(A.heavy_len, 0, sizeof(unsigned int), s);
         if (e != cudaSuccess) return e;
     }
-#endif
     if (A.scene.depth <= 60)
         photon_gather_kernel<true><<<grid, 128, 0, s>>>(A);
     else
         photon_gather_kernel<false><<<grid, 128, 0, s>>>(A);
-#if !RC_EXACT
     if (A.heavy) {
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         photon_gather_heavy<<<sms * 8, 256, 0, s>>>(A);
     }
-#endif
     return cudaGetLastError();
 }
 

@@ -110,6 +110,12 @@ DI bool lca_on(const CamParams& c) { return (fabs_(c.lca[0]) + fabs_(c.lca[2])) 
 __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     __shared__ BlockAppend sh;
+    // aperture corners for the first segment's blade count (segments with
+    // another count compute theirs directly)
+    __shared__ float2 ngon[kNgonTab];
+    const int tab_n = seg_at(A, 0).cam.blades;
+    const bool tab_ok = ngon_table_ok(tab_n);
+    if (tab_ok) fill_ngon_table(ngon, tab_n);
     if (threadIdx.x == 0) sh.cnt[0] = sh.cnt[1] = 0u;
     __syncthreads();
     uint32_t paths = 0;
@@ -123,7 +129,8 @@ __global__ void __launch_bounds__(256) wf_generate(WaveArgs A) {
             const int f = sg.first_frame + id.sample;
             uint32_t s = init_seed(id.px, id.py, lca ? f * 3 + id.channel : f);
             const Ray r = generate_ray(sg.cam, A.width, A.height, id.px, id.py, s,
-                                       lca ? sg.cam.lca[id.channel] : 0.0f);
+                                       lca ? sg.cam.lca[id.channel] : 0.0f,
+                                       tab_ok && sg.cam.blades == tab_n ? ngon : nullptr);
             B.o[p] = make_float4(r.o.x, r.o.y, r.o.z, 0.0f);
             B.d[p] = make_float4(r.d.x, r.d.y, r.d.z, 0.0f);
             // throughput (1, 1, 1) and radiance 0 are implied at bounce 0:
