@@ -252,7 +252,11 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
 #else
 // Exact build: one step of L with trace_closest's order for closest-hit
 // lanes (see the file comment); shadow lanes park and walk on.
-template <bool kWide, class Scn>
+// kUnordered: trace_unordered's order instead (the photon walks,
+// photon_trace.comp:102-128): the left child first whatever the distances,
+// and a node met with 62 or more entries on the stack has neither child
+// tested nor visited.
+template <bool kWide, bool kUnordered = false, class Scn>
 DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
     bool done = false;
     if (leaf_phase) {
@@ -289,18 +293,20 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                     L.have_node = false;
                     break;
                 }
+            } else if (kUnordered && L.top >= 62) {
+                L.have_node = false;
             } else {
                 const NodeRec* nrec = S.nodes + L.node.ref;
                 const float4 a = __ldg(&nrec->a), b = __ldg(&nrec->b), c = __ldg(&nrec->c);
                 const int4 d = __ldg(&nrec->d);
                 float tl, tr;
                 // a child whose entry lies past the current hit is the one
-                // trace_closest would push and then drop when popping it
+                // the reference's walk would push and then drop when popping it
                 const bool hl = tslab_left(g, L.r, a, b, c, tl) && !(tl > L.h.t);
                 const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
                 if (hl && hr) {
-                    const bool left_first = tl < tr;
-                    if (L.top < 62) {
+                    const bool left_first = kUnordered || tl < tr;
+                    if (kUnordered || L.top < 62) {
                         stk.e[L.top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
                         stk.t[L.top++] = left_first ? tr : tl;
                     }

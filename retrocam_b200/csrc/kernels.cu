@@ -368,6 +368,87 @@ __global__ void __launch_bounds__(256) photon_emit_full_kernel(PhotonArgs A) {
     store_photons(A, none, rays, g);
 }
 
+#if RC_EXACT
+// The first phase as a refill kernel (exact build, trees up to 60 levels):
+// a lane emits the next photon (work counter A.work) when its photon is
+// done and walks the full scene in trace_unordered's order (dyn_step
+// <kUnordered>: left child first, the same culls and stack guard, a
+// reached leaf tested before the next pop), so each photon gets
+// photon_emit_full_kernel's hit bit for bit; photons whose first hit is
+// glass or metal are queued as that kernel queues them.
+__global__ void __launch_bounds__(128) photon_emit_full_dyn(PhotonArgs A) {
+    const unsigned int FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const DeviceScene& S = A.scene;
+    const unsigned int total = S.light_count != 0 ? (unsigned int)A.photon_count : 0u;
+    Guard g = {0u, 0u, 0u};
+    uint32_t rays = 0;
+    DynStack stk;
+    LaneRay L;
+    L.item = -1;
+    L.top = 0;
+    L.have_node = false;
+    L.leaf.cnt = 0;
+    L.any = false;
+    uint32_t seed = 0u;
+    float3 power = f3(0.0f, 0.0f, 0.0f);
+    while (true) {
+        const unsigned int idle = __ballot_sync(FULL, L.item == -1);
+        if (idle) {
+            const int leader = __ffs(idle) - 1;
+            unsigned int base = 0;
+            if (lane == leader) base = atomicAdd(A.work, (unsigned int)__popc(idle));
+            base = __shfl_sync(FULL, base, leader);
+            if (L.item == -1) {
+                const unsigned int i = base + __popc(idle & ((1u << lane) - 1u));
+                L.item = i < total ? (int)i : -2;
+                if (L.item >= 0) {
+                    const PhotonState st = emit_photon(A, S, L.item);
+                    seed = st.seed;
+                    power = st.power;
+                    L.r = st.ray;
+                    ++rays;
+                    dyn_start(S, L, 1e30f, false, g);
+                }
+            }
+        }
+        if (__all_sync(FULL, L.item == -2)) break;
+        while (true) {
+            bool busy = L.item >= 0;
+            bool push = false;
+            bool leaf_phase;
+            if (dyn_schedule(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
+                dyn_step<false, true>(S, L, stk, leaf_phase, g, A.interior_steps)) {
+                if (L.h.prim >= 0) {
+                    const int m = __float_as_int(__ldg(S.tri_shade + 3 * L.h.prim).w);
+                    push = __ldg(S.materials + 4 * m + 2).z > 0.5f || __ldg(S.materials + 4 * m + 0).w > 0.5f;
+                }
+                L.item = -1;
+                busy = false;
+            }
+            const unsigned int mq = __ballot_sync(FULL, push);
+            if (mq) {
+                const int leader = __ffs(mq) - 1;
+                unsigned int base = 0;
+                if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mq));
+                base = __shfl_sync(FULL, base, leader);
+                if (push) {
+                    float4* q = A.queue + 4 * (size_t)(base + __popc(mq & ((1u << lane) - 1u)));
+                    q[0] = make_float4(L.r.o.x, L.r.o.y, L.r.o.z, __uint_as_float(seed));
+                    q[1] = make_float4(L.r.d.x, L.r.d.y, L.r.d.z, power.x);
+                    q[2] = make_float4(power.y, power.z, L.h.t, L.h.u);
+                    q[3] = make_float4(L.h.v, __int_as_float(L.h.prim), 0.0f, 0.0f);
+                }
+            }
+            if (__popc(__ballot_sync(FULL, busy)) < A.refill_lanes) break;
+        }
+    }
+    const unsigned int rsum = __reduce_add_sync(FULL, rays);
+    if (lane == 0 && rsum) atomicAdd(&A.counters->photon_rays, (unsigned long long)rsum);
+    flush_work(g, 0u, 0u, A.counters, true);
+}
+#endif
+
 template <bool kAtParent>
 __global__ void __launch_bounds__(256) photon_bounce_kernel(PhotonArgs A) {
     const unsigned int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1024,9 +1105,14 @@ cudaError_t launch_render(const RenderArgs& A, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-#if !RC_EXACT
-// One persistent grid of photon_emit_dyn per device: every SM times the
-// blocks that fit it, computed once per device.
+// One persistent grid of the build's refill emission kernel
+// (photon_emit_dyn, exact build photon_emit_full_dyn) per device: every SM
+// times the blocks that fit it, computed once per device.
+#if RC_EXACT
+#define RC_EMIT_DYN photon_emit_full_dyn
+#else
+#define RC_EMIT_DYN photon_emit_dyn
+#endif
 static int emit_grid() {
     constexpr int kDevs = 64;
     static std::atomic<int> cache[kDevs];
@@ -1038,12 +1124,12 @@ static int emit_grid() {
         if (g > 0) return g;
     }
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, photon_emit_dyn, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pe, RC_EMIT_DYN, 128, 0);
     const int g = sms * (pe > 0 ? pe : 1);
     if (cached) cache[dev].store(g, std::memory_order_relaxed);
     return g;
 }
-#endif
+#undef RC_EMIT_DYN
 
 cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) {
     const int b = block <= 64 ? 64 : (block <= 128 ? 128 : 256);
@@ -1080,6 +1166,16 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) 
     // queued walks (photon_trace.comp:168-252 in two launches)
     cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
+#if RC_EXACT
+    // the refill emission follows the test-at-parent walk (trees up to 60 levels)
+    if (A.work && A.scene.depth <= 60) {
+        e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
+        if (e != cudaSuccess) return e;
+        photon_emit_full_dyn<<<emit_grid(), 128, 0, s>>>(A);
+        photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
+        return cudaGetLastError();
+    }
+#endif
     if (A.scene.depth <= 60) {
         photon_emit_full_kernel<true><<<blocks, b, 0, s>>>(A);
         photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
