@@ -143,7 +143,11 @@ DI bool dyn_schedule(const LaneRay& L, bool busy, unsigned int act, int leaf_qua
 // not blocked (a leaf parked and the next node a leaf too, or none), so the
 // warp's scheduling work is shared by several moves.  Returns true when the
 // ray is finished: its walk ended, an any-hit ray hit, or the step cap.
-template <bool kWide, class Scn>
+// kDeep: keep the reference's push guard (no push once 62 entries are on
+// the stack); the wavefront trace clears it, since it only runs on trees of
+// at most 28 levels, whose walks never hold more than 28 entries (0.8 ms of
+// a 59 ms trace per export frame).  kUnordered is the exact build's.
+template <bool kWide, bool kUnordered = false, bool kDeep = true, class Scn>
 DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
     bool done = false;
     if (leaf_phase) {
@@ -220,7 +224,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                 const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
                 if (hl && hr) {
                     const bool left_first = tl < tr;
-                    if (L.top < 62) {
+                    if (!kDeep || L.top < 62) {
                         const float tf = left_first ? tr : tl;
                         const int cf = left_first ? d.w : d.y;
                         stk.e[L.top++] =
@@ -256,7 +260,9 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
 // photon_trace.comp:102-128): the left child first whatever the distances,
 // and a node met with 62 or more entries on the stack has neither child
 // tested nor visited.
-template <bool kWide, bool kUnordered = false, class Scn>
+// kDeep as in the fast build (the closest-hit walk's guard; the unordered
+// walk keeps its own).
+template <bool kWide, bool kUnordered = false, bool kDeep = true, class Scn>
 DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
     bool done = false;
     if (leaf_phase) {
@@ -306,7 +312,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                 const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
                 if (hl && hr) {
                     const bool left_first = kUnordered || tl < tr;
-                    if (kUnordered || L.top < 62) {
+                    if (kUnordered || !kDeep || L.top < 62) {
                         stk.e[L.top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
                         stk.t[L.top++] = left_first ? tr : tl;
                     }

@@ -670,7 +670,7 @@ DI void trace_dyn(const WaveArgs& A) {
             bool busy = L.item >= 0;
             bool leaf_phase;
             if (dyn_schedule(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
-                dyn_step<kWide>(S, L, stk, leaf_phase, g, A.interior_steps)) {
+                dyn_step<kWide, false, false>(S, L, stk, leaf_phase, g, A.interior_steps)) {
                 const int item = L.item;
                 if ((unsigned int)item < nr) {
                     const int p = B.rq[cur][item];
