@@ -88,7 +88,7 @@ struct rc_ctx {
     // scene
     DeviceScene scene;
     bool has_scene = false;
-    DevBuf nodes, nodes4, tri_isect, tri_shade, mats, lights, cdf;
+    DevBuf nodes, nodes_packed, nodes4, tri_isect, tri_shade, mats, lights, cdf;
     // SPPM
     DevBuf photons, heads, next, counter, cell_of, cell_count, cell_start, block_sums, seg_photon, seg_posw,
         seg_powyz;
@@ -310,7 +310,7 @@ int rc_ctx_destroy(rc_ctx* ctx) {
     for (void* p : {(void*)ctx->img.accum, (void*)ctx->img.gbuf, (void*)ctx->img.galb, (void*)ctx->img.var,
                     (void*)ctx->out, (void*)ctx->ping, (void*)ctx->pong, (void*)ctx->counters})
         if (p) cudaFree(p);
-    for (DevBuf* b : {&ctx->nodes, &ctx->nodes4, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
+    for (DevBuf* b : {&ctx->nodes, &ctx->nodes_packed, &ctx->nodes4, &ctx->tri_isect, &ctx->tri_shade, &ctx->mats, &ctx->lights, &ctx->cdf,
                       &ctx->photons, &ctx->heads, &ctx->next, &ctx->counter, &ctx->cell_of, &ctx->cell_count,
                       &ctx->cell_start, &ctx->block_sums, &ctx->seg_photon, &ctx->seg_posw, &ctx->seg_powyz,
                       &ctx->wf_o, &ctx->wf_d, &ctx->wf_thr,
@@ -831,6 +831,22 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
         if (n.prim_count > 0 || !seen[i] || (tri_count == 0)) continue;
         node_record(nodes, n, recs[i]);
     }
+    // packed-reference copy for the refill trace (DeviceScene::nodes_packed)
+    const bool packable = tri_count > 0 && max_leaf <= 31 && tri_count < (1 << 26);
+    auto packed_ref = [&](int c) {
+        return nodes[c].prim_count > 0
+                   ? (int)(0x80000000u | ((unsigned int)nodes[c].prim_start << 5) | (unsigned int)nodes[c].prim_count)
+                   : c;
+    };
+    std::vector<NodeRec> precs;
+    if (packable) {
+        precs = recs;
+        for (int i = 0; i < node_count; ++i) {
+            const rc_bvh_node& n = nodes[i];
+            if (n.prim_count > 0 || !seen[i]) continue;
+            precs[i].d = make_int4(packed_ref(n.left_child), packed_ref(n.right_child), 0, 0);
+        }
+    }
     // 4-wide copy for the fast build's traversal; a tree deeper than any SAH
     // build makes keeps the binary traversal (the collapse recurses per level).
     std::vector<Node4> wide;
@@ -860,6 +876,10 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     CK(ensure(ctx->lights, (size_t)(light_count > 0 ? light_count : 1) * sizeof(rc_light)));
     CK(ensure(ctx->cdf, cdf.size() * sizeof(float)));
     CK(copy_h2d(ctx, ctx->nodes.ptr, recs.data(), recs.size() * sizeof(NodeRec)));
+    if (packable) {
+        CK(ensure(ctx->nodes_packed, precs.size() * sizeof(NodeRec)));
+        CK(copy_h2d(ctx, ctx->nodes_packed.ptr, precs.data(), precs.size() * sizeof(NodeRec)));
+    }
     if (tri_count > 0) {
         CK(copy_h2d(ctx, ctx->tri_isect.ptr, isect.data(), isect.size() * sizeof(float4)));
         CK(copy_h2d(ctx, ctx->tri_shade.ptr, shade.data(), shade.size() * sizeof(float4)));
@@ -871,6 +891,8 @@ int rc_scene_upload(rc_ctx* ctx, const rc_triangle* tris, int tri_count, const r
     CK(cudaStreamSynchronize(ctx->stream));  // host staging vectors go out of scope
     DeviceScene& S = ctx->scene;
     S.nodes = (const NodeRec*)ctx->nodes.ptr;
+    S.nodes_packed = packable ? (const NodeRec*)ctx->nodes_packed.ptr : nullptr;
+    S.root_packed = packable ? packed_ref(0) : 0;
     S.nodes4 = wide.empty() ? nullptr : (const Node4*)ctx->nodes4.ptr;
     S.tri_isect = (const float4*)ctx->tri_isect.ptr;
     S.tri_shade = (const float4*)ctx->tri_shade.ptr;

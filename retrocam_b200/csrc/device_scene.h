@@ -49,6 +49,13 @@ struct Node4 {
 
 struct DeviceScene {
     const NodeRec* nodes = nullptr;
+    // The refill trace's copy of the interior records (fast build): as
+    // `nodes` with d = (left, right, 0, 0) packed child references -- a
+    // child node's index, or for a leaf INT_MIN | prim_start << 5 | count --
+    // built when every leaf holds 1..31 triangles and the scene fewer than
+    // 2^26; null otherwise.  root_packed: the root as such a reference.
+    const NodeRec* nodes_packed = nullptr;
+    int root_packed = 0;
     const Node4* nodes4 = nullptr;       // root at index 0 unless the root is a leaf
     const float4* tri_isect = nullptr;   // 3 per triangle
     const float4* tri_shade = nullptr;   // 3 per triangle

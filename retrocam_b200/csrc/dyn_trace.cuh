@@ -49,6 +49,23 @@ DI bool pop_entry(DynStack& stk, int& top, float cull, TravNode& n) {
     }
     return false;
 }
+
+// Packed child references (DeviceScene::nodes_packed): a TravNode's ref
+// alone names a child -- a node index, or for a leaf INT_MIN | prim_start
+// << 5 | count -- so choosing a child is one select, and a stack entry is
+// (reference, the full entry distance).
+DI int pk_start(int p) { return (int)(((unsigned int)p >> 5) & 0x3ffffffu); }
+DI int pk_count(int p) { return p & 31; }
+
+DI bool pop_packed(DynStack& stk, int& top, float cull, TravNode& n) {
+    while (top > 0) {
+        const int2 e = stk.e[--top];
+        if (__int_as_float(e.y) > cull) continue;
+        n.ref = e.x;
+        return true;
+    }
+    return false;
+}
 #else
 // Exact build: (ref, count) and the exact entry distance the parent
 // computed (what the reference's re-test on pop returns); at most 61
@@ -114,6 +131,7 @@ DI void dyn_start(const Scn& S, LaneRay& L, float tmax, bool any, Guard& g) {
     L.h.u = L.h.v = 0.0f;
     L.top = 0;
     L.leaf.cnt = 0;
+    L.leaf.ref = 0;
     L.node.ref = S.root_ref;
     L.node.cnt = S.root_count;
     L.steps = 0;
@@ -124,16 +142,28 @@ DI void dyn_start(const Scn& S, LaneRay& L, float tmax, bool any, Guard& g) {
                   !(tmin > L.h.t);
 }
 
+// Whether n is a leaf, and whether L has a leaf parked, in either encoding.
+template <bool kPacked>
+DI bool is_leaf(const TravNode& n) {
+    return kPacked ? n.ref < 0 : n.cnt > 0;
+}
+template <bool kPacked>
+DI bool parked_leaf(const LaneRay& L) {
+    return is_leaf<kPacked>(L.leaf);
+}
+
 // The warp's choice for this iteration; every lane of the warp calls it with
 // the warp's busy mask `act` (the caller's ballot of `busy`).  Returns
 // whether this lane steps, and the phase.
+template <bool kPacked = false>
 DI bool dyn_schedule(const LaneRay& L, bool busy, unsigned int act, int leaf_quarters, bool& leaf_phase) {
     const unsigned int FULL = 0xffffffffu;
-    const bool blocked = busy && L.leaf.cnt > 0 && (!L.have_node || L.node.cnt > 0);
-    const unsigned int parked = __ballot_sync(FULL, busy && L.leaf.cnt > 0);
+    const bool has = parked_leaf<kPacked>(L);
+    const bool blocked = busy && has && (!L.have_node || is_leaf<kPacked>(L.node));
+    const unsigned int parked = __ballot_sync(FULL, busy && has);
     const unsigned int blk = __ballot_sync(FULL, blocked);
     leaf_phase = parked == act || 4 * __popc(blk) >= leaf_quarters * __popc(act);
-    return busy && (leaf_phase ? L.leaf.cnt > 0 : !blocked);
+    return busy && (leaf_phase ? has : !blocked);
 }
 
 #if !RC_EXACT
@@ -147,11 +177,13 @@ DI bool dyn_schedule(const LaneRay& L, bool busy, unsigned int act, int leaf_qua
 // the stack); the wavefront trace clears it, since it only runs on trees of
 // at most 28 levels, whose walks never hold more than 28 entries (0.8 ms of
 // a 59 ms trace per export frame).  kUnordered is the exact build's.
-template <bool kWide, bool kUnordered = false, bool kDeep = true, class Scn>
+template <bool kWide, bool kUnordered = false, bool kDeep = true, bool kPacked = false, class Scn>
 DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
     bool done = false;
     if (leaf_phase) {
-        for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
+        const int first = kPacked ? pk_start(L.leaf.ref) : L.leaf.ref;
+        const int end = first + (kPacked ? pk_count(L.leaf.ref) : L.leaf.cnt);
+        for (int i = first; i < end; ++i) {
             float t, u, v;
             if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
                 L.h.t = t;
@@ -164,14 +196,17 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                 }
             }
         }
-        L.leaf.cnt = 0;
+        if (kPacked)
+            L.leaf.ref = 0;
+        else
+            L.leaf.cnt = 0;
     } else {
         int m = 0;
         for (; m < interior_steps && L.have_node; ++m) {
-            if (L.node.cnt > 0) {
-                if (L.leaf.cnt > 0) break;   // blocked: a leaf is parked already
+            if (is_leaf<kPacked>(L.node)) {
+                if (parked_leaf<kPacked>(L)) break;   // blocked: a leaf is parked already
                 L.leaf = L.node;
-                L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
+                L.have_node = kPacked ? pop_packed(stk, L.top, L.h.t, L.node) : pop_entry(stk, L.top, L.h.t, L.node);
             } else if (kWide) {
                 // 4-wide node: hit children ordered by entry distance, the
                 // nearest entered, the others pushed far to near
@@ -222,7 +257,19 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                 float tl, tr;
                 const bool hl = tslab_left(g, L.r, a, b, c, tl) && !(tl > L.h.t);
                 const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
-                if (hl && hr) {
+                if (kPacked) {
+                    // d = (left, right) packed references
+                    if (hl && hr) {
+                        const bool left_first = tl < tr;
+                        if (!kDeep || L.top < 62)
+                            stk.e[L.top++] = make_int2(left_first ? d.y : d.x, __float_as_int(left_first ? tr : tl));
+                        L.node.ref = left_first ? d.x : d.y;
+                    } else if (hl || hr) {
+                        L.node.ref = hl ? d.x : d.y;
+                    } else {
+                        L.have_node = pop_packed(stk, L.top, L.h.t, L.node);
+                    }
+                } else if (hl && hr) {
                     const bool left_first = tl < tr;
                     if (!kDeep || L.top < 62) {
                         const float tf = left_first ? tr : tl;
@@ -245,7 +292,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
         }
         L.steps += m;
     }
-    if (!L.have_node && L.leaf.cnt == 0) done = true;
+    if (!L.have_node && !parked_leaf<kPacked>(L)) done = true;
     if (++L.steps > 4 * S.node_count + 64) {
         g.flags |= RC_GUARD_TRAVERSAL_CAP;
         done = true;
@@ -262,8 +309,9 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
 // tested nor visited.
 // kDeep as in the fast build (the closest-hit walk's guard; the unordered
 // walk keeps its own).
-template <bool kWide, bool kUnordered = false, bool kDeep = true, class Scn>
+template <bool kWide, bool kUnordered = false, bool kDeep = true, bool kPacked = false, class Scn>
 DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
+    static_assert(!kPacked, "the exact build walks the unpacked records");
     bool done = false;
     if (leaf_phase) {
         for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {

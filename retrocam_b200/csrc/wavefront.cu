@@ -612,10 +612,13 @@ static int grid_for(const void* fn, int block) {
 // as wf_trace (bit for bit in the exact build); only the schedule differs.
 // kWide: interior steps over the 4-wide nodes (scene.nodes4) instead of the
 // binary records.
-template <bool kWide>
+// kPacked: interior steps over S.nodes_packed (one-register child
+// references, full entry distances on the stack).
+template <bool kWide, bool kPacked>
 DI void trace_dyn(const WaveArgs& A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
+    const StepScene SP = {kPacked ? S.nodes_packed : S.nodes, S.nodes4, S.tri_isect, S.node_count};
     const int cur = A.bounce & 1;
     const int prev = cur ^ 1;
     const unsigned int nr = A.bounce < 6 ? B.qlen[cur] : 0u;
@@ -637,6 +640,7 @@ DI void trace_dyn(const WaveArgs& A) {
     L.top = 0;
     L.have_node = false;
     L.leaf.cnt = 0;
+    L.leaf.ref = 0;
     L.any = false;
     while (true) {
         // ---- refill idle lanes ----
@@ -654,12 +658,14 @@ DI void trace_dyn(const WaveArgs& A) {
                         const int p = B.rq[cur][L.item];
                         L.r = make_ray(xyz(B.o[p]), xyz(B.d[p]));
                         dyn_start(S, L, 1e30f, false, g);
+                        if (kPacked) L.node.ref = S.root_packed;
                         ++closest;
                     } else {
                         const float4* rec = B.srec[prev] + 3 * (L.item - (int)nr);
                         const float4 so = rec[0], sd = rec[1];
                         L.r = make_ray(xyz(so), xyz(sd));
                         dyn_start(S, L, so.w, true, g);
+                        if (kPacked) L.node.ref = S.root_packed;
                         ++shadow;
                     }
                 }
@@ -669,8 +675,8 @@ DI void trace_dyn(const WaveArgs& A) {
         while (true) {
             bool busy = L.item >= 0;
             bool leaf_phase;
-            if (dyn_schedule(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
-                dyn_step<kWide, false, false>(S, L, stk, leaf_phase, g, A.interior_steps)) {
+            if (dyn_schedule<kPacked>(L, busy, __ballot_sync(FULL, busy), A.leaf_quarters, leaf_phase) &&
+                dyn_step<kWide, false, false, kPacked>(SP, L, stk, leaf_phase, g, A.interior_steps)) {
                 const int item = L.item;
                 if ((unsigned int)item < nr) {
                     const int p = B.rq[cur][item];
@@ -702,10 +708,14 @@ DI void trace_dyn(const WaveArgs& A) {
 // Binary walk: registers capped at 56 (62 uncapped, no spills either way),
 // so 9 blocks of 128 threads fit an SM instead of 8; the kernel waits on L1
 // latency and the extra warps pay (65.0 vs 67.4 ms per export frame).
-__global__ void __maxnreg__(56) wf_trace_dyn(WaveArgs A) { trace_dyn<false>(A); }
+__global__ void __maxnreg__(56) wf_trace_dyn(WaveArgs A) { trace_dyn<false, false>(A); }
+#if !RC_EXACT
+// The same over the packed-reference records (scenes that have them).
+__global__ void __maxnreg__(56) wf_trace_dynp(WaveArgs A) { trace_dyn<false, true>(A); }
+#endif
 #if !RC_EXACT
 // 4-wide walk: uncapped (77 registers; 56 spills)
-__global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<true>(A); }
+__global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<true, false>(A); }
 #endif
 
 // Launchers; the chunk sequence (generate, 7 x trace, 6 x shade interleaved,
@@ -714,7 +724,7 @@ __global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<tru
 // kernel and block size (64, 128 or 256 threads).
 struct WfGrids {
     int gen = 0, acc = 0, sort = 0;
-    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, shade_mq[3] = {}, dyn[3] = {}, dyn4[3] = {};
+    int trace0[3] = {}, trace1[3] = {}, shade[3] = {}, shade_mq[3] = {}, dyn[3] = {}, dynp[3] = {}, dyn4[3] = {};
 };
 static int block_class(int block) { return block <= 64 ? 0 : (block <= 128 ? 1 : 2); }
 static void fill_grids(WfGrids& g) {
@@ -730,6 +740,7 @@ static void fill_grids(WfGrids& g) {
         g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
 #if !RC_EXACT
         g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
+        g.dynp[c] = grid_for((const void*)wf_trace_dynp, b);
 #endif
     }
 }
@@ -772,6 +783,12 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
 #if !RC_EXACT
         if (A.scene.nodes4) {
             wf_trace_dyn4<<<grids().dyn4[c], b, 0, s>>>(A);
+            return cudaGetLastError();
+        }
+#endif
+#if !RC_EXACT
+        if (A.scene.nodes_packed) {
+            wf_trace_dynp<<<grids().dynp[c], b, 0, s>>>(A);
             return cudaGetLastError();
         }
 #endif
