@@ -49,7 +49,7 @@ struct Node4 {
 
 struct DeviceScene {
     const NodeRec* nodes = nullptr;
-    // The refill trace's copy of the interior records (fast build): as
+    // The refill trace's copy of the interior records (both builds): as
     // `nodes` with d = (left, right, 0, 0) packed child references -- a
     // child node's index, or for a leaf INT_MIN | prim_start << 5 | count --
     // built when every leaf holds 1..31 triangles and the scene fewer than

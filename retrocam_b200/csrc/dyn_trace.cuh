@@ -50,22 +50,6 @@ DI bool pop_entry(DynStack& stk, int& top, float cull, TravNode& n) {
     return false;
 }
 
-// Packed child references (DeviceScene::nodes_packed): a TravNode's ref
-// alone names a child -- a node index, or for a leaf INT_MIN | prim_start
-// << 5 | count -- so choosing a child is one select, and a stack entry is
-// (reference, the full entry distance).
-DI int pk_start(int p) { return (int)(((unsigned int)p >> 5) & 0x3ffffffu); }
-DI int pk_count(int p) { return p & 31; }
-
-DI bool pop_packed(DynStack& stk, int& top, float cull, TravNode& n) {
-    while (top > 0) {
-        const int2 e = stk.e[--top];
-        if (__int_as_float(e.y) > cull) continue;
-        n.ref = e.x;
-        return true;
-    }
-    return false;
-}
 #else
 // Exact build: (ref, count) and the exact entry distance the parent
 // computed (what the reference's re-test on pop returns); at most 61
@@ -88,6 +72,22 @@ DI bool pop_entry(DynStack& stk, int& top, float cull, TravNode& n) {
 }
 #endif
 
+// Packed child references (DeviceScene::nodes_packed): a TravNode's ref
+// alone names a child -- a node index, or for a leaf INT_MIN | prim_start
+// << 5 | count -- so choosing a child is one select, and a stack entry is
+// (reference, the full entry distance bits) in both builds.
+DI int pk_start(int p) { return (int)(((unsigned int)p >> 5) & 0x3ffffffu); }
+DI int pk_count(int p) { return p & 31; }
+
+DI bool pop_packed(DynStack& stk, int& top, float cull, TravNode& n) {
+    while (top > 0) {
+        const int2 e = stk.e[--top];
+        if (__int_as_float(e.y) > cull) continue;
+        n.ref = e.x;
+        return true;
+    }
+    return false;
+}
 // The members of a DeviceScene that dyn_step reads, for walks whose scene
 // is chosen per lane (a select of four values instead of a whole scene).
 struct StepScene {
@@ -311,10 +311,11 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
 // walk keeps its own).
 template <bool kWide, bool kUnordered = false, bool kDeep = true, bool kPacked = false, class Scn>
 DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard& g, int interior_steps = 1) {
-    static_assert(!kPacked, "the exact build walks the unpacked records");
     bool done = false;
     if (leaf_phase) {
-        for (int i = L.leaf.ref; i < L.leaf.ref + L.leaf.cnt; ++i) {
+        const int first = kPacked ? pk_start(L.leaf.ref) : L.leaf.ref;
+        const int end = first + (kPacked ? pk_count(L.leaf.ref) : L.leaf.cnt);
+        for (int i = first; i < end; ++i) {
             float t, u, v;
             if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
                 L.h.t = t;
@@ -327,22 +328,26 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                 }
             }
         }
-        L.leaf.cnt = 0;
+        if (kPacked)
+            L.leaf.ref = 0;
+        else
+            L.leaf.cnt = 0;
     } else {
         int m = 0;
         for (; m < interior_steps; ++m) {
             if (!L.have_node) {
                 // a closest-hit lane pops only after its parked leaf was
                 // tested, against the distance that leaf may have lowered
-                if (L.leaf.cnt > 0 || L.top == 0) break;
-                L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
+                if (parked_leaf<kPacked>(L) || L.top == 0) break;
+                L.have_node = kPacked ? pop_packed(stk, L.top, L.h.t, L.node) : pop_entry(stk, L.top, L.h.t, L.node);
                 if (!L.have_node) break;
             }
-            if (L.node.cnt > 0) {
-                if (L.leaf.cnt > 0) break;   // blocked: a leaf is parked already
+            if (is_leaf<kPacked>(L.node)) {
+                if (parked_leaf<kPacked>(L)) break;   // blocked: a leaf is parked already
                 L.leaf = L.node;
                 if (L.any) {
-                    L.have_node = pop_entry(stk, L.top, L.h.t, L.node);
+                    L.have_node =
+                        kPacked ? pop_packed(stk, L.top, L.h.t, L.node) : pop_entry(stk, L.top, L.h.t, L.node);
                 } else {
                     L.have_node = false;
                     break;
@@ -358,7 +363,20 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
                 // the reference's walk would push and then drop when popping it
                 const bool hl = tslab_left(g, L.r, a, b, c, tl) && !(tl > L.h.t);
                 const bool hr = tslab_right(g, L.r, a, b, c, tr) && !(tr > L.h.t);
-                if (hl && hr) {
+                if (kPacked) {
+                    // d = (left, right) packed references; the entry
+                    // distance rides in the stack entry
+                    if (hl && hr) {
+                        const bool left_first = kUnordered || tl < tr;
+                        if (kUnordered || !kDeep || L.top < 62)
+                            stk.e[L.top++] = make_int2(left_first ? d.y : d.x, __float_as_int(left_first ? tr : tl));
+                        L.node.ref = left_first ? d.x : d.y;
+                    } else if (hl || hr) {
+                        L.node.ref = hl ? d.x : d.y;
+                    } else {
+                        L.have_node = false;
+                    }
+                } else if (hl && hr) {
                     const bool left_first = kUnordered || tl < tr;
                     if (kUnordered || !kDeep || L.top < 62) {
                         stk.e[L.top] = left_first ? make_int2(d.z, d.w) : make_int2(d.x, d.y);
@@ -379,7 +397,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
         }
         L.steps += m;
     }
-    if (!L.have_node && L.leaf.cnt == 0 && L.top == 0) done = true;
+    if (!L.have_node && !parked_leaf<kPacked>(L) && L.top == 0) done = true;
     if (++L.steps > 4 * S.node_count + 64) {
         g.flags |= RC_GUARD_TRAVERSAL_CAP;
         done = true;

@@ -709,10 +709,8 @@ DI void trace_dyn(const WaveArgs& A) {
 // so 9 blocks of 128 threads fit an SM instead of 8; the kernel waits on L1
 // latency and the extra warps pay (65.0 vs 67.4 ms per export frame).
 __global__ void __maxnreg__(56) wf_trace_dyn(WaveArgs A) { trace_dyn<false, false>(A); }
-#if !RC_EXACT
 // The same over the packed-reference records (scenes that have them).
 __global__ void __maxnreg__(56) wf_trace_dynp(WaveArgs A) { trace_dyn<false, true>(A); }
-#endif
 #if !RC_EXACT
 // 4-wide walk: uncapped (77 registers; 56 spills)
 __global__ void __launch_bounds__(256) wf_trace_dyn4(WaveArgs A) { trace_dyn<true, false>(A); }
@@ -738,9 +736,9 @@ static void fill_grids(WfGrids& g) {
         g.shade[c] = grid_for((const void*)wf_shade<false>, b);
         g.shade_mq[c] = grid_for((const void*)wf_shade<true>, b);
         g.dyn[c] = grid_for((const void*)wf_trace_dyn, b);
+        g.dynp[c] = grid_for((const void*)wf_trace_dynp, b);
 #if !RC_EXACT
         g.dyn4[c] = grid_for((const void*)wf_trace_dyn4, b);
-        g.dynp[c] = grid_for((const void*)wf_trace_dynp, b);
 #endif
     }
 }
@@ -786,12 +784,10 @@ cudaError_t launch_wf_trace(const WaveArgs& A, cudaStream_t s, int block) {
             return cudaGetLastError();
         }
 #endif
-#if !RC_EXACT
         if (A.scene.nodes_packed) {
             wf_trace_dynp<<<grids().dynp[c], b, 0, s>>>(A);
             return cudaGetLastError();
         }
-#endif
         wf_trace_dyn<<<grids().dyn[c], b, 0, s>>>(A);
         return cudaGetLastError();
     }
