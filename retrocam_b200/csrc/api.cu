@@ -376,10 +376,17 @@ static void node_record(const rc_bvh_node* nodes, const rc_bvh_node& n, NodeRec&
 }
 
 static void isect_record(const rc_triangle& t, float4* out3) {
-    // e1, e2 with the same float subtraction the reference does per test
-    out3[0] = make_float4(t.v0[0], t.v0[1], t.v0[2], 0.0f);
-    out3[1] = make_float4(t.v1[0] - t.v0[0], t.v1[1] - t.v0[1], t.v1[2] - t.v0[2], 0.0f);
-    out3[2] = make_float4(t.v2[0] - t.v0[0], t.v2[1] - t.v0[1], t.v2[2] - t.v0[2], 0.0f);
+    // e1, e2 with the same float subtraction the reference does per test;
+    // the w components hold n = e1 x e2 for the fast build's test (the
+    // exact build reads only xyz)
+    const float e1[3] = {t.v1[0] - t.v0[0], t.v1[1] - t.v0[1], t.v1[2] - t.v0[2]};
+    const float e2[3] = {t.v2[0] - t.v0[0], t.v2[1] - t.v0[1], t.v2[2] - t.v0[2]};
+    const float nx = e1[1] * e2[2] - e1[2] * e2[1];
+    const float ny = e1[2] * e2[0] - e1[0] * e2[2];
+    const float nz = e1[0] * e2[1] - e1[1] * e2[0];
+    out3[0] = make_float4(t.v0[0], t.v0[1], t.v0[2], nx);
+    out3[1] = make_float4(e1[0], e1[1], e1[2], ny);
+    out3[2] = make_float4(e2[0], e2[1], e2[2], nz);
 }
 
 // A BVH over a subset of the scene's triangles, in the kernels' layout,

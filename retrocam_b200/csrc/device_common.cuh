@@ -180,7 +180,41 @@ DI bool slab_xy(const Ray& r, float2 lo, float loz, float2 hi, float hiz, float&
 #endif
 }
 
-DI bool hit_triangle(const Ray& r, const float4* __restrict__ tri_isect, int i, float& t, float& u, float& v) {
+#if !RC_EXACT
+// Fast build: Moller-Trumbore with the triangle's normal n = e1 x e2 from the
+// record's w components.  The same determinant and barycentrics as scalar
+// triple products -- a = -d.n, t = f s.n, u = f e2.(s x d), v = -f e1.(s x d)
+// -- so one cross product instead of two, and the distance first: a
+// triangle at or beyond `tmax` (the caller's current hit) is refused before
+// its barycentrics.  Accepts what the reference's test accepts, up to
+// rounding.
+DI bool hit_triangle(const Ray& r, const float4* __restrict__ tri_isect, int i, float tmax, float& t, float& u,
+                     float& v) {
+    const float4 A = __ldg(tri_isect + 3 * i + 0);
+    const float4 B = __ldg(tri_isect + 3 * i + 1);
+    const float4 Cc = __ldg(tri_isect + 3 * i + 2);
+    const float3 v0 = xyz(A), e1 = xyz(B), e2 = xyz(Cc), n = f3(A.w, B.w, Cc.w);
+    const float a = -dot(r.d, n);
+    if (fabs_(a) < 1e-8f) return false;
+    const float f = 1.0f / a;
+    const float3 s = r.o - v0;
+    const float tt = f * dot(s, n);
+    if (tt < 1e-4f || !(tt < tmax)) return false;
+    const float3 c = cross(s, r.d);
+    const float uu = f * dot(e2, c);
+    if (uu < 0.0f || uu > 1.0f) return false;
+    const float vv = -f * dot(e1, c);
+    if (vv < 0.0f || uu + vv > 1.0f) return false;
+    t = tt;
+    u = uu;
+    v = vv;
+    return true;
+}
+#else
+// pathtrace.comp's Moller-Trumbore, operation for operation (tmax unused:
+// the caller compares the distance).
+DI bool hit_triangle(const Ray& r, const float4* __restrict__ tri_isect, int i, float tmax, float& t, float& u,
+                     float& v) {
     const float4 A = __ldg(tri_isect + 3 * i + 0);
     const float4 B = __ldg(tri_isect + 3 * i + 1);
     const float4 Cc = __ldg(tri_isect + 3 * i + 2);
@@ -202,6 +236,7 @@ DI bool hit_triangle(const Ray& r, const float4* __restrict__ tri_isect, int i, 
     v = vv;
     return true;
 }
+#endif
 
 struct Hit {
     float t, u, v;
@@ -258,9 +293,12 @@ DI bool enter_root(const DeviceScene& S, Guard& g, const Ray& r, float& tmin) {
            tslab(g, r, S.root_min[0], S.root_min[1], S.root_min[2], S.root_max[0], S.root_max[1], S.root_max[2], tmin);
 }
 
-DI bool thit(Guard& g, const Ray& r, const float4* __restrict__ tri_isect, int i, float& t, float& u, float& v) {
+// tmax: the caller's current hit distance (or shadow length), which it
+// compares the returned distance against; the fast test may stop early.
+DI bool thit(Guard& g, const Ray& r, const float4* __restrict__ tri_isect, int i, float tmax, float& t, float& u,
+             float& v) {
     ++g.tris;
-    return hit_triangle(r, tri_isect, i, t, u, v);
+    return hit_triangle(r, tri_isect, i, tmax, t, u, v);
 }
 
 // A node to visit: cnt > 0 a leaf with primitives [ref, ref+cnt), else the
@@ -291,7 +329,7 @@ DI Hit trace_closest(const DeviceScene& S, const Ray& r, Guard& g) {
         if (cnt > 0) {
             for (int i = ref; i < ref + cnt; ++i) {
                 float t, u, v;
-                if (thit(g, r, S.tri_isect, i, t, u, v) && t < h.t) {
+                if (thit(g, r, S.tri_isect, i, h.t, t, u, v) && t < h.t) {
                     h.t = t;
                     h.u = u;
                     h.v = v;
@@ -360,7 +398,7 @@ DI Hit trace_unordered(const DeviceScene& S, const Ray& r, Guard& g) {
         if (cnt > 0) {
             for (int i = ref; i < ref + cnt; ++i) {
                 float t, u, v;
-                if (thit(g, r, S.tri_isect, i, t, u, v) && t < h.t) {
+                if (thit(g, r, S.tri_isect, i, h.t, t, u, v) && t < h.t) {
                     h.t = t;
                     h.u = u;
                     h.v = v;
@@ -429,7 +467,7 @@ DI bool trace_shadow(const DeviceScene& S, const Ray& r, float max_dist, Guard& 
         if (cnt > 0) {
             for (int i = ref; i < ref + cnt; ++i) {
                 float t, u, v;
-                if (thit(g, r, S.tri_isect, i, t, u, v) && t < max_dist) return false;
+                if (thit(g, r, S.tri_isect, i, max_dist, t, u, v) && t < max_dist) return false;
             }
         } else if (top < 30) {
             if (kTestAtParent) {
@@ -549,7 +587,7 @@ DI bool traverse_ww(const DeviceScene& S, const Ray& r, float max_t, Guard& g, H
         if (leaf.cnt > 0) {
             for (int i = leaf.ref; i < leaf.ref + leaf.cnt; ++i) {
                 float t, u, v;
-                if (thit(g, r, S.tri_isect, i, t, u, v) && t < h.t) {
+                if (thit(g, r, S.tri_isect, i, h.t, t, u, v) && t < h.t) {
                     if (kAnyHit) return true;
                     h.t = t;
                     h.u = u;
@@ -651,7 +689,7 @@ DI bool traverse4(const DeviceScene& S, const Ray& r, float max_t, Guard& g, Hit
         if (leaf.cnt > 0) {
             for (int i = leaf.ref; i < leaf.ref + leaf.cnt; ++i) {
                 float tt, u, v;
-                if (thit(g, r, S.tri_isect, i, tt, u, v) && tt < h.t) {
+                if (thit(g, r, S.tri_isect, i, h.t, tt, u, v) && tt < h.t) {
                     if (kAnyHit) return true;
                     h.t = tt;
                     h.u = u;

@@ -185,7 +185,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
         const int end = first + (kPacked ? pk_count(L.leaf.ref) : L.leaf.cnt);
         for (int i = first; i < end; ++i) {
             float t, u, v;
-            if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
+            if (thit(g, L.r, S.tri_isect, i, L.h.t, t, u, v) && t < L.h.t) {
                 L.h.t = t;
                 L.h.u = u;
                 L.h.v = v;
@@ -317,7 +317,7 @@ DI bool dyn_step(const Scn& S, LaneRay& L, DynStack& stk, bool leaf_phase, Guard
         const int end = first + (kPacked ? pk_count(L.leaf.ref) : L.leaf.cnt);
         for (int i = first; i < end; ++i) {
             float t, u, v;
-            if (thit(g, L.r, S.tri_isect, i, t, u, v) && t < L.h.t) {
+            if (thit(g, L.r, S.tri_isect, i, L.h.t, t, u, v) && t < L.h.t) {
                 L.h.t = t;
                 L.h.u = u;
                 L.h.v = v;
