@@ -451,27 +451,54 @@ __global__ void __launch_bounds__(128) photon_emit_full_dyn(PhotonArgs A) {
 
 template <bool kAtParent>
 __global__ void __launch_bounds__(256) photon_bounce_kernel(PhotonArgs A) {
-    const unsigned int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const unsigned int n = *A.queue_len;
+    const unsigned int n = min(*A.queue_len, (unsigned int)A.photon_count);
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0;
-    PhotonStore out;
-    out.store = false;
-    if (i < n && i < (unsigned int)A.photon_count) {
-        const float4* q = A.queue + 4 * (size_t)i;
-        const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
-        PhotonState st;
-        st.ray = make_ray(xyz(q0), xyz(q1));
-        st.seed = __float_as_uint(q0.w);
-        st.power = f3(q1.w, q2.x, q2.y);
-        Hit h;
-        h.t = q2.z;
-        h.u = q2.w;
-        h.v = q3.x;
-        h.prim = __float_as_int(q3.y);
-        out = photon_walk<kAtParent>(A, A.scene, st, true, h, g, rays);
+    const int lane = threadIdx.x & 31;
+    // a warp takes the next 32 queued photons (work counter A.work, zero at
+    // launch) when its last ones are done: a persistent grid sized to the
+    // GPU instead of one thread per emitted photon, most of them idle
+    while (true) {
+        unsigned int base = 0;
+        if (lane == 0) base = atomicAdd(A.work, 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= n) break;
+        const unsigned int i = base + lane;
+        PhotonStore out;
+        out.store = false;
+        if (i < n) {
+            const float4* q = A.queue + 4 * (size_t)i;
+            const float4 q0 = q[0], q1 = q[1], q2 = q[2], q3 = q[3];
+            PhotonState st;
+            st.ray = make_ray(xyz(q0), xyz(q1));
+            st.seed = __float_as_uint(q0.w);
+            st.power = f3(q1.w, q2.x, q2.y);
+            Hit h;
+            h.t = q2.z;
+            h.u = q2.w;
+            h.v = q3.x;
+            h.prim = __float_as_int(q3.y);
+            out = photon_walk<kAtParent>(A, A.scene, st, true, h, g, rays);
+        }
+        append_photons(A, out);
     }
-    store_photons(A, out, rays, g);
+    PhotonStore none;
+    none.store = false;
+    store_photons(A, none, rays, g);
+}
+
+// The queued walks: the work counter cleared, then a grid of every SM times
+// the blocks that fit it (at most one thread per queue slot).
+template <bool kAtParent>
+static cudaError_t launch_bounce(const PhotonArgs& A, cudaStream_t s, int b, int blocks) {
+    cudaError_t e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
+    if (e != cudaSuccess) return e;
+    int dev = 0, sms = 148, per = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, photon_bounce_kernel<kAtParent>, b, 0);
+    photon_bounce_kernel<kAtParent><<<std::min(blocks, sms * std::max(per, 1)), b, 0, s>>>(A);
+    return cudaGetLastError();
 }
 
 #if !RC_EXACT
@@ -1135,55 +1162,44 @@ cudaError_t launch_photon_trace(const PhotonArgs& A, cudaStream_t s, int block) 
     const int b = block <= 64 ? 64 : (block <= 128 ? 128 : 256);
     const int blocks = (A.photon_count + b - 1) / b;
     if (blocks == 0) return cudaSuccess;
-#if !RC_EXACT
-    if (A.split && A.queue && A.work && A.scene.max_leaf < 0x10000 && A.spec.max_leaf < 0x10000 &&
-        A.diff.max_leaf < 0x10000) {
-        // refill emission: one persistent grid (the stack entries pack a
-        // leaf's triangle count into 16 bits)
-        cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
-        if (e == cudaSuccess) e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
-        if (e != cudaSuccess) return e;
-        photon_emit_dyn<<<emit_grid(), 128, 0, s>>>(A);
-        if (A.scene.depth <= 60)
-            photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
-        else
-            photon_bounce_kernel<false><<<blocks, b, 0, s>>>(A);
-        return cudaGetLastError();
-    }
-    if (A.split && A.queue) {
-        cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
-        if (e != cudaSuccess) return e;
-        photon_emit_kernel<<<blocks, b, 0, s>>>(A);
-        if (A.scene.depth <= 60)
-            photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
-        else
-            photon_bounce_kernel<false><<<blocks, b, 0, s>>>(A);
-        return cudaGetLastError();
-    }
-#endif
-    // without the split (exact math, or scenes too large for the split
-    // BVHs): the emission and first segment over the full scene, then the
-    // queued walks (photon_trace.comp:168-252 in two launches)
+    // both phases count in A.queue_len (the queue) and A.work (the refill
+    // kernels' and the walks' work counters)
+    if (!A.queue || !A.queue_len || !A.work) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(A.queue_len, 0, sizeof(unsigned int), s);
     if (e != cudaSuccess) return e;
-#if RC_EXACT
+    const bool at_parent = A.scene.depth <= 60;
+#if !RC_EXACT
+    if (A.split) {
+        if (A.scene.max_leaf < 0x10000 && A.spec.max_leaf < 0x10000 && A.diff.max_leaf < 0x10000) {
+            // refill emission: one persistent grid (the stack entries pack a
+            // leaf's triangle count into 16 bits)
+            e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
+            if (e != cudaSuccess) return e;
+            photon_emit_dyn<<<emit_grid(), 128, 0, s>>>(A);
+        } else {
+            photon_emit_kernel<<<blocks, b, 0, s>>>(A);
+        }
+    } else
+#else
     // the refill emission follows the test-at-parent walk (trees up to 60 levels)
-    if (A.work && A.scene.depth <= 60) {
+    if (at_parent) {
         e = cudaMemsetAsync(A.work, 0, sizeof(unsigned int), s);
         if (e != cudaSuccess) return e;
         photon_emit_full_dyn<<<emit_grid(), 128, 0, s>>>(A);
-        photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
-        return cudaGetLastError();
-    }
+    } else
 #endif
-    if (A.scene.depth <= 60) {
-        photon_emit_full_kernel<true><<<blocks, b, 0, s>>>(A);
-        photon_bounce_kernel<true><<<blocks, b, 0, s>>>(A);
-    } else {
-        photon_emit_full_kernel<false><<<blocks, b, 0, s>>>(A);
-        photon_bounce_kernel<false><<<blocks, b, 0, s>>>(A);
+    {
+        // without the split (exact math, or scenes too large for the split
+        // BVHs): the emission and first segment over the full scene, then
+        // the queued walks (photon_trace.comp:168-252 in two launches)
+        if (at_parent)
+            photon_emit_full_kernel<true><<<blocks, b, 0, s>>>(A);
+        else
+            photon_emit_full_kernel<false><<<blocks, b, 0, s>>>(A);
     }
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return at_parent ? launch_bounce<true>(A, s, b, blocks) : launch_bounce<false>(A, s, b, blocks);
 }
 
 // The cell-sorted layout of the map the trace just stored (4 launches).
