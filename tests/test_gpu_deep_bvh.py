@@ -222,8 +222,8 @@ def test_render_exact_bit_identical_stress_scene(product, orc, stress, engine):
 
 
 def test_render_fast_close_stress_scene(product, orc, stress):
-    """The stress scene in the benchmarked build (refill trace, packed
-    8-byte stack entries with truncated entry distances)."""
+    """The stress scene in the benchmarked build (the refill trace over the
+    packed-reference records)."""
     w, sc, cam = stress
     W, H, spp = 96, 54, 2
     settings = (w.nee_enabled, w.nee_firefly_clamp)
