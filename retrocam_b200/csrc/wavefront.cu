@@ -282,11 +282,13 @@ __global__ void __launch_bounds__(256) wf_sort(WaveArgs A) {
 // One bounce of pathtrace.comp's traceRadiance for every path in ray queue
 // rq[bounce&1] whose closest hit wf_trace has stored (misses end here), or,
 // with material queues (kMQ), for the hits wf_sort queued from it.
-// Registers capped at 72 (105 uncapped, no spills at 72; 64 spills): the
-// kernel streams path state and waits on memory, so resident warps matter
-// more than registers (7 blocks of 128 threads per SM instead of 4).
+// Registers capped: the kernel streams path state and waits on memory, so
+// resident warps matter more than registers.  Fast build 64 (no spills
+// since the radiance is read lazily; 56 spills): 8 blocks of 128 threads
+// per SM, 14.8 ms per export frame vs 15.3 at a 72 cap.  Exact build 72
+// (64 spills 40 bytes).
 template <bool kMQ>
-__global__ void __maxnreg__(72) wf_shade(WaveArgs A) {
+__global__ void __maxnreg__(RC_EXACT ? 72 : 64) wf_shade(WaveArgs A) {
     const WaveBuffers& B = A.wb;
     const DeviceScene& S = A.scene;
     const int cur = A.bounce & 1;
