@@ -1,6 +1,7 @@
 // dyn_trace.cuh -- the per-lane traversal state machine of the refill
-// kernels (camera / shadow rays in wavefront.cu, both builds; photon
-// segments in kernels.cu, fast build).
+// kernels (camera / shadow rays in wavefront.cu, both builds; photon first
+// segments in kernels.cu: the fast build's split walk, the exact build's
+// full-scene walk in the reference's photon order).
 //
 // A lane owns one ray at a time and advances it per loop iteration of its
 // warp: interior nodes, parking a reached leaf, or the triangles of a parked
@@ -19,6 +20,10 @@
 // kept exactly -- trace_closest's visits in trace_closest's order, so the
 // same hit bit for bit; shadow lanes walk on as in the fast build (a yes/no
 // that does not depend on the order).
+//
+// Node references come in two encodings: (ref, count) pairs from the plain
+// records, or one packed word per child from DeviceScene::nodes_packed
+// (kPacked), whose stack entries keep the full entry distance.
 #ifndef RC_DYN_TRACE_CUH
 #define RC_DYN_TRACE_CUH
 
@@ -29,10 +34,11 @@ namespace RC_NS {
 
 #if !RC_EXACT
 // Stack entries: the binary walk pushes at most one per level (guarded at
-// 62, as the reference), the 4-wide walk up to three.  An entry is 8 bytes:
-// (ref, count | entry distance truncated to its top 16 bits); truncation
-// rounds a positive distance down, so the cull `t > hit` never drops a
-// needed entry.
+// 62, as the reference, where the tree can be that deep), the 4-wide walk
+// up to three.  An entry is 8 bytes: over the plain records (ref, count |
+// entry distance truncated to its top 16 bits) -- truncation rounds a
+// positive distance down, so the cull `t > hit` never drops a needed
+// entry; over the packed records (reference, entry distance).
 constexpr int kDynStack = 96;
 struct DynStack {
     int2 e[kDynStack];
