@@ -259,6 +259,27 @@ DI void append_photons(const PhotonArgs& A, const PhotonStore& s) {
     }
 }
 
+// Queues, for the walks, the photons of the warp that `want` it: (origin,
+// seed), (direction, power.x), (power.y, power.z, t, u), (v, triangle) --
+// the ray, generator state and power after emission, and the first hit.
+// One atomicAdd on A.queue_len per warp; every lane of the warp calls it.
+DI void queue_photon(const PhotonArgs& A, bool want, const Ray& ray, uint32_t seed, float3 power, const Hit& h) {
+    const unsigned int mask = __ballot_sync(0xffffffffu, want);
+    if (mask == 0u) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    unsigned int base = 0;
+    if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (want) {
+        float4* q = A.queue + 4 * (size_t)(base + __popc(mask & ((1u << lane) - 1u)));
+        q[0] = make_float4(ray.o.x, ray.o.y, ray.o.z, __uint_as_float(seed));
+        q[1] = make_float4(ray.d.x, ray.d.y, ray.d.z, power.x);
+        q[2] = make_float4(power.y, power.z, h.t, h.u);
+        q[3] = make_float4(h.v, __int_as_float(h.prim), 0.0f, 0.0f);
+    }
+}
+
 // append_photons, then the warp's ray and work counters.
 DI void store_photons(const PhotonArgs& A, const PhotonStore& s, uint32_t rays, Guard& g) {
     append_photons(A, s);
@@ -295,28 +316,14 @@ __global__ void __launch_bounds__(256) photon_emit_kernel(PhotonArgs A) {
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0;
     bool want = false;
-    PhotonState st;
-    Hit h;
+    PhotonState st{};
+    Hit h{};
     if (gid < A.photon_count && S.light_count != 0) {
         st = emit_photon(A, S, gid);
         ++rays;
         want = first_specular(A, st.ray, g, h);
     }
-    const unsigned int mask = __ballot_sync(0xffffffffu, want);
-    const int lane = threadIdx.x & 31;
-    if (mask != 0u) {
-        const int leader = __ffs(mask) - 1;
-        unsigned int base = 0;
-        if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mask));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (want) {
-            float4* q = A.queue + 4 * (size_t)(base + __popc(mask & ((1u << lane) - 1u)));
-            q[0] = make_float4(st.ray.o.x, st.ray.o.y, st.ray.o.z, __uint_as_float(st.seed));
-            q[1] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, st.power.x);
-            q[2] = make_float4(st.power.y, st.power.z, h.t, h.u);
-            q[3] = make_float4(h.v, __int_as_float(h.prim), 0.0f, 0.0f);
-        }
-    }
+    queue_photon(A, want, st.ray, st.seed, st.power, h);
     PhotonStore none;
     none.store = false;
     store_photons(A, none, rays, g);
@@ -337,8 +344,8 @@ __global__ void __launch_bounds__(256) photon_emit_full_kernel(PhotonArgs A) {
     Guard g = {0u, 0u, 0u};
     uint32_t rays = 0;
     bool want = false;
-    PhotonState st;
-    Hit h;
+    PhotonState st{};
+    Hit h{};
     if (gid < A.photon_count && S.light_count != 0) {
         st = emit_photon(A, S, gid);
         ++rays;
@@ -348,21 +355,7 @@ __global__ void __launch_bounds__(256) photon_emit_full_kernel(PhotonArgs A) {
             want = __ldg(S.materials + 4 * m + 2).z > 0.5f || __ldg(S.materials + 4 * m + 0).w > 0.5f;
         }
     }
-    const unsigned int mask = __ballot_sync(0xffffffffu, want);
-    const int lane = threadIdx.x & 31;
-    if (mask != 0u) {
-        const int leader = __ffs(mask) - 1;
-        unsigned int base = 0;
-        if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mask));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (want) {
-            float4* q = A.queue + 4 * (size_t)(base + __popc(mask & ((1u << lane) - 1u)));
-            q[0] = make_float4(st.ray.o.x, st.ray.o.y, st.ray.o.z, __uint_as_float(st.seed));
-            q[1] = make_float4(st.ray.d.x, st.ray.d.y, st.ray.d.z, st.power.x);
-            q[2] = make_float4(st.power.y, st.power.z, h.t, h.u);
-            q[3] = make_float4(h.v, __int_as_float(h.prim), 0.0f, 0.0f);
-        }
-    }
+    queue_photon(A, want, st.ray, st.seed, st.power, h);
     PhotonStore none;
     none.store = false;
     store_photons(A, none, rays, g);
@@ -426,20 +419,7 @@ __global__ void __launch_bounds__(128) photon_emit_full_dyn(PhotonArgs A) {
                 L.item = -1;
                 busy = false;
             }
-            const unsigned int mq = __ballot_sync(FULL, push);
-            if (mq) {
-                const int leader = __ffs(mq) - 1;
-                unsigned int base = 0;
-                if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(mq));
-                base = __shfl_sync(FULL, base, leader);
-                if (push) {
-                    float4* q = A.queue + 4 * (size_t)(base + __popc(mq & ((1u << lane) - 1u)));
-                    q[0] = make_float4(L.r.o.x, L.r.o.y, L.r.o.z, __uint_as_float(seed));
-                    q[1] = make_float4(L.r.d.x, L.r.d.y, L.r.d.z, power.x);
-                    q[2] = make_float4(power.y, power.z, L.h.t, L.h.u);
-                    q[3] = make_float4(L.h.v, __int_as_float(L.h.prim), 0.0f, 0.0f);
-                }
-            }
+            queue_photon(A, push, L.r, seed, power, L.h);
             if (__popc(__ballot_sync(FULL, busy)) < A.refill_lanes) break;
         }
     }
@@ -570,20 +550,7 @@ __global__ void __launch_bounds__(128) photon_emit_dyn(PhotonArgs A) {
                     busy = false;
                 }
             }
-            const unsigned int m = __ballot_sync(FULL, push);
-            if (m) {
-                const int leader = __ffs(m) - 1;
-                unsigned int base = 0;
-                if (lane == leader) base = atomicAdd(A.queue_len, (unsigned int)__popc(m));
-                base = __shfl_sync(FULL, base, leader);
-                if (push) {
-                    float4* q = A.queue + 4 * (size_t)(base + __popc(m & ((1u << lane) - 1u)));
-                    q[0] = make_float4(L.r.o.x, L.r.o.y, L.r.o.z, __uint_as_float(seed));
-                    q[1] = make_float4(L.r.d.x, L.r.d.y, L.r.d.z, power.x);
-                    q[2] = make_float4(power.y, power.z, hs.t, hs.u);
-                    q[3] = make_float4(hs.v, __int_as_float(hs.prim), 0.0f, 0.0f);
-                }
-            }
+            queue_photon(A, push, L.r, seed, power, hs);
             if (__popc(__ballot_sync(FULL, busy)) < A.refill_lanes) break;
         }
     }
