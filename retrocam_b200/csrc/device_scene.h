@@ -5,15 +5,18 @@
 //   node records   64 B per BVH node: the AABBs of BOTH children plus their
 //                  (ref, count) pairs, so an interior visit is one 64-byte
 //                  line and the child tests need no further loads.
-//                    a = (L.min.x, L.min.y, L.min.z, L.max.x)
-//                    b = (L.max.y, L.max.z, R.min.x, R.min.y)
-//                    c = (R.min.z, R.max.x, R.max.y, R.max.z)
+//                    a = (L.min.x, L.min.y, L.max.x, L.max.y)
+//                    b = (R.min.x, R.min.y, R.max.x, R.max.y)
+//                    c = (L.min.z, L.max.z, R.min.z, R.max.z)
 //                    d = (L.ref, L.count, R.ref, R.count)
 //                  ref is a node index when count == 0, else prim_start.
-//                  Records of leaf nodes are never read.
+//                  Records of leaf nodes are never read.  A second copy with
+//                  packed child references (DeviceScene::nodes_packed) serves
+//                  the refill trace.
 //   tri_isect      48 B per triangle: v0, e1 = v1 - v0, e2 = v2 - v0 (the
 //                  differences the reference computes per test, computed once
-//                  on the host with the same float subtraction).
+//                  on the host with the same float subtraction); the w
+//                  components hold n = e1 x e2 for the fast build's test.
 //   tri_shade      48 B per triangle: n0 (+ material index bits in .w), n1, n2;
 //                  read only for the accepted closest hit.
 //   materials      64 B per material (the std430 record).
